@@ -1,0 +1,302 @@
+"""exafmm-dev_b200: Python binding of the B200 Laplace FMM (libexafmm_b200.so).
+
+The solver runs entirely on the GPU through the C ABI declared in include/exafmm_b200.h;
+this module only marshals arrays.  It mirrors the reference's single-node API surface
+(examples/serial.cxx:46-60):
+
+    s = Solver(basis="spherical", P=10, theta=0.35, ncrit=64, precision="f32")
+    s.set_bodies(x, q)                 # Bodies (include/types.h:66-72)
+    s.build_tree()                     # BoundBox::getBounds + BuildTree::buildTree
+    s.upward_pass()                    # UpDownPass::upwardPass
+    s.traverse()                       # Traversal::dualTreeTraversal (M2L + P2P)
+    s.downward_pass()                  # UpDownPass::downwardPass
+    trg = s.trg()                      # (n, 4): phi, dphi/dx, dphi/dy, dphi/dz
+
+or ``s.solve(x, q)`` for the whole sequence.  There is no CPU fallback: without the
+built library or a B200 every call raises FmmError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexafmm_b200.so")
+
+FMM_OK, FMM_ERR_INVALID, FMM_ERR_CUDA, FMM_ERR_NOT_SUPPORTED = 0, 1, 2, 3
+FMM_ERR_NO_MEMORY, FMM_ERR_STATE, FMM_ERR_NO_DEVICE, FMM_ERR_DEVICE = 4, 5, 6, 7
+SPHERICAL, CARTESIAN = 0, 1
+FP32, FP64 = 0, 1
+PHASES = ("bounds", "tree", "upward", "traverse", "m2l", "p2p", "downward", "total")
+
+
+class FmmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("exafmm_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Config(C.Structure):
+    """fmm_b200_config (include/exafmm_b200.h)."""
+    _fields_ = [("basis", C.c_int), ("P", C.c_int), ("theta", C.c_double),
+                ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
+                ("use_ropt", C.c_int), ("precision", C.c_int), ("eps2", C.c_double),
+                ("images", C.c_int), ("device", C.c_int)]
+
+
+# every entry point of include/exafmm_b200.h with its ctypes signature
+_vp, _i, _d, _ll = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+SIGNATURES = {
+    "fmm_b200_default_config": (_i, [_vp]),
+    "fmm_b200_create": (_i, [_vp, _vp]),
+    "fmm_b200_destroy": (_i, [_vp]),
+    "fmm_b200_set_stream": (_i, [_vp, _vp]),
+    "fmm_b200_last_error": (C.c_char_p, [_vp]),
+    "fmm_b200_supported_orders": (_i, [_i, _vp, _i]),
+    "fmm_b200_solve_device": (_i, [_vp, _i, _vp, _vp]),
+    "fmm_b200_solve_host": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "fmm_b200_set_bodies_host": (_i, [_vp, _i, _vp, _vp]),
+    "fmm_b200_set_bodies_device": (_i, [_vp, _i, _vp]),
+    "fmm_b200_build_tree": (_i, [_vp]),
+    "fmm_b200_upward_pass": (_i, [_vp]),
+    "fmm_b200_traverse": (_i, [_vp]),
+    "fmm_b200_downward_pass": (_i, [_vp]),
+    "fmm_b200_get_trg_host": (_i, [_vp, _vp]),
+    "fmm_b200_get_trg_device": (_i, [_vp, _vp]),
+    "fmm_b200_num_cells": (_i, [_vp, _vp, _vp]),
+    "fmm_b200_get_cells": (_i, [_vp] + [_vp] * 9),
+    "fmm_b200_get_order": (_i, [_vp, _vp]),
+    "fmm_b200_get_box": (_i, [_vp, _vp]),
+    "fmm_b200_get_expansion": (_i, [_vp, _i, _vp]),
+    "fmm_b200_num_lists": (_i, [_vp, _vp, _vp, _vp]),
+    "fmm_b200_get_lists": (_i, [_vp, _vp, _vp]),
+    "fmm_b200_get_timings": (_i, [_vp, _vp]),
+    "fmm_b200_direct": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
+    "fmm_b200_fp32_peak": (_i, [_i, _vp]),
+    "fmm_b200_kernel_launches": (_ll, []),
+    "FMM_Init": (None, [_i]),
+    "FMM_Finalize": (None, []),
+    "FMM_Partition": (None, [_vp, _vp, _vp, _vp, _d]),
+    "FMM_Coulomb": (None, [_i, _vp, _vp, _vp, _vp, _d]),
+    "fmm_init_": (None, [_vp, _vp, _vp]),
+    "fmm_finalize_": (None, []),
+    "fmm_partition_": (None, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "fmm_coulomb_": (None, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libexafmm_b200.so (built by __graft_entry__.build() / make -C csrc)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise FmmError(FMM_ERR_NO_DEVICE, "libexafmm_b200.so is not built (%s)" % path)
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype, f.argtypes = res, args
+        _lib = lib
+    return _lib
+
+
+def supported_orders(basis=SPHERICAL):
+    lib = load_library()
+    buf = (C.c_int * 64)()
+    n = lib.fmm_b200_supported_orders(basis, buf, 64)
+    return list(buf[:n])
+
+
+def direct(xt, xs, qs, eps2=0.0, device=0):
+    """FP64 direct sum on the GPU (Traversal::direct + normalize): (nt, 4) phi, grad phi."""
+    lib = load_library()
+    xt = np.ascontiguousarray(xt, np.float64).reshape(-1, 3)
+    xs = np.ascontiguousarray(xs, np.float64).reshape(-1, 3)
+    qs = np.ascontiguousarray(qs, np.float64).reshape(-1)
+    out = np.zeros((len(xt), 4))
+    rc = lib.fmm_b200_direct(device, len(xt), _p(xt), len(xs), _p(xs), _p(qs), eps2, _p(out))
+    if rc != FMM_OK:
+        raise FmmError(rc, "direct sum failed")
+    return out
+
+
+def fp32_peak_tflops(device=0):
+    lib = load_library()
+    t = C.c_double()
+    rc = lib.fmm_b200_fp32_peak(device, C.byref(t))
+    if rc != FMM_OK:
+        raise FmmError(rc, "fp32 peak probe failed")
+    return t.value
+
+
+def kernel_launches():
+    return load_library().fmm_b200_kernel_launches()
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _basis(b):
+    if isinstance(b, str):
+        return {"spherical": SPHERICAL, "cartesian": CARTESIAN}[b.lower()]
+    return int(b)
+
+
+def _prec(p):
+    if isinstance(p, str):
+        return {"f32": FP32, "fp32": FP32, "f64": FP64, "fp64": FP64}[p.lower()]
+    return int(p)
+
+
+class Solver:
+    """One device-resident FMM solver handle (re-entrant per instance)."""
+
+    def __init__(self, basis="spherical", P=10, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
+                 use_ropt=1, precision="f32", eps2=0.0, images=0, device=0):
+        self.lib = load_library()
+        cfg = Config()
+        self.lib.fmm_b200_default_config(C.byref(cfg))
+        cfg.basis, cfg.P, cfg.theta, cfg.ncrit = _basis(basis), P, theta, ncrit
+        cfg.nspawn, cfg.use_rmax, cfg.use_ropt = nspawn, use_rmax, use_ropt
+        cfg.precision, cfg.eps2, cfg.images, cfg.device = _prec(precision), eps2, images, device
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        rc = self.lib.fmm_b200_create(C.byref(cfg), C.byref(self.h))
+        if rc != FMM_OK:
+            raise FmmError(rc, self.lib.fmm_b200_last_error(None).decode())
+        self.n = 0
+        spherical = cfg.basis == SPHERICAL
+        self.nterm = P * (P + 1) // 2 if spherical else P * (P + 1) * (P + 2) // 6
+        self.spherical = spherical
+        self.dtype = np.float32 if cfg.precision == FP32 else np.float64
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.fmm_b200_destroy(h)
+            self.h = None
+
+    def close(self):
+        self.__del__()
+
+    def _check(self, rc):
+        if rc != FMM_OK:
+            raise FmmError(rc, self.lib.fmm_b200_last_error(self.h).decode())
+
+    # ---- configuration
+    def set_stream(self, stream_handle):
+        """Issue work on a cudaStream_t (an int handle, e.g. torch.cuda.Stream.cuda_stream)."""
+        self._check(self.lib.fmm_b200_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    # ---- stages
+    def set_bodies(self, x, q):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, np.float64).reshape(-1)
+        self.n = len(q)
+        self._check(self.lib.fmm_b200_set_bodies_host(self.h, self.n, _p(x), _p(q)))
+
+    def set_bodies_device(self, n, dev_ptr):
+        self.n = n
+        self._check(self.lib.fmm_b200_set_bodies_device(self.h, n, C.c_void_p(dev_ptr)))
+
+    def build_tree(self):
+        self._check(self.lib.fmm_b200_build_tree(self.h))
+
+    def upward_pass(self):
+        self._check(self.lib.fmm_b200_upward_pass(self.h))
+
+    def traverse(self):
+        self._check(self.lib.fmm_b200_traverse(self.h))
+
+    def downward_pass(self):
+        self._check(self.lib.fmm_b200_downward_pass(self.h))
+
+    def trg(self):
+        out = np.zeros((self.n, 4))
+        if self.n:
+            self._check(self.lib.fmm_b200_get_trg_host(self.h, _p(out)))
+        return out
+
+    # ---- whole solves
+    def solve(self, x, q):
+        """Host arrays in, (n, 4) potential + gradient out (FMM_Coulomb-style call)."""
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, np.float64).reshape(-1)
+        n = len(q)
+        p = np.zeros(n)
+        f = np.zeros((n, 3))
+        self._check(self.lib.fmm_b200_solve_host(self.h, n, _p(x), _p(q), _p(p), _p(f)))
+        self.n = n
+        return np.concatenate([p[:, None], f], axis=1)
+
+    def solve_host_ptrs(self, n, x_ptr, q_ptr, p_ptr, f_ptr):
+        """solve_host on raw host pointers (pinned buffers for end-to-end timing)."""
+        self.n = n
+        self._check(self.lib.fmm_b200_solve_host(self.h, n, C.c_void_p(x_ptr), C.c_void_p(q_ptr),
+                                                 C.c_void_p(p_ptr), C.c_void_p(f_ptr)))
+
+    def solve_device(self, n, bodies_ptr, trg_ptr):
+        """Device 4-vectors (x, y, z, q) in, device 4-vectors out, working precision."""
+        self.n = n
+        self._check(self.lib.fmm_b200_solve_device(self.h, n, C.c_void_p(bodies_ptr),
+                                                   C.c_void_p(trg_ptr)))
+
+    # ---- introspection
+    def num_cells(self):
+        nc, ml = C.c_int(), C.c_int()
+        self._check(self.lib.fmm_b200_num_cells(self.h, C.byref(nc), C.byref(ml)))
+        return nc.value, ml.value
+
+    def cells(self):
+        nc, _ = self.num_cells()
+        out = dict(iparent=np.zeros(nc, np.int32), ichild=np.zeros(nc, np.int32),
+                   nchild=np.zeros(nc, np.int32), ibody=np.zeros(nc, np.int32),
+                   nbody=np.zeros(nc, np.int32), icell=np.zeros(nc, np.uint64),
+                   level=np.zeros(nc, np.int32), X=np.zeros((nc, 3)), R=np.zeros(nc))
+        if nc:
+            self._check(self.lib.fmm_b200_get_cells(
+                self.h, *[_p(out[k]) for k in ("iparent", "ichild", "nchild", "ibody", "nbody",
+                                                 "icell", "level", "X", "R")]))
+        return out
+
+    def order(self):
+        o = np.zeros(self.n, np.int32)
+        if self.n:
+            self._check(self.lib.fmm_b200_get_order(self.h, _p(o)))
+        return o
+
+    def box(self):
+        b = np.zeros(4)
+        self._check(self.lib.fmm_b200_get_box(self.h, _p(b)))
+        return b
+
+    def expansion(self, which):
+        """which: 0 = M, 1 = L.  Spherical -> complex (nc, nterm), Cartesian -> (nc, nterm)."""
+        nc, _ = self.num_cells()
+        w = 2 if self.spherical else 1
+        a = np.zeros(nc * self.nterm * w)
+        if nc:
+            self._check(self.lib.fmm_b200_get_expansion(self.h, which, _p(a)))
+        if self.spherical:
+            a = a.reshape(-1, 2)
+            return (a[:, 0] + 1j * a[:, 1]).reshape(nc, self.nterm)
+        return a.reshape(nc, self.nterm)
+
+    def list_counts(self):
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._check(self.lib.fmm_b200_num_lists(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def lists(self):
+        nm2l, np2p, _ = self.list_counts()
+        m2l = np.zeros(nm2l, np.int64)
+        p2p = np.zeros(np2p, np.int64)
+        self._check(self.lib.fmm_b200_get_lists(self.h, _p(m2l), _p(p2p)))
+        return m2l, p2p
+
+    def timings(self):
+        t = np.zeros(len(PHASES))
+        self._check(self.lib.fmm_b200_get_timings(self.h, _p(t)))
+        return dict(zip(PHASES, t))

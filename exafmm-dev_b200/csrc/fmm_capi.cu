@@ -1,0 +1,507 @@
+// The C ABI (include/exafmm_b200.h): handle lifecycle, stages, whole solves, introspection.
+// Every entry point converts exceptions into status codes; a handle's last failure message
+// stays readable through fmm_b200_last_error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "fmm_solver.cuh"
+
+using namespace fmmb200;
+
+struct fmm_b200_solver {
+  int precision = FMM_FP32;
+  SolverBase* base = nullptr;
+};
+
+static thread_local std::string g_create_error;
+
+namespace fmmb200 {
+
+void phase_begin(SolverBase& s, int ph) {
+  FMM_CUDA(cudaEventRecord(s.ev[2 * ph], s.stream));
+}
+void phase_end(SolverBase& s, int ph) {
+  FMM_CUDA(cudaEventRecord(s.ev[2 * ph + 1], s.stream));
+  s.ev_used[ph] = true;
+}
+
+// double host-side layout (x[3n], q[n]) -> working-precision 4-vectors
+template <typename T>
+__global__ void k_pack(int n, const double* __restrict__ x, const double* __restrict__ q,
+                       vec4<T>* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_v4<T>((T)x[3 * i], (T)x[3 * i + 1], (T)x[3 * i + 2], (T)q[i]);
+}
+template <typename T>
+__global__ void k_unpack(int n, const vec4<T>* __restrict__ in, double* __restrict__ trg4) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    vec4<T> v = in[i];
+    trg4[4 * i] = v.x;
+    trg4[4 * i + 1] = v.y;
+    trg4[4 * i + 2] = v.z;
+    trg4[4 * i + 3] = v.w;
+  }
+}
+template <typename T>
+__global__ void k_unpack_pf(int n, const vec4<T>* __restrict__ in, double* __restrict__ p,
+                            double* __restrict__ f) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    vec4<T> v = in[i];
+    p[i] = v.x;
+    f[3 * i] = v.y;
+    f[3 * i + 1] = v.z;
+    f[3 * i + 2] = v.w;
+  }
+}
+template <typename T>
+__global__ void k_cells_out(int nc, const vec4<T>* __restrict__ cX, double* __restrict__ X,
+                            double* __restrict__ R) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nc) {
+    vec4<T> v = cX[c];
+    X[3 * c] = v.x;
+    X[3 * c + 1] = v.y;
+    X[3 * c + 2] = v.z;
+    R[c] = v.w;
+  }
+}
+template <typename T>
+__global__ void k_to_double(size_t n, const T* __restrict__ in, double* __restrict__ out) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i];
+}
+
+}  // namespace fmmb200
+
+namespace {
+
+template <typename T> Solver<T>& S(fmm_b200_solver* h) { return *static_cast<Solver<T>*>(h->base); }
+
+template <typename F> int guarded(fmm_b200_solver* h, F&& f) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  try {
+    FMM_CUDA(cudaSetDevice(h->base->cfg.device));
+    f();
+    h->base->err.clear();
+    return FMM_OK;
+  } catch (const FmmError& e) {
+    h->base->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->base->err = e.what();
+    return FMM_ERR_INVALID;
+  }
+}
+
+template <typename T> void set_bodies_host_t(Solver<T>& s, int n, const double* x, const double* q,
+                                             DevArr<double>& tmp) {
+  s.n = n;
+  s.bodies_in.ensure(std::max(n, 1));
+  if (n > 0) {
+    tmp.ensure(4 * (size_t)n);
+    FMM_CUDA(cudaMemcpyAsync(tmp.p, x, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, s.stream));
+    FMM_CUDA(cudaMemcpyAsync(tmp.p + 3 * (size_t)n, q, sizeof(double) * n,
+                             cudaMemcpyHostToDevice, s.stream));
+    k_pack<T><<<ceil_div(n, 256), 256, 0, s.stream>>>(n, tmp.p, tmp.p + 3 * (size_t)n,
+                                                      s.bodies_in.p);
+    FMM_LAUNCH_CHECK();
+  }
+  s.stage = ST_BODIES;
+}
+
+template <typename T> void stage_tree(Solver<T>& s) {
+  if (s.stage < ST_BODIES) throw FmmError(FMM_ERR_STATE, "bodies not set");
+  for (int p = 0; p < FMM_NUM_PHASES; p++) s.ev_used[p] = false;
+  phase_begin(s, FMM_PHASE_TOTAL);
+  phase_begin(s, FMM_PHASE_BOUNDS);
+  build_tree(s);
+  if (s.n == 0) phase_end(s, FMM_PHASE_BOUNDS);
+  else phase_end(s, FMM_PHASE_TREE);
+  s.stage = ST_TREE;
+}
+template <typename T> void stage_up(Solver<T>& s) {
+  if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+  phase_begin(s, FMM_PHASE_UPWARD);
+  upward_pass(s);
+  phase_end(s, FMM_PHASE_UPWARD);
+  s.stage = ST_UP;
+}
+template <typename T> void stage_trav(Solver<T>& s) {
+  if (s.stage < ST_UP) throw FmmError(FMM_ERR_STATE, "upward pass not done");
+  phase_begin(s, FMM_PHASE_TRAVERSE);
+  build_lists(s);
+  phase_end(s, FMM_PHASE_TRAVERSE);
+  phase_begin(s, FMM_PHASE_M2L);
+  run_m2l(s);
+  phase_end(s, FMM_PHASE_M2L);
+  phase_begin(s, FMM_PHASE_P2P);
+  s.trg_s.ensure(std::max(s.n, 1));
+  s.trg_e.ensure(std::max(s.n, 1));
+  if (s.n > 0) {
+    FMM_CUDA(cudaMemsetAsync(s.trg_s.p, 0, sizeof(vec4<T>) * s.n, s.stream));
+    FMM_CUDA(cudaMemsetAsync(s.trg_e.p, 0, sizeof(vec4<T>) * s.n, s.stream));
+  }
+  run_p2p(s);
+  phase_end(s, FMM_PHASE_P2P);
+  s.stage = ST_TRAV;
+}
+template <typename T> void stage_down(Solver<T>& s) {
+  if (s.stage < ST_TRAV) throw FmmError(FMM_ERR_STATE, "traversal not done");
+  phase_begin(s, FMM_PHASE_DOWNWARD);
+  downward_pass(s);
+  if (s.n == 0) s.trg_out.ensure(1);
+  phase_end(s, FMM_PHASE_DOWNWARD);
+  phase_end(s, FMM_PHASE_TOTAL);
+  s.stage = ST_DOWN;
+}
+template <typename T> void solve_all(Solver<T>& s) {
+  stage_tree(s);
+  stage_up(s);
+  stage_trav(s);
+  stage_down(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmm_b200_default_config(fmm_b200_config* c) {
+  if (!c) return FMM_ERR_INVALID;
+  c->basis = FMM_SPHERICAL;
+  c->P = 10;
+  c->theta = 0.4;
+  c->ncrit = 64;
+  c->nspawn = 1000;
+  c->use_rmax = 1;
+  c->use_ropt = 1;
+  c->precision = FMM_FP32;
+  c->eps2 = 0.0;
+  c->images = 0;
+  c->device = 0;
+  return FMM_OK;
+}
+
+int fmm_b200_supported_orders(int basis, int* orders, int cap) {
+  std::vector<int> v = basis == FMM_CARTESIAN ? cartesian_orders() : spherical_orders();
+  for (int i = 0; i < (int)v.size() && i < cap; i++) orders[i] = v[i];
+  return (int)v.size();
+}
+
+int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
+  g_create_error.clear();
+  if (!cfg || !out) {
+    g_create_error = "null argument";
+    return FMM_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (cfg->images != 0) {
+    g_create_error = "periodic images are not supported";
+    return FMM_ERR_NOT_SUPPORTED;
+  }
+  if (cfg->basis != FMM_SPHERICAL && cfg->basis != FMM_CARTESIAN) {
+    g_create_error = "unknown basis";
+    return FMM_ERR_INVALID;
+  }
+  std::vector<int> ords = cfg->basis == FMM_CARTESIAN ? cartesian_orders() : spherical_orders();
+  if (std::find(ords.begin(), ords.end(), cfg->P) == ords.end()) {
+    g_create_error = "expansion order P=" + std::to_string(cfg->P) + " not compiled for this basis";
+    return FMM_ERR_INVALID;
+  }
+  if (!(cfg->theta > 0.0 && cfg->theta < 1.0) || cfg->ncrit < 1 || cfg->nspawn < 1 ||
+      (cfg->precision != FMM_FP32 && cfg->precision != FMM_FP64) || !(cfg->eps2 >= 0.0)) {
+    g_create_error = "invalid theta / ncrit / nspawn / precision / eps2";
+    return FMM_ERR_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0) {
+    (void)cudaGetLastError();
+    g_create_error = "no CUDA device " + std::to_string(cfg->device);
+    return FMM_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+    (void)cudaGetLastError();
+    g_create_error = "kernels are built for sm_100a (B200); device is sm_" +
+                     std::to_string(prop.major) + std::to_string(prop.minor);
+    return FMM_ERR_NO_DEVICE;
+  }
+  fmm_b200_solver* h = new fmm_b200_solver();
+  h->precision = cfg->precision;
+  if (cfg->precision == FMM_FP64) h->base = new Solver<double>();
+  else h->base = new Solver<float>();
+  SolverBase& s = *h->base;
+  s.cfg = *cfg;
+  s.nterm = cfg->basis == FMM_SPHERICAL ? nterm_sph(cfg->P) : nterm_cart(cfg->P);
+  s.ncoef = cfg->basis == FMM_SPHERICAL ? 2 * s.nterm : s.nterm;
+  try {
+    FMM_CUDA(cudaSetDevice(cfg->device));
+    s.scal.ensure(64);
+    FMM_CUDA(cudaMallocHost((void**)&s.scal_host, 64 * sizeof(int)));
+    for (int i = 0; i < 2 * FMM_NUM_PHASES; i++) FMM_CUDA(cudaEventCreate(&s.ev[i]));
+  } catch (const FmmError& e) {
+    g_create_error = e.what();
+    delete h->base;
+    delete h;
+    return e.code;
+  }
+  *out = h;
+  return FMM_OK;
+}
+
+#define FMM_RELEASE_ALL(s)                                                                 \
+  do {                                                                                     \
+    DevArr<int>* ia[] = {&s.nbegin,   &s.ncount,   &s.nparent,  &s.nchildn, &s.nfirst,     \
+                         &s.nnode,    &s.npos,     &s.ncb,      &s.nlevel,  &s.nsplit,     \
+                         &s.coff,     &s.leaves,   &s.idx,      &s.idx2,    &s.scal,       \
+                         &s.c_iparent, &s.c_ichild, &s.c_nchild, &s.c_ibody, &s.c_nbody,   \
+                         &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off};               \
+    for (auto* a : ia) a->release();                                                       \
+    s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
+    s.p2p.release(); s.list_tmp.release(); s.p2p_pairs_count.release();                   \
+    s.cub_tmp.release(); s.front.release(); s.front2.release();                           \
+  } while (0)
+
+int fmm_b200_destroy(fmm_b200_solver* h) {
+  if (!h) return FMM_ERR_INVALID;
+  if (h->base) {
+    SolverBase& s = *h->base;
+    cudaSetDevice(s.cfg.device);
+    cudaStreamSynchronize(s.stream);
+    FMM_RELEASE_ALL(s);
+    if (h->precision == FMM_FP64) {
+      Solver<double>& d = *static_cast<Solver<double>*>(h->base);
+      d.bodies_in.release(); d.bodies.release(); d.trg_s.release(); d.trg_e.release();
+      d.trg_out.release(); d.cX.release(); d.box.release(); d.M.release(); d.L.release();
+      d.nX.release(); d.minmax_part.release();
+    } else {
+      Solver<float>& d = *static_cast<Solver<float>*>(h->base);
+      d.bodies_in.release(); d.bodies.release(); d.trg_s.release(); d.trg_e.release();
+      d.trg_out.release(); d.cX.release(); d.box.release(); d.M.release(); d.L.release();
+      d.nX.release(); d.minmax_part.release();
+    }
+    h->base->dtmp.release();
+    for (int i = 0; i < 2 * FMM_NUM_PHASES; i++)
+      if (s.ev[i]) cudaEventDestroy(s.ev[i]);
+    if (s.scal_host) cudaFreeHost(s.scal_host);
+    delete h->base;
+  }
+  delete h;
+  return FMM_OK;
+}
+
+int fmm_b200_set_stream(fmm_b200_solver* h, void* stream) {
+  return guarded(h, [&] { h->base->stream = (cudaStream_t)stream; });
+}
+
+const char* fmm_b200_last_error(const fmm_b200_solver* h) {
+  if (!h || !h->base) return g_create_error.c_str();
+  return h->base->err.c_str();
+}
+
+#define FMM_DISPATCH(h, ...)                                   \
+  guarded(h, [&] {                                             \
+    if (h->precision == FMM_FP64) {                            \
+      using T = double;                                        \
+      Solver<T>& s = S<T>(h);                                  \
+      __VA_ARGS__;                                             \
+    } else {                                                   \
+      using T = float;                                         \
+      Solver<T>& s = S<T>(h);                                  \
+      __VA_ARGS__;                                             \
+    }                                                          \
+  })
+
+int fmm_b200_set_bodies_host(fmm_b200_solver* h, int n, const double* x, const double* q) {
+  if (n < 0 || (n > 0 && (!x || !q))) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, set_bodies_host_t(s, n, x, q, h->base->dtmp));
+}
+
+int fmm_b200_set_bodies_device(fmm_b200_solver* h, int n, const void* d_bodies) {
+  if (n < 0 || (n > 0 && !d_bodies)) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    s.n = n;
+    s.bodies_in.ensure(std::max(n, 1));
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p, d_bodies, sizeof(s.bodies_in.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+    s.stage = ST_BODIES;
+  });
+}
+
+int fmm_b200_build_tree(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_tree(s)); }
+int fmm_b200_upward_pass(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_up(s)); }
+int fmm_b200_traverse(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_trav(s)); }
+int fmm_b200_downward_pass(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_down(s)); }
+
+int fmm_b200_solve_device(fmm_b200_solver* h, int n, const void* d_bodies, void* d_trg) {
+  if (n < 0 || (n > 0 && (!d_bodies || !d_trg))) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    s.n = n;
+    s.bodies_in.ensure(std::max(n, 1));
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p, d_bodies, sizeof(s.bodies_in.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+    s.stage = ST_BODIES;
+    solve_all(s);
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(d_trg, s.trg_out.p, sizeof(s.trg_out.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+  });
+}
+
+int fmm_b200_solve_host(fmm_b200_solver* h, int n, const double* x, const double* q, double* p,
+                        double* f) {
+  if (n < 0 || (n > 0 && (!x || !q || !p || !f))) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    DevArr<double>& tmp = h->base->dtmp;
+    set_bodies_host_t(s, n, x, q, tmp);
+    solve_all(s);
+    if (n > 0) {
+      tmp.ensure(4 * (size_t)n);
+      k_unpack_pf<T><<<ceil_div(n, 256), 256, 0, s.stream>>>(n, s.trg_out.p, tmp.p, tmp.p + n);
+      FMM_LAUNCH_CHECK();
+      FMM_CUDA(cudaMemcpyAsync(p, tmp.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s.stream));
+      FMM_CUDA(cudaMemcpyAsync(f, tmp.p + n, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               s.stream));
+    }
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_trg_host(fmm_b200_solver* h, double* trg) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_DOWN) throw FmmError(FMM_ERR_STATE, "downward pass not done");
+    if (s.n > 0) {
+      DevArr<double>& tmp = h->base->dtmp;
+      tmp.ensure(4 * (size_t)s.n);
+      k_unpack<T><<<ceil_div(s.n, 256), 256, 0, s.stream>>>(s.n, s.trg_out.p, tmp.p);
+      FMM_LAUNCH_CHECK();
+      FMM_CUDA(cudaMemcpyAsync(trg, tmp.p, 4 * sizeof(double) * s.n, cudaMemcpyDeviceToHost,
+                               s.stream));
+    }
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_trg_device(fmm_b200_solver* h, void* d_trg) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_DOWN) throw FmmError(FMM_ERR_STATE, "downward pass not done");
+    if (s.n > 0)
+      FMM_CUDA(cudaMemcpyAsync(d_trg, s.trg_out.p, sizeof(s.trg_out.p[0]) * s.n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+  });
+}
+
+int fmm_b200_num_cells(fmm_b200_solver* h, int* nc, int* ml) {
+  return guarded(h, [&] {
+    if (h->base->stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+    if (nc) *nc = h->base->ncells;
+    if (ml) *ml = h->base->maxlevel;
+  });
+}
+
+int fmm_b200_get_cells(fmm_b200_solver* h, int* iparent, int* ichild, int* nchild, int* ibody,
+                       int* nbody, unsigned long long* icell, int* level, double* X, double* R) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+    const int nc = s.ncells;
+    if (nc == 0) return;
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (dst) FMM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream));
+    };
+    cp(iparent, s.c_iparent.p, 4 * (size_t)nc);
+    cp(ichild, s.c_ichild.p, 4 * (size_t)nc);
+    cp(nchild, s.c_nchild.p, 4 * (size_t)nc);
+    cp(ibody, s.c_ibody.p, 4 * (size_t)nc);
+    cp(nbody, s.c_nbody.p, 4 * (size_t)nc);
+    cp(icell, s.c_icell.p, 8 * (size_t)nc);
+    cp(level, s.c_level.p, 4 * (size_t)nc);
+    if (X || R) {
+      DevArr<double>& tmp = h->base->dtmp;
+      tmp.ensure(4 * (size_t)nc);
+      k_cells_out<T><<<ceil_div(nc, 256), 256, 0, s.stream>>>(nc, s.cX.p, tmp.p, tmp.p + 3 * (size_t)nc);
+      FMM_LAUNCH_CHECK();
+      cp(X, tmp.p, 24 * (size_t)nc);
+      cp(R, tmp.p + 3 * (size_t)nc, 8 * (size_t)nc);
+    }
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_order(fmm_b200_solver* h, int* ibody) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+    if (s.n > 0)
+      FMM_CUDA(cudaMemcpyAsync(ibody, s.order.p, 4 * (size_t)s.n, cudaMemcpyDeviceToHost, s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_box(fmm_b200_solver* h, double* x0r0) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+    DevArr<double>& tmp = h->base->dtmp;
+    tmp.ensure(4);
+    k_to_double<T><<<1, 32, 0, s.stream>>>((size_t)4, s.box.p, tmp.p);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpyAsync(x0r0, tmp.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_expansion(fmm_b200_solver* h, int which, double* out) {
+  return FMM_DISPATCH(h, {
+    if (s.stage < ST_UP) throw FmmError(FMM_ERR_STATE, "upward pass not done");
+    const size_t ne = (size_t)s.ncells * s.ncoef;
+    if (ne == 0) return;
+    DevArr<double>& tmp = h->base->dtmp;
+    tmp.ensure(ne);
+    k_to_double<T><<<ceil_div((long long)ne, 256), 256, 0, s.stream>>>(ne, which ? s.L.p : s.M.p, tmp.p);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpyAsync(out, tmp.p, ne * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_num_lists(fmm_b200_solver* h, long long* nm2l, long long* np2p, long long* bp) {
+  return guarded(h, [&] {
+    if (h->base->stage < ST_TRAV) throw FmmError(FMM_ERR_STATE, "traversal not done");
+    if (nm2l) *nm2l = h->base->nm2l;
+    if (np2p) *np2p = h->base->np2p;
+    if (bp) *bp = h->base->p2p_body_pairs;
+  });
+}
+
+int fmm_b200_get_lists(fmm_b200_solver* h, long long* m2l, long long* p2p) {
+  return guarded(h, [&] {
+    SolverBase& s = *h->base;
+    if (s.stage < ST_TRAV) throw FmmError(FMM_ERR_STATE, "traversal not done");
+    if (m2l && s.nm2l)
+      FMM_CUDA(cudaMemcpyAsync(m2l, s.m2l.p, 8 * (size_t)s.nm2l, cudaMemcpyDeviceToHost, s.stream));
+    if (p2p && s.np2p)
+      FMM_CUDA(cudaMemcpyAsync(p2p, s.p2p.p, 8 * (size_t)s.np2p, cudaMemcpyDeviceToHost, s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_get_timings(fmm_b200_solver* h, double* ms) {
+  return guarded(h, [&] {
+    SolverBase& s = *h->base;
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+    for (int p = 0; p < FMM_NUM_PHASES; p++) {
+      ms[p] = 0;
+      if (!s.ev_used[p]) continue;
+      float t = 0;
+      FMM_CUDA(cudaEventElapsedTime(&t, s.ev[2 * p], s.ev[2 * p + 1]));
+      ms[p] = t;
+    }
+  });
+}
+
+}  // extern "C"

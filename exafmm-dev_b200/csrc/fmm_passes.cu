@@ -1,0 +1,97 @@
+// Level-synchronous upward and downward passes (UpDownPass, include/up_down_pass.h).
+//
+// The reference walks the tree recursively: post-order P2M / M2M with setRmax and
+// R /= theta (:45-84), then SetRopt over every cell (:15-42), and pre-order L2L / L2P
+// (:87-111).  Here each tree level is one launch: P2M over all leaves, M2M from the
+// deepest parent level up to the root, one launch of the error-optimised radius over all
+// cells; after the traversal, L2L from level 1 down and L2P over all leaves.
+#include <algorithm>
+
+#include "fmm_solver.cuh"
+
+namespace fmmb200 {
+
+// SetRopt (include/up_down_pass.h:22-41) with the root coefficient of :125, evaluated in
+// the reference's mix of real_t and double arithmetic.  Multipoles stay unnormalised
+// here (the reference's MASS normalisation M[i] /= M[0] is a change of scale that the
+// M2L / L2L of the MASS build undo again), so only |M[0]| enters.
+template <typename T>
+__global__ void k_ropt(int ncells, vec4<T>* __restrict__ cX, const T* __restrict__ M,
+                       int ncoef, int P, T theta) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const T m0root = fabs(M[0]);
+  const T omt = sub_rn((T)1, theta);
+  const T cc = (T)__ddiv_rn(__ddiv_rn((double)mul_rn(omt, omt), pow((double)theta, (double)(P + 2))),
+                           (double)powf((float)m0root, (float)(1.0 / 3)));
+  T x = (T)__ddiv_rn(1.0, (double)theta);
+  const T m0 = fabs(M[(size_t)c * ncoef]);
+  const T a = mul_rn(cc, (T)powf((float)m0, (float)(1.0 / 3)));
+  for (int i = 0; i < 5; i++) {
+    const T q = add_rn(sub_rn(mul_rn(x, x), mul_rn((T)2, x)), (T)1);
+    const T f = (T)__dsub_rn((double)q, __dmul_rn((double)a, pow((double)x, (double)(-P))));
+    const T df = add_rn(sub_rn(mul_rn((T)(P + 2), x), (T)(2 * (P + 1))), div_rn((T)P, x));
+    x = sub_rn(x, div_rn(f, df));
+  }
+  cX[c].w = mul_rn(cX[c].w, mul_rn(x, theta));
+}
+
+template <typename T>
+__global__ void k_output(int n, const int* __restrict__ order, const vec4<T>* __restrict__ s,
+                         const vec4<T>* __restrict__ e, vec4<T>* __restrict__ out) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  vec4<T> a = s[b], c = e[b];
+  out[order[b]] = make_v4<T>(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+}
+
+template <typename T> static ExpansionOps<T> ops_of(const Solver<T>& s) {
+  ExpansionOps<T> ops;
+  bool ok = s.cfg.basis == FMM_SPHERICAL ? spherical_ops<T>(s.cfg.P, &ops)
+                                         : cartesian_ops<T>(s.cfg.P, &ops);
+  if (!ok) throw FmmError(FMM_ERR_INVALID, "expansion order not compiled");
+  return ops;
+}
+
+template <typename T> void upward_pass(Solver<T>& s) {
+  if (s.ncells == 0) return;
+  ExpansionOps<T> ops = ops_of(s);
+  const size_t ne = (size_t)s.ncells * s.ncoef;
+  s.M.ensure(ne);
+  s.L.ensure(ne);
+  FMM_CUDA(cudaMemsetAsync(s.M.p, 0, ne * sizeof(T), s.stream));
+  FMM_CUDA(cudaMemsetAsync(s.L.p, 0, ne * sizeof(T), s.stream));
+  ops.p2m(s);
+  for (int l = s.maxlevel - 1; l >= 0; l--) ops.m2m_level(s, s.level_lo[l], s.level_lo[l + 1]);
+  if (s.cfg.use_ropt) {
+    k_ropt<T><<<ceil_div(s.ncells, 256), 256, 0, s.stream>>>(s.ncells, s.cX.p, s.M.p, s.ncoef,
+                                                            s.cfg.P, (T)s.cfg.theta);
+    FMM_LAUNCH_CHECK();
+  }
+}
+
+template <typename T> void run_m2l(Solver<T>& s) {
+  if (s.ncells == 0 || s.nm2l == 0) return;
+  ExpansionOps<T> ops = ops_of(s);
+  ops.m2l(s);
+}
+
+template <typename T> void downward_pass(Solver<T>& s) {
+  if (s.ncells == 0) return;
+  ExpansionOps<T> ops = ops_of(s);
+  for (int l = 1; l <= s.maxlevel; l++) ops.l2l_level(s, s.level_lo[l], s.level_lo[l + 1]);
+  ops.l2p(s);
+  s.trg_out.ensure(s.n);
+  k_output<T><<<ceil_div(s.n, 256), 256, 0, s.stream>>>(s.n, s.order.p, s.trg_s.p, s.trg_e.p,
+                                                        s.trg_out.p);
+  FMM_LAUNCH_CHECK();
+}
+
+template void upward_pass<float>(Solver<float>&);
+template void upward_pass<double>(Solver<double>&);
+template void run_m2l<float>(Solver<float>&);
+template void run_m2l<double>(Solver<double>&);
+template void downward_pass<float>(Solver<float>&);
+template void downward_pass<double>(Solver<double>&);
+
+}  // namespace fmmb200

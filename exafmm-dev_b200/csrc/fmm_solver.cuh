@@ -1,0 +1,128 @@
+// Per-handle solver state and the stage entry points each translation unit implements.
+//
+// HBM layout of one solve (T = float or double, N bodies, C cells):
+//   bodies_in   vec4<T>[N]   caller order (x, y, z, q)
+//   bodies      vec4<T>[N]   tree order (the reference's permuted Bodies)
+//   order       int[N]       original index of each tree-order body (Body::IBODY)
+//   trg_s/trg_e vec4<T>[N]   potential + gradient, compensated sum and its error term
+//   cells       SoA over C:  iparent, ichild, nchild, ibody, nbody, level (int),
+//                            icell (u64), X = (x, y, z, R) vec4<T>
+//   M, L        T[C * ncoef] expansions, ncoef = 2 * NTERM (spherical) or NTERM
+//   m2l, p2p    u64 pairs (target << 32 | source) sorted by target, + CSR offsets[C + 1]
+// Tree nodes are built breadth first (level by level) and each node knows its cell slot,
+// so level-synchronous passes walk node ranges and write cells in the reference layout.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fmm_common.cuh"
+
+namespace fmmb200 {
+
+template <typename U> struct DevArr {
+  U* p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t n) {
+    if (n <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = n + n / 4 + 256;
+    cudaError_t e = cudaMalloc((void**)&p, want * sizeof(U));
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw FmmError(FMM_ERR_NO_MEMORY, "cudaMalloc of " + std::to_string(want * sizeof(U)) +
+                                            " bytes failed: " + cudaGetErrorString(e));
+    }
+    cap = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+enum Stage { ST_NONE = 0, ST_BODIES = 1, ST_TREE = 2, ST_UP = 3, ST_TRAV = 4, ST_DOWN = 5 };
+
+struct SolverBase {
+  fmm_b200_config cfg;
+  cudaStream_t stream = nullptr;
+  int n = 0;
+  int ncoef = 0, nterm = 0;
+  Stage stage = ST_NONE;
+  std::string err;
+  // tree shape (host copies of the few scalars the level loops need)
+  int ncells = 0, maxlevel = 0, nleaves = 0;
+  std::vector<int> level_lo;  // node index range of level l: [level_lo[l], level_lo[l+1])
+  long long nm2l = 0, np2p = 0, p2p_body_pairs = 0;
+  // node arrays (breadth-first)
+  DevArr<int> nbegin, ncount, nparent, nchildn, nfirst, nnode, npos, ncb, nlevel, nsplit;
+  DevArr<int> coff;
+  DevArr<int> leaves;  // cell index of every leaf
+  // sort scratch
+  DevArr<unsigned long long> keys, keys2;
+  DevArr<int> idx, idx2;
+  DevArr<char> cub_tmp;
+  DevArr<int> scal;          // small device scalars (counters, flags)
+  int* scal_host = nullptr;  // pinned mirror of scal
+  // cells
+  DevArr<int> c_iparent, c_ichild, c_nchild, c_ibody, c_nbody, c_level;
+  DevArr<unsigned long long> c_icell;
+  DevArr<int> order;
+  // interaction lists
+  DevArr<int2> front, front2;
+  DevArr<unsigned long long> m2l, p2p, list_tmp;
+  DevArr<int> m2l_off, p2p_off;
+  DevArr<unsigned long long> p2p_pairs_count;
+  DevArr<double> dtmp;  // host <-> device conversion scratch
+  // phase timing
+  cudaEvent_t ev[2 * FMM_NUM_PHASES] = {};
+  bool ev_used[FMM_NUM_PHASES] = {};
+  virtual ~SolverBase() {}
+};
+
+template <typename T> struct Solver : SolverBase {
+  DevArr<vec4<T>> bodies_in, bodies, trg_s, trg_e, trg_out, cX;
+  DevArr<T> box;  // X0[3], R0, Xmin[3], Xmax[3]
+  DevArr<T> M, L, nX;
+  DevArr<T> minmax_part;
+};
+
+// ---- stage implementations (one translation unit each) ---------------------------------
+template <typename T> void build_tree(Solver<T>& s);          // fmm_tree.cu
+template <typename T> void upward_pass(Solver<T>& s);         // fmm_passes.cu
+template <typename T> void downward_pass(Solver<T>& s);       // fmm_passes.cu
+template <typename T> void build_lists(Solver<T>& s);         // fmm_traverse.cu
+template <typename T> void run_m2l(Solver<T>& s);             // fmm_passes.cu
+template <typename T> void run_p2p(Solver<T>& s);             // fmm_p2p.cu
+
+// dispatch of the P-templated expansion kernels (fmm_spherical.cu, fmm_cartesian.cu)
+template <typename T> struct ExpansionOps {
+  // leaves: list of leaf cells; level cells given by node range + npos
+  void (*p2m)(Solver<T>& s);
+  void (*m2m_level)(Solver<T>& s, int lo, int hi);
+  void (*m2l)(Solver<T>& s);
+  void (*l2l_level)(Solver<T>& s, int lo, int hi);
+  void (*l2p)(Solver<T>& s);
+};
+template <typename T> bool spherical_ops(int P, ExpansionOps<T>* ops);
+template <typename T> bool cartesian_ops(int P, ExpansionOps<T>* ops);
+std::vector<int> spherical_orders();
+std::vector<int> cartesian_orders();
+
+// phase timing helpers (fmm_capi.cu)
+void phase_begin(SolverBase& s, int phase);
+void phase_end(SolverBase& s, int phase);
+
+// CUB wrappers compiled once (fmm_sort.cu)
+void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
+                    const int* vin, int* vout, int n, int end_bit);
+void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
+                   int n, int end_bit);
+void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n);
+void sum_u64(SolverBase& s, const unsigned long long* in, unsigned long long* out, int n);
+
+}  // namespace fmmb200

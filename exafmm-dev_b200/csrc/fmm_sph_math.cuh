@@ -1,0 +1,335 @@
+// Spherical-harmonic translation operators of the Laplace FMM, P known at compile time.
+//
+// Restates kernels/LaplaceSphericalCPU.cxx (evalMultipole :29-65, evalLocal :68-101,
+// P2M :103-118, M2M :120-147, M2L :149-191, L2L :193-224, L2P :226-256) for the device:
+//   * angles come straight from the Cartesian offset: cos(alpha) = dz / r,
+//     sin(alpha) = |(dx, dy)| / r, e^(i beta) = (dx + i dy) / |(dx, dy)|, in place of the
+//     reference's acos / atan2 / cos / sin round trip (same values up to rounding);
+//   * harmonics are stored for m >= 0 only, Y[n, -m] = conj(Y[n, m]) (the reference keeps
+//     both halves, :41-42), at index n (n + 1) / 2 + m, the layout of the expansions;
+//   * the M2L sum over m < 0 and m >= 0 is folded into per-(n, |m|) terms with the signs
+//     of :158-185 resolved at compile time.
+// Every function is __host__ __device__ so the CPU tests run the exact device arithmetic.
+#pragma once
+#include <cmath>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+namespace fmmb200 {
+namespace sph {
+
+__host__ __device__ constexpr int NT(int P) { return P * (P + 1) / 2; }
+__host__ __device__ constexpr int sidx(int n, int m) { return n * (n + 1) / 2 + m; }
+
+template <typename T> struct Angles {
+  T r, x, y, cb, sb;  // |dX|, cos(alpha), sin(alpha), cos(beta), sin(beta)
+};
+
+template <typename T> __host__ __device__ __forceinline__ T hsqrt(T v) { return std::sqrt(v); }
+
+// cart2sph (:9-13): alpha = acos(dz / r) (0 when r = 0), beta = atan2(dy, dx)
+template <typename T> __host__ __device__ __forceinline__ Angles<T> angles(T dx, T dy, T dz) {
+  Angles<T> a;
+  T rxy2 = dx * dx + dy * dy;
+  a.r = hsqrt(rxy2 + dz * dz);
+  T rxy = hsqrt(rxy2);
+  if (a.r > T(0)) {
+    T inv = T(1) / a.r;
+    a.x = dz * inv;
+    a.y = rxy * inv;
+  } else {
+    a.x = T(1);
+    a.y = T(0);
+  }
+  if (rxy > T(0)) {
+    T inv = T(1) / rxy;
+    a.cb = dx * inv;
+    a.sb = dy * inv;
+  } else {
+    a.cb = dx < T(0) ? T(-1) : T(1);  // atan2(+-0, x) = 0 or pi
+    a.sb = T(0);
+  }
+  return a;
+}
+
+// evalMultipole (:29-65) without the theta derivative: Y[n, m] = rho^n P_n^m e^(i m beta)
+// / (-1)^n (n + m)!-style normalisation of the reference.
+template <typename T, int P>
+__host__ __device__ __forceinline__ void multipole(const Angles<T>& a, T rho, T* yr, T* yi) {
+  T fact = 1, pn = 1, rhom = 1;
+  T er = 1, ei = 0;
+#pragma unroll
+  for (int m = 0; m < P; m++) {
+    T p = pn;
+    yr[sidx(m, m)] = rhom * p * er;
+    yi[sidx(m, m)] = rhom * p * ei;
+    T p1 = p;
+    p = a.x * (2 * m + 1) * p1;
+    rhom *= rho;
+    T rhon = rhom;
+#pragma unroll
+    for (int n = m + 1; n < P; n++) {
+      rhon /= -(n + m);
+      yr[sidx(n, m)] = rhon * p * er;
+      yi[sidx(n, m)] = rhon * p * ei;
+      T p2 = p1;
+      p1 = p;
+      p = (a.x * (2 * n + 1) * p1 - (n + m) * p2) * (T(1) / T(n - m + 1));
+      rhon *= rho;
+    }
+    rhom /= -(2 * m + 2) * (2 * m + 1);
+    pn = -pn * fact * a.y;
+    fact += 2;
+    T t = er * a.cb - ei * a.sb;
+    ei = er * a.sb + ei * a.cb;
+    er = t;
+  }
+}
+
+// evalLocal (:68-101): singular harmonics rho^(-n-1) P_n^m e^(i m beta) (n - m)!-scaled
+template <typename T, int P>
+__host__ __device__ __forceinline__ void local(const Angles<T>& a, T* yr, T* yi) {
+  T fact = 1, pn = 1;
+  T invR = -T(1) / a.r;
+  T rhom = -invR;
+  T er = 1, ei = 0;
+#pragma unroll
+  for (int m = 0; m < P; m++) {
+    T p = pn;
+    yr[sidx(m, m)] = rhom * p * er;
+    yi[sidx(m, m)] = rhom * p * ei;
+    T p1 = p;
+    p = a.x * (2 * m + 1) * p1;
+    rhom *= invR;
+    T rhon = rhom;
+#pragma unroll
+    for (int n = m + 1; n < P; n++) {
+      yr[sidx(n, m)] = rhon * p * er;
+      yi[sidx(n, m)] = rhon * p * ei;
+      T p2 = p1;
+      p1 = p;
+      p = (a.x * (2 * n + 1) * p1 - (n + m) * p2) * (T(1) / T(n - m + 1));
+      rhon *= invR * (n - m + 1);
+    }
+    pn = -pn * fact * a.y;
+    fact += 2;
+    T t = er * a.cb - ei * a.sb;
+    ei = er * a.sb + ei * a.cb;
+    er = t;
+  }
+}
+
+// M2L of one source multipole into a register local expansion (:149-191, mutual = false,
+// unnormalised multipoles).  Mj holds NT (re, im) pairs.
+template <typename T, int P>
+__host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, const T* Mj, T* Lr,
+                                                  T* Li) {
+#pragma unroll
+  for (int n = 0; n < P; n++) {
+#pragma unroll
+    for (int mu = 0; mu <= n; mu++) {
+      const T mr = Mj[2 * sidx(n, mu)], mi = Mj[2 * sidx(n, mu) + 1];
+#pragma unroll
+      for (int j = 0; j < P - n; j++) {
+        const int a = j + n;
+#pragma unroll
+        for (int k = 0; k <= j; k++) {
+          const int t = sidx(j, k);
+          T re, im;
+          if (mu == 0) {
+            // M[n,0] conj(Y[a,k])
+            const T ur = yr[sidx(a, k)], ui = yi[sidx(a, k)];
+            re = mr * ur + mi * ui;
+            im = mi * ur - mr * ui;
+          } else {
+            // m = -mu: conj(M[n,mu] Y[a, k+mu])
+            const T ur = yr[sidx(a, k + mu)], ui = yi[sidx(a, k + mu)];
+            re = mr * ur - mi * ui;
+            im = -(mr * ui + mi * ur);
+            // m = +mu: (-1)^(k < mu ? k : mu) M[n,mu] Y[a, mu-k]
+            const bool neg = ((k < mu ? k : mu) & 1) != 0;
+            T vr, vi;
+            if (mu >= k) {
+              const T wr = yr[sidx(a, mu - k)], wi = yi[sidx(a, mu - k)];
+              vr = mr * wr - mi * wi;
+              vi = mr * wi + mi * wr;
+            } else {
+              const T wr = yr[sidx(a, k - mu)], wi = yi[sidx(a, k - mu)];
+              vr = mr * wr + mi * wi;
+              vi = mi * wr - mr * wi;
+            }
+            if (neg) {
+              re -= vr;
+              im -= vi;
+            } else {
+              re += vr;
+              im += vi;
+            }
+          }
+          if (j & 1) {
+            Lr[t] -= re;
+            Li[t] -= im;
+          } else {
+            Lr[t] += re;
+            Li[t] += im;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Y[a, b] for any sign of b from an interleaved (re, im) m >= 0 store
+template <typename T>
+__host__ __device__ __forceinline__ void yget(const T* y, int a, int b, T& r, T& i) {
+  if (b >= 0) {
+    r = y[2 * sidx(a, b)];
+    i = y[2 * sidx(a, b) + 1];
+  } else {
+    r = y[2 * sidx(a, -b)];
+    i = -y[2 * sidx(a, -b) + 1];
+  }
+}
+
+// M2M output coefficient (j, k) from one child (:127-144); Y from multipole() at
+// Xparent - Xchild as interleaved (re, im) pairs, Mc the child's NT (re, im) pairs.
+// Runtime indices (shared memory).
+template <typename T>
+__host__ __device__ __forceinline__ void m2m_term(int j, int k, const T* y, const T* Mc,
+                                                  T& outr, T& outi) {
+  T sr = 0, si = 0;
+  for (int n = 0; n <= j; n++) {
+    int mlo = -n > -j + k + n ? -n : -j + k + n;
+    int mhi = k - 1 < n ? k - 1 : n;
+    for (int m = mlo; m <= mhi; m++) {
+      // Cj->M[(j-n)(j-n+1)/2 + k - m] * Ynm[n*n+n-m] * IPOW2N(m) * ODDEVEN(n)
+      int q = (j - n) * (j - n + 1) / 2 + k - m;
+      T Mr = Mc[2 * q], Mi = Mc[2 * q + 1];
+      T ur, ui;
+      yget(y, n, -m, ur, ui);
+      T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
+      int sgn = ((m < 0 && (m & 1)) ? -1 : 1) * ((n & 1) ? -1 : 1);
+      sr += sgn * pr;
+      si += sgn * pi;
+    }
+    int mhi2 = n < j + k - n ? n : j + k - n;
+    for (int m = k; m <= mhi2; m++) {
+      // conj(Cj->M[(j-n)(j-n+1)/2 - k + m]) * Ynm[n*n+n-m] * ODDEVEN(k+n+m)
+      int q = (j - n) * (j - n + 1) / 2 - k + m;
+      T Mr = Mc[2 * q], Mi = -Mc[2 * q + 1];
+      T ur, ui;
+      yget(y, n, -m, ur, ui);
+      T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
+      int sgn = ((k + n + m) & 1) ? -1 : 1;
+      sr += sgn * pr;
+      si += sgn * pi;
+    }
+  }
+  outr = sr;
+  outi = si;
+}
+
+// L2L output coefficient (j, k) from the parent (:203-222); Y from multipole() at
+// Xchild - Xparent as interleaved (re, im) pairs, Lp the parent's NT (re, im) pairs.
+template <typename T>
+__host__ __device__ __forceinline__ void l2l_term(int P, int j, int k, const T* y,
+                                                  const T* Lp, T& outr, T& outi) {
+  T sr = 0, si = 0;
+  for (int n = j; n < P; n++) {
+    for (int m = j + k - n; m < 0; m++) {
+      // conj(Cj->L[n(n+1)/2 - m]) * Ynm[(n-j)^2 + n-j + m-k] * ODDEVEN(k)
+      int q = n * (n + 1) / 2 - m;
+      T Lr = Lp[2 * q], Li = -Lp[2 * q + 1];
+      T ur, ui;
+      yget(y, n - j, m - k, ur, ui);
+      T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
+      int sgn = (k & 1) ? -1 : 1;
+      sr += sgn * pr;
+      si += sgn * pi;
+    }
+    for (int m = 0; m <= n; m++) {
+      int d = m - k;
+      if (n - j >= (d < 0 ? -d : d)) {
+        // Cj->L[n(n+1)/2 + m] * Ynm[(n-j)^2 + n-j + m-k] * ODDEVEN((m-k)(m<k))
+        int q = n * (n + 1) / 2 + m;
+        T Lr = Lp[2 * q], Li = Lp[2 * q + 1];
+        T ur, ui;
+        yget(y, n - j, d, ur, ui);
+        T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
+        int sgn = (d < 0 && (d & 1)) ? -1 : 1;
+        sr += sgn * pr;
+        si += sgn * pi;
+      }
+    }
+  }
+  outr = sr;
+  outi = si;
+}
+
+// L2P of one body (:226-256): potential and gradient of the local expansion L (NT (re, im)
+// pairs) at offset dX from the cell centre.  Harmonics and their theta derivatives are
+// generated column by column and consumed on the fly.
+template <typename T, int P>
+__host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, T& pot, T& gx,
+                                                  T& gy, T& gz) {
+  Angles<T> a = angles(dx, dy, dz);
+  const T rho = a.r;
+  T s0 = 0, s1 = 0, s2 = 0, ph = 0;
+  T fact = 1, pn = 1, rhom = 1;
+  T er = 1, ei = 0;
+  const T invy = T(1) / a.y;
+#pragma unroll
+  for (int m = 0; m < P; m++) {
+    const T w = m == 0 ? T(1) : T(2);
+    T p = pn;
+    T p1 = p;
+    p = a.x * (2 * m + 1) * p1;
+    {
+      // Y[m,m] and its theta derivative
+      const T yv = rhom * p1;
+      const T tv = rhom * (p - (m + 1) * a.x * p1) * invy;
+      const T Lr = L[2 * sidx(m, m)], Li = L[2 * sidx(m, m) + 1];
+      const T re = Lr * er - Li * ei, im = Lr * ei + Li * er;  // L * e^(i m beta)
+      ph += w * yv * re;
+      s0 += w * yv * re / rho * m;
+      s1 += w * tv * re;
+      s2 -= w * yv * im * m;
+    }
+    rhom *= rho;
+    T rhon = rhom;
+#pragma unroll
+    for (int n = m + 1; n < P; n++) {
+      rhon /= -(n + m);
+      const T yv = rhon * p;
+      T p2 = p1;
+      p1 = p;
+      p = (a.x * (2 * n + 1) * p1 - (n + m) * p2) * (T(1) / T(n - m + 1));
+      const T tv = rhon * ((n - m + 1) * p - (n + 1) * a.x * p1) * invy;
+      const T Lr = L[2 * sidx(n, m)], Li = L[2 * sidx(n, m) + 1];
+      const T re = Lr * er - Li * ei, im = Lr * ei + Li * er;
+      ph += w * yv * re;
+      s0 += w * yv * re / rho * n;
+      s1 += w * tv * re;
+      s2 -= w * yv * im * m;
+      rhon *= rho;
+    }
+    rhom /= -(2 * m + 2) * (2 * m + 1);
+    pn = -pn * fact * a.y;
+    fact += 2;
+    T t = er * a.cb - ei * a.sb;
+    ei = er * a.sb + ei * a.cb;
+    er = t;
+  }
+  // sph2cart (:17-26)
+  pot = ph;
+  gx = a.y * a.cb * s0 + a.x * a.cb / rho * s1 - a.sb / rho * invy * s2;
+  gy = a.y * a.sb * s0 + a.x * a.sb / rho * s1 + a.cb / rho * invy * s2;
+  gz = a.x * s0 - a.y / rho * s1;
+}
+
+}  // namespace sph
+}  // namespace fmmb200

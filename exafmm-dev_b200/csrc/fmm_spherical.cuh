@@ -1,0 +1,440 @@
+// Spherical-basis expansion kernels (P2M, M2M, M2L, L2L, L2P) for compile-time P.
+//
+// Warp mappings:
+//   P2M  warp per leaf, lane per body; each lane's q conj(Y) row goes to shared memory and
+//        the warp sums columns in body order, so M[0] is the reference's sequential sum.
+//   M2M  warp per parent, lane per output coefficient, children in order (reference order
+//        of Ci->M += ..., include/up_down_pass.h:79-80 / LaplaceSphericalCPU.cxx:143).
+//   M2L  FP32: warp per target cell, lane per source cell, harmonics and the local
+//        expansion held in registers, one warp reduction per target.  FP64: warp per
+//        target, lanes over output coefficients (harmonics in shared memory).
+//   L2L  warp per cell, lane per output coefficient.
+//   L2P  warp per leaf, lane per body, harmonics generated and consumed on the fly.
+// setRmax / R /= theta (include/up_down_pass.h:51-67, :81-82) are fused into P2M and M2M.
+#pragma once
+#include <algorithm>
+
+#include "fmm_solver.cuh"
+#include "fmm_sph_math.cuh"
+
+namespace fmmb200 {
+
+template <typename T> struct SphCfg {
+  static constexpr int W = sizeof(T) == 4 ? 4 : 2;  // warps per block
+};
+// P2M keeps one row of 2 NT (+1 pad) values per lane in shared memory: as many warps per
+// block as fit in 40 KB of static shared memory.
+template <typename T, int P> struct P2MCfg {
+  static constexpr int RS = (2 * sph::NT(P)) | 1;
+  static constexpr int BYTES = 32 * RS * (int)sizeof(T);
+  static constexpr int W = 40960 / BYTES >= 4 ? 4 : (40960 / BYTES >= 2 ? 2 : 1);
+};
+
+// ---------------------------------------------------------------- P2M (+ setRmax)
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * P2MCfg<T, P>::W)
+    k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
+          const int* __restrict__ nbody, vec4<T>* __restrict__ cX,
+          const vec4<T>* __restrict__ bodies, T* __restrict__ M, int ncoef, int use_rmax,
+          T theta) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, RS = NC | 1, KA = (NC + 31) / 32;
+  constexpr int W = P2MCfg<T, P>::W;
+  __shared__ T rows[W][32 * RS];
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int w = blockIdx.x * W + wl;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int b0 = ibody[c], nb = nbody[c];
+  const vec4<T> C = cX[c];
+  T acc[KA];
+#pragma unroll
+  for (int i = 0; i < KA; i++) acc[i] = 0;
+  T rmax = 0;
+  for (int base = 0; base < nb; base += 32) {
+    const int cnt = min(32, nb - base);
+    __syncwarp();
+    if (lane < cnt) {
+      const vec4<T> b = bodies[b0 + base + lane];
+      const T dx = b.x - C.x, dy = b.y - C.y, dz = b.z - C.z;
+      T yr[NT], yi[NT];
+      sph::Angles<T> a = sph::angles(dx, dy, dz);
+      sph::multipole<T, P>(a, a.r, yr, yi);
+      T* row = &rows[wl][lane * RS];
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        row[2 * t] = b.w * yr[t];
+        row[2 * t + 1] = -(b.w * yi[t]);
+      }
+      const T r = sqrt_rn(norm_rn(sub_rn(C.x, b.x), sub_rn(C.y, b.y), sub_rn(C.z, b.z)));
+      rmax = r > rmax ? r : rmax;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KA; i++) {
+      const int t = lane + 32 * i;
+      if (t < NC)
+        for (int r = 0; r < cnt; r++) acc[i] += rows[wl][r * RS + t];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KA; i++) {
+    const int t = lane + 32 * i;
+    if (t < NC) M[(size_t)c * ncoef + t] = acc[i];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T v = __shfl_xor_sync(0xffffffffu, rmax, o);
+    rmax = v > rmax ? v : rmax;
+  }
+  if (lane == 0) {
+    T R = C.w;
+    if (use_rmax) R = rmax < R ? rmax : R;
+    cX[c].w = div_rn(R, theta);
+  }
+}
+
+// write the register harmonics of one lane's pair into shared memory, entry t by lane t%32
+template <typename T, int NT>
+__device__ __forceinline__ void spread_y(const T* yr, const T* yi, T* sy, int lane) {
+#pragma unroll
+  for (int t = 0; t < NT; t++)
+    if ((t & 31) == lane) {
+      sy[2 * t] = yr[t];
+      sy[2 * t + 1] = yi[t];
+    }
+}
+
+__device__ __forceinline__ void jk_of(int t, int& j, int& k) {
+  j = 0;
+  while ((j + 1) * (j + 2) / 2 <= t) j++;
+  k = t - j * (j + 1) / 2;
+}
+
+// ---------------------------------------------------------------- M2M (+ setRmax)
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * SphCfg<T>::W)
+    k_m2m(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
+          const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
+          int ncoef, int use_rmax, T theta) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
+  constexpr int W = SphCfg<T>::W;
+  __shared__ T sy[W][NC], sm[W][NC];
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int v = lo + blockIdx.x * W + wl;
+  if (v >= hi) return;
+  const int c = npos[v];
+  const int nch = nchild[c];
+  if (nch == 0) return;
+  const int c0 = ichild[c];
+  const vec4<T> Xp = cX[c];
+  T ar[KO], ai[KO];
+  int oj[KO], ok[KO];
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    ar[i] = ai[i] = 0;
+    jk_of(lane + 32 * i, oj[i], ok[i]);
+  }
+  T rmax = 0;
+  for (int ch = 0; ch < nch; ch++) {
+    const int cc = c0 + ch;
+    const vec4<T> Xc = cX[cc];
+    {
+      T yr[NT], yi[NT];
+      sph::Angles<T> a = sph::angles(Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
+      sph::multipole<T, P>(a, a.r, yr, yi);
+      __syncwarp();
+      spread_y<T, NT>(yr, yi, sy[wl], lane);
+      for (int t = lane; t < NC; t += 32) sm[wl][t] = M[(size_t)cc * ncoef + t];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KO; i++) {
+      if (lane + 32 * i < NT) {
+        T r, im;
+        sph::m2m_term<T>(oj[i], ok[i], sy[wl], sm[wl], r, im);
+        ar[i] += r;
+        ai[i] += im;
+      }
+    }
+    if (lane == ch) {
+      const T d = sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z)));
+      rmax = add_rn(d, Xc.w);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    const int t = lane + 32 * i;
+    if (t < NT) {
+      M[(size_t)c * ncoef + 2 * t] = ar[i];
+      M[(size_t)c * ncoef + 2 * t + 1] = ai[i];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T x = __shfl_xor_sync(0xffffffffu, rmax, o);
+    rmax = x > rmax ? x : rmax;
+  }
+  if (lane == 0) {
+    T R = Xp.w;
+    if (use_rmax) R = rmax < R ? rmax : R;
+    cX[c].w = div_rn(R, theta);
+  }
+}
+
+// ---------------------------------------------------------------- M2L
+// FP32: lane per source, Y and L in registers.
+template <typename T, int P>
+__global__ void __launch_bounds__(128)
+    k_m2l_reg(int ncells, const int* __restrict__ off, const unsigned long long* __restrict__ pairs,
+              const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L,
+              int ncoef) {
+  constexpr int NT = sph::NT(P);
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = lane_id();
+  if (c >= ncells) return;
+  const int s0 = off[c], s1 = off[c + 1];
+  if (s0 == s1) return;
+  const vec4<T> Xi = cX[c];
+  T Lr[NT], Li[NT];
+#pragma unroll
+  for (int t = 0; t < NT; t++) Lr[t] = Li[t] = 0;
+  for (int s = s0 + lane; s < s1; s += 32) {
+    const int j = (int)(pairs[s] & 0xffffffffULL);
+    const vec4<T> Xj = cX[j];
+    T yr[NT], yi[NT];
+    sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
+    sph::local<T, P>(a, yr, yi);
+    sph::m2l_pair<T, P>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
+  }
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    const T r = warp_sum(Lr[t]);
+    const T i = warp_sum(Li[t]);
+    if (lane == (t & 31)) {
+      L[(size_t)c * ncoef + 2 * t] += r;
+      L[(size_t)c * ncoef + 2 * t + 1] += i;
+    }
+  }
+}
+
+// M2L output coefficient (j, k) from one source (:156-189), runtime indices
+template <typename T>
+__device__ __forceinline__ void m2l_term(int P, int j, int k, const T* y, const T* Mj, T& outr,
+                                         T& outi) {
+  T sr = 0, si = 0;
+  for (int n = 0; n < P - j; n++) {
+    const int a = j + n;
+    for (int mu = 1; mu <= n; mu++) {
+      const T mr = Mj[2 * sph::sidx(n, mu)], mi = Mj[2 * sph::sidx(n, mu) + 1];
+      const T ur = y[2 * sph::sidx(a, k + mu)], ui = y[2 * sph::sidx(a, k + mu) + 1];
+      sr += mr * ur - mi * ui;
+      si -= mr * ui + mi * ur;
+    }
+    for (int m = 0; m <= n; m++) {
+      const T mr = Mj[2 * sph::sidx(n, m)], mi = Mj[2 * sph::sidx(n, m) + 1];
+      T vr, vi;
+      if (m >= k) {
+        const T wr = y[2 * sph::sidx(a, m - k)], wi = y[2 * sph::sidx(a, m - k) + 1];
+        vr = mr * wr - mi * wi;
+        vi = mr * wi + mi * wr;
+      } else {
+        const T wr = y[2 * sph::sidx(a, k - m)], wi = y[2 * sph::sidx(a, k - m) + 1];
+        vr = mr * wr + mi * wi;
+        vi = mi * wr - mr * wi;
+      }
+      if ((k < m ? k : m) & 1) {
+        sr -= vr;
+        si -= vi;
+      } else {
+        sr += vr;
+        si += vi;
+      }
+    }
+  }
+  if (j & 1) {
+    sr = -sr;
+    si = -si;
+  }
+  outr = sr;
+  outi = si;
+}
+
+// FP64: lanes over output coefficients; outputs dealt so heavy (low j) and light (high j)
+// coefficients pair up on a lane.
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * SphCfg<T>::W)
+    k_m2l_lanes(int ncells, const int* __restrict__ off,
+                const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
+                const T* __restrict__ M, T* __restrict__ L, int ncoef) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
+  constexpr int W = SphCfg<T>::W;
+  __shared__ T sy[W][NC], sm[W][NC];
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int c = blockIdx.x * W + wl;
+  if (c >= ncells) return;
+  const int s0 = off[c], s1 = off[c + 1];
+  if (s0 == s1) return;
+  const vec4<T> Xi = cX[c];
+  T ar[KO], ai[KO];
+  int ot[KO], oj[KO], ok[KO];
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    ar[i] = ai[i] = 0;
+    const int cnt = NT - 32 * i < 32 ? NT - 32 * i : 32;  // outputs in block i
+    ot[i] = (i & 1) ? (lane < cnt ? 32 * i + cnt - 1 - lane : NT) : lane + 32 * i;
+    jk_of(ot[i] < NT ? ot[i] : 0, oj[i], ok[i]);
+  }
+  for (int s = s0; s < s1; s++) {
+    const int j = (int)(pairs[s] & 0xffffffffULL);
+    const vec4<T> Xj = cX[j];
+    {
+      T yr[NT], yi[NT];
+      sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
+      sph::local<T, P>(a, yr, yi);
+      __syncwarp();
+      spread_y<T, NT>(yr, yi, sy[wl], lane);
+      for (int t = lane; t < NC; t += 32) sm[wl][t] = M[(size_t)j * ncoef + t];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KO; i++) {
+      if (ot[i] < NT) {
+        T r, im;
+        m2l_term<T>(P, oj[i], ok[i], sy[wl], sm[wl], r, im);
+        ar[i] += r;
+        ai[i] += im;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    if (ot[i] < NT) {
+      L[(size_t)c * ncoef + 2 * ot[i]] += ar[i];
+      L[(size_t)c * ncoef + 2 * ot[i] + 1] += ai[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- L2L
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * SphCfg<T>::W)
+    k_l2l(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
+          const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
+  constexpr int W = SphCfg<T>::W;
+  __shared__ T sy[W][NC], sl[W][NC];
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int v = lo + blockIdx.x * W + wl;
+  if (v >= hi) return;
+  const int c = npos[v];
+  const int p = iparent[c];
+  const vec4<T> Xc = cX[c], Xp = cX[p];
+  {
+    T yr[NT], yi[NT];
+    sph::Angles<T> a = sph::angles(Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
+    sph::multipole<T, P>(a, a.r, yr, yi);
+    spread_y<T, NT>(yr, yi, sy[wl], lane);
+    for (int t = lane; t < NC; t += 32) sl[wl][t] = L[(size_t)p * ncoef + t];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    const int t = lane + 32 * i;
+    if (t < NT) {
+      int j, k;
+      jk_of(t, j, k);
+      T r, im;
+      sph::l2l_term<T>(P, j, k, sy[wl], sl[wl], r, im);
+      L[(size_t)c * ncoef + 2 * t] += r;
+      L[(size_t)c * ncoef + 2 * t + 1] += im;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- L2P
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * SphCfg<T>::W)
+    k_l2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
+          const int* __restrict__ nbody, const vec4<T>* __restrict__ cX,
+          const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
+          vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT;
+  constexpr int W = SphCfg<T>::W;
+  __shared__ T sl[W][NC];
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int w = blockIdx.x * W + wl;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int b0 = ibody[c], nb = nbody[c];
+  const vec4<T> C = cX[c];
+  for (int t = lane; t < NC; t += 32) sl[wl][t] = L[(size_t)c * ncoef + t];
+  __syncwarp();
+  for (int i = lane; i < nb; i += 32) {
+    const vec4<T> b = bodies[b0 + i];
+    T pot, gx, gy, gz;
+    sph::l2p_body<T, P>(b.x - C.x, b.y - C.y, b.z - C.z, sl[wl], pot, gx, gy, gz);
+    vec4<T> s = trg_s[b0 + i], e = trg_e[b0 + i];
+    Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
+    comp_add(a0, pot);
+    comp_add(a1, gx);
+    comp_add(a2, gy);
+    comp_add(a3, gz);
+    trg_s[b0 + i] = make_v4<T>(a0.s, a1.s, a2.s, a3.s);
+    trg_e[b0 + i] = make_v4<T>(a0.e, a1.e, a2.e, a3.e);
+  }
+}
+
+// ---------------------------------------------------------------- dispatch
+template <typename T, int P> static void p2m_(Solver<T>& s) {
+  constexpr int W = P2MCfg<T, P>::W;
+  if (!s.nleaves) return;
+  k_p2m<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
+      s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.M.p, s.ncoef,
+      s.cfg.use_rmax, (T)s.cfg.theta);
+  FMM_LAUNCH_CHECK();
+}
+template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
+  constexpr int W = SphCfg<T>::W;
+  k_m2m<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(
+      lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
+      (T)s.cfg.theta);
+  FMM_LAUNCH_CHECK();
+}
+template <typename T, int P> static void m2l_(Solver<T>& s) {
+  if constexpr (sizeof(T) == 4) {
+    k_m2l_reg<T, P><<<ceil_div(s.ncells, 4), 128, 0, s.stream>>>(
+        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+  } else {
+    constexpr int W = SphCfg<T>::W;
+    k_m2l_lanes<T, P><<<ceil_div(s.ncells, W), 32 * W, 0, s.stream>>>(
+        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+  }
+}
+template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
+  constexpr int W = SphCfg<T>::W;
+  k_l2l<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
+                                                              s.cX.p, s.L.p, s.ncoef);
+  FMM_LAUNCH_CHECK();
+}
+template <typename T, int P> static void l2p_(Solver<T>& s) {
+  constexpr int W = SphCfg<T>::W;
+  if (!s.nleaves) return;
+  k_l2p<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
+      s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef,
+      s.trg_s.p, s.trg_e.p);
+  FMM_LAUNCH_CHECK();
+}
+
+
+// fill the dispatch table for one (precision, order); one object file per instantiation
+template <typename T, int P> void sph_fill(ExpansionOps<T>* ops) {
+  ops->p2m = &p2m_<T, P>;
+  ops->m2m_level = &m2m_<T, P>;
+  ops->m2l = &m2l_<T, P>;
+  ops->l2l_level = &l2l_<T, P>;
+  ops->l2p = &l2p_<T, P>;
+}
+
+}  // namespace fmmb200

@@ -1,0 +1,225 @@
+// Dual-tree traversal on the device (Traversal::dualTreeTraversal, include/traversal.h).
+//
+// The reference recurses from (root, root) (:248): a pair is far (M2L) when
+// |Xi - Xj|^2 > (Ri + Rj)^2 (:40), two leaves interact directly (P2P, :44-58), and
+// otherwise splitCell (:188-212) descends into the children of the leaf-less side, of both
+// sides when NBODY_i + NBODY_j >= nspawn (TraverseRange :65-124, which for mutual = false
+// visits every child pair), or of the larger cell (ties split Ci).  The set of emitted
+// pairs depends only on each pair, so here the recursion runs breadth first: every
+// iteration classifies a frontier of pairs in parallel (count pass + write pass, exact
+// sizes, no overflow) and emits M2L pairs, P2P pairs and the next frontier.  Lists are
+// then sorted by (target, source) into per-target CSR for the M2L and P2P kernels.
+#include <algorithm>
+
+#include "fmm_solver.cuh"
+
+namespace fmmb200 {
+
+enum { PAIR_M2L = 0, PAIR_P2P = 1, PAIR_SPLIT_I = 2, PAIR_SPLIT_J = 3, PAIR_SPLIT_IJ = 4 };
+
+template <typename T>
+__device__ __forceinline__ int classify(int ci, int cj, const vec4<T>* __restrict__ X,
+                                        const int* __restrict__ nchild,
+                                        const int* __restrict__ nbody, int nspawn, int* nout) {
+  vec4<T> a = X[ci], b = X[cj];
+  T R2 = norm_rn(sub_rn(a.x, b.x), sub_rn(a.y, b.y), sub_rn(a.z, b.z));
+  T Rs = add_rn(a.w, b.w);
+  if (R2 > mul_rn(Rs, Rs)) {
+    *nout = 1;
+    return PAIR_M2L;
+  }
+  int ni = nchild[ci], nj = nchild[cj];
+  if (ni == 0 && nj == 0) {
+    *nout = 1;
+    return PAIR_P2P;
+  }
+  if (nj == 0) {
+    *nout = ni;
+    return PAIR_SPLIT_I;
+  }
+  if (ni == 0) {
+    *nout = nj;
+    return PAIR_SPLIT_J;
+  }
+  if (nbody[ci] + nbody[cj] >= nspawn) {
+    *nout = ni * nj;
+    return PAIR_SPLIT_IJ;
+  }
+  if (a.w >= b.w) {
+    *nout = ni;
+    return PAIR_SPLIT_I;
+  }
+  *nout = nj;
+  return PAIR_SPLIT_J;
+}
+
+// pass 1: per-block totals of (M2L, P2P, children) added to three device counters
+template <typename T>
+__global__ void k_trav_count(const int2* __restrict__ front, int nfront,
+                             const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
+                             const int* __restrict__ nbody, int nspawn,
+                             unsigned long long* __restrict__ counters) {
+  unsigned long long c[3] = {0, 0, 0};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
+    int2 p = front[t];
+    int k;
+    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+    c[ty == PAIR_M2L ? 0 : ty == PAIR_P2P ? 1 : 2] += k;
+  }
+  for (int i = 0; i < 3; i++) {
+    unsigned long long v = warp_sum(c[i]);
+    if (lane_id() == 0 && v) atomicAdd(&counters[i], v);
+  }
+}
+
+// pass 2: write.  Output slots come from atomics (the final lists are sorted afterwards, so
+// their order does not depend on scheduling).
+template <typename T>
+__global__ void k_trav_write(const int2* __restrict__ front, int nfront,
+                             const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
+                             const int* __restrict__ ichild, const int* __restrict__ nbody,
+                             int nspawn, unsigned long long* __restrict__ counters,
+                             unsigned long long* __restrict__ m2l,
+                             unsigned long long* __restrict__ p2p, int2* __restrict__ next) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
+    int2 p = front[t];
+    int k;
+    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+    unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+    if (ty == PAIR_M2L) {
+      m2l[atomicAdd(&counters[0], 1ULL)] = packed;
+    } else if (ty == PAIR_P2P) {
+      p2p[atomicAdd(&counters[1], 1ULL)] = packed;
+    } else {
+      unsigned long long o = atomicAdd(&counters[2], (unsigned long long)k);
+      if (ty == PAIR_SPLIT_I) {
+        int c0 = ichild[p.x];
+        for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
+      } else if (ty == PAIR_SPLIT_J) {
+        int c0 = ichild[p.y];
+        for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, c0 + j);
+      } else {
+        int ci0 = ichild[p.x], cj0 = ichild[p.y];
+        int nj = nchild[p.y];
+        for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+      }
+    }
+  }
+}
+
+// CSR offsets of a sorted packed list: off[c] = first pair whose target >= c
+__global__ void k_csr(const unsigned long long* __restrict__ pairs, long long n, int ncells,
+                      int* __restrict__ off) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncells) return;
+  unsigned long long key = (unsigned long long)(unsigned)c << 32;
+  long long a = 0, z = n;
+  while (a < z) {
+    long long m = (a + z) >> 1;
+    if (pairs[m] < key) a = m + 1;
+    else z = m;
+  }
+  off[c] = (int)a;
+}
+
+// body-pair count of the P2P list: sum over pairs of nbody(target) * nbody(source)
+__global__ void k_p2p_bodypairs(const unsigned long long* __restrict__ pairs, long long n,
+                                const int* __restrict__ nbody,
+                                unsigned long long* __restrict__ out) {
+  unsigned long long s = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    unsigned long long p = pairs[t];
+    s += (unsigned long long)nbody[p >> 32] * (unsigned long long)nbody[p & 0xffffffffULL];
+  }
+  s = warp_sum(s);
+  if (lane_id() == 0 && s) atomicAdd(out, s);
+}
+
+static int bits_for(int n) {
+  int b = 1;
+  while ((1LL << b) < (long long)n) b++;
+  return b;
+}
+
+template <typename T> void build_lists(Solver<T>& s) {
+  const int TB = 256;
+  s.nm2l = s.np2p = s.p2p_body_pairs = 0;
+  if (s.ncells == 0) return;
+  unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
+  unsigned long long* hc = (unsigned long long*)s.scal_host;
+  s.front.ensure(1);
+  int2 root = make_int2(0, 0);
+  FMM_CUDA(cudaMemcpyAsync(s.front.p, &root, sizeof(int2), cudaMemcpyHostToDevice, s.stream));
+  long long nfront = 1;
+  long long nm2l = 0, np2p = 0;
+  s.m2l.ensure(1024);
+  s.p2p.ensure(1024);
+  while (nfront > 0) {
+    FMM_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s.stream));
+    int grid = std::min(ceil_div(nfront, TB), 148 * 16);
+    k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
+                                               s.c_nbody.p, s.cfg.nspawn, cnt);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpyAsync(hc, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+    long long am = (long long)hc[0], ap = (long long)hc[1], an = (long long)hc[2];
+    if (nm2l + am > (long long)s.m2l.cap) {
+      DevArr<unsigned long long> t;
+      t.ensure(std::max<size_t>(2 * s.m2l.cap, nm2l + am));
+      if (nm2l) FMM_CUDA(cudaMemcpyAsync(t.p, s.m2l.p, nm2l * 8, cudaMemcpyDeviceToDevice, s.stream));
+      FMM_CUDA(cudaStreamSynchronize(s.stream));
+      s.m2l.release();
+      s.m2l = t;
+    }
+    if (np2p + ap > (long long)s.p2p.cap) {
+      DevArr<unsigned long long> t;
+      t.ensure(std::max<size_t>(2 * s.p2p.cap, np2p + ap));
+      if (np2p) FMM_CUDA(cudaMemcpyAsync(t.p, s.p2p.p, np2p * 8, cudaMemcpyDeviceToDevice, s.stream));
+      FMM_CUDA(cudaStreamSynchronize(s.stream));
+      s.p2p.release();
+      s.p2p = t;
+    }
+    s.front2.ensure(std::max<long long>(an, 1));
+    unsigned long long base[3] = {(unsigned long long)nm2l, (unsigned long long)np2p, 0};
+    FMM_CUDA(cudaMemcpyAsync(cnt, base, sizeof(base), cudaMemcpyHostToDevice, s.stream));
+    k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
+                                               s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn, cnt,
+                                               s.m2l.p, s.p2p.p, s.front2.p);
+    FMM_LAUNCH_CHECK();
+    nm2l += am;
+    np2p += ap;
+    nfront = an;
+    std::swap(s.front, s.front2);
+  }
+  FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
+  s.nm2l = nm2l;
+  s.np2p = np2p;
+  const int endbit = 32 + bits_for(s.ncells);
+  s.list_tmp.ensure(std::max<long long>(std::max(nm2l, np2p), 1));
+  sort_keys_u64(s, s.m2l.p, s.list_tmp.p, (int)nm2l, endbit);
+  std::swap(s.m2l, s.list_tmp);
+  s.list_tmp.ensure(std::max<long long>(np2p, 1));
+  sort_keys_u64(s, s.p2p.p, s.list_tmp.p, (int)np2p, endbit);
+  std::swap(s.p2p, s.list_tmp);
+  s.m2l_off.ensure(s.ncells + 1);
+  s.p2p_off.ensure(s.ncells + 1);
+  k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.m2l.p, nm2l, s.ncells, s.m2l_off.p);
+  FMM_LAUNCH_CHECK();
+  k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.p2p.p, np2p, s.ncells, s.p2p_off.p);
+  FMM_LAUNCH_CHECK();
+  FMM_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned long long), s.stream));
+  k_p2p_bodypairs<<<std::max(1, std::min(ceil_div(np2p, TB), 148 * 8)), TB, 0, s.stream>>>(
+      s.p2p.p, np2p, s.c_nbody.p, cnt + 3);
+  FMM_LAUNCH_CHECK();
+  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           s.stream));
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  s.p2p_body_pairs = (long long)hc[3];
+}
+
+template void build_lists<float>(Solver<float>&);
+template void build_lists<double>(Solver<double>&);
+
+}  // namespace fmmb200

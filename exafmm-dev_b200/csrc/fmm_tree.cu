@@ -1,0 +1,456 @@
+// Adaptive octree build on the device, bit-exact with BuildTree (include/build_tree_tbb.h).
+//
+// The reference splits a node while it holds more than ncrit bodies (:172), scattering its
+// bodies stably by octant (x > Xc) + 2 (y > Yc) + 4 (z > Zc) (:59, :101) around a centre
+// that each level moves by +-R0 / 2^(level+1) (:199-203).  Here every body walks that same
+// chain of centres once (k_keys), recording its octant at each of kMaxLevel levels as a
+// 63-bit path key; a stable radix sort by key then lays the bodies out in octant order, and
+// nodes are carved out of the sorted keys level by level (k_split / k_emit), each node's
+// octant sub-ranges found by binary search.  Bodies inside a leaf keep their input order,
+// as the stable partitions leave them, via a second stable sort by leaf-truncated key.
+// Cells take the reference's layout (Nodes2cells :250-294): root first, the children of a
+// cell contiguous, each child's subtree after the previous child's.
+#include <cfloat>
+
+#include "fmm_solver.cuh"
+
+namespace fmmb200 {
+
+template <typename T> __device__ __forceinline__ T tmax();
+template <> __device__ __forceinline__ float tmax<float>() { return FLT_MAX; }
+template <> __device__ __forceinline__ double tmax<double>() { return DBL_MAX; }
+
+// ---------------------------------------------------------------- bounds
+// BoundBox::getBounds (include/bound_box.h:76-88): elementwise min / max of positions.
+template <typename T>
+__global__ void k_minmax_partial(const vec4<T>* __restrict__ b, int n, T* __restrict__ part) {
+  T mn[3] = {tmax<T>(), tmax<T>(), tmax<T>()};
+  T mx[3] = {-tmax<T>(), -tmax<T>(), -tmax<T>()};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    vec4<T> p = b[i];
+    mn[0] = p.x < mn[0] ? p.x : mn[0];
+    mn[1] = p.y < mn[1] ? p.y : mn[1];
+    mn[2] = p.z < mn[2] ? p.z : mn[2];
+    mx[0] = p.x > mx[0] ? p.x : mx[0];
+    mx[1] = p.y > mx[1] ? p.y : mx[1];
+    mx[2] = p.z > mx[2] ? p.z : mx[2];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T a = __shfl_xor_sync(0xffffffffu, mn[d], o);
+      T c = __shfl_xor_sync(0xffffffffu, mx[d], o);
+      mn[d] = a < mn[d] ? a : mn[d];
+      mx[d] = c > mx[d] ? c : mx[d];
+    }
+  __shared__ T sh[32][6];
+  int w = threadIdx.x >> 5;
+  if (lane_id() == 0)
+    for (int d = 0; d < 3; d++) sh[w][d] = mn[d], sh[w][3 + d] = mx[d];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+      for (int d = 0; d < 3; d++) {
+        mn[d] = sh[k][d] < mn[d] ? sh[k][d] : mn[d];
+        mx[d] = sh[k][3 + d] > mx[d] ? sh[k][3 + d] : mx[d];
+      }
+    for (int d = 0; d < 3; d++) part[6 * blockIdx.x + d] = mn[d], part[6 * blockIdx.x + 3 + d] = mx[d];
+  }
+}
+
+// BuildTree::bounds2box (include/build_tree_tbb.h:298-310); box = X0[3], R0, Xmin[3], Xmax[3]
+template <typename T>
+__global__ void k_box(const T* __restrict__ part, int nblk, T* __restrict__ box) {
+  if (threadIdx.x != 0) return;
+  T mn[3], mx[3];
+  for (int d = 0; d < 3; d++) mn[d] = part[d], mx[d] = part[3 + d];
+  for (int k = 1; k < nblk; k++)
+    for (int d = 0; d < 3; d++) {
+      T a = part[6 * k + d], c = part[6 * k + 3 + d];
+      mn[d] = a < mn[d] ? a : mn[d];
+      mx[d] = c > mx[d] ? c : mx[d];
+    }
+  T X[3], R = 0;
+  for (int d = 0; d < 3; d++) X[d] = div_rn(add_rn(mx[d], mn[d]), (T)2);
+  for (int d = 0; d < 3; d++) {
+    T a = sub_rn(X[d], mn[d]);
+    R = R < a ? a : R;
+    T c = sub_rn(mx[d], X[d]);
+    R = R < c ? c : R;
+  }
+  for (int d = 0; d < 3; d++) box[d] = X[d], box[4 + d] = mn[d], box[7 + d] = mx[d];
+  box[3] = (T)__dmul_rn((double)R, 1.00001);
+}
+
+// ---------------------------------------------------------------- path keys
+template <typename T>
+__global__ void k_keys(const vec4<T>* __restrict__ b, int n, const T* __restrict__ box,
+                       unsigned long long* __restrict__ keys, int* __restrict__ idx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vec4<T> p = b[i];
+  T c0 = box[0], c1 = box[1], c2 = box[2], R0 = box[3];
+  unsigned long long key = 0;
+#pragma unroll 1
+  for (int l = 0; l < kMaxLevel; l++) {
+    T r = div_rn(R0, (T)(1 << (l + 1)));
+    int o = (p.x > c0) | ((p.y > c1) << 1) | ((p.z > c2) << 2);
+    key = (key << 3) | (unsigned)o;
+    c0 = add_rn(c0, (o & 1) ? r : -r);
+    c1 = add_rn(c1, (o & 2) ? r : -r);
+    c2 = add_rn(c2, (o & 4) ? r : -r);
+  }
+  keys[i] = key;
+  idx[i] = i;
+}
+
+__device__ __forceinline__ int digit_at(unsigned long long key, int level) {
+  return (int)((key >> (3 * (kMaxLevel - 1 - level))) & 7ULL);
+}
+
+__global__ void k_root(int n, int* nbegin, int* ncount, int* nparent, int* nlevel) {
+  nbegin[0] = 0;
+  ncount[0] = n;
+  nparent[0] = -1;
+  nlevel[0] = 0;
+}
+
+template <typename T> __global__ void k_root_x(const T* __restrict__ box, T* __restrict__ nX) {
+  for (int d = 0; d < 3; d++) nX[d] = box[d];
+  nX[3] = 0;
+}
+
+// One level of BuildNodes (include/build_tree_tbb.h:165-218): a node with more than ncrit
+// bodies gets one child per non-empty octant; octant boundaries by binary search.
+__global__ void k_split(int lo, int hi, int level, int ncrit,
+                        const unsigned long long* __restrict__ keys,
+                        const int* __restrict__ nbegin, const int* __restrict__ ncount,
+                        int* __restrict__ cnt, int* __restrict__ starts) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int m = hi - lo;
+  if (t == m) cnt[m] = 0;
+  if (t >= m) return;
+  int v = lo + t;
+  int b = nbegin[v], c = ncount[v];
+  int nch = 0;
+  int* st = starts + 9 * t;
+  if (c > ncrit && level < kMaxLevel) {
+    st[0] = b;
+    st[8] = b + c;
+    for (int o = 1; o < 8; o++) {
+      int a = b, z = b + c;
+      while (a < z) {
+        int mid = (a + z) >> 1;
+        if (digit_at(keys[mid], level) < o) a = mid + 1;
+        else z = mid;
+      }
+      st[o] = a;
+    }
+    for (int o = 0; o < 8; o++) nch += st[o + 1] > st[o];
+  }
+  cnt[t] = nch;
+}
+
+template <typename T>
+__global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
+                       const int* __restrict__ coff, const int* __restrict__ starts,
+                       const T* __restrict__ box, int* __restrict__ nbegin,
+                       int* __restrict__ ncount, int* __restrict__ nparent,
+                       int* __restrict__ nchildn, int* __restrict__ nfirst,
+                       int* __restrict__ nlevel, T* __restrict__ nX) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi - lo) return;
+  int v = lo + t;
+  int nch = cnt[t];
+  nchildn[v] = nch;
+  if (nch == 0) {
+    nfirst[v] = -1;
+    return;
+  }
+  int first = hi + coff[t];
+  nfirst[v] = first;
+  const int* st = starts + 9 * t;
+  T r = div_rn(box[3], (T)(1 << (level + 1)));
+  T X0 = nX[4 * v], X1 = nX[4 * v + 1], X2 = nX[4 * v + 2];
+  int k = 0;
+  for (int o = 0; o < 8; o++) {
+    if (st[o + 1] <= st[o]) continue;
+    int u = first + k++;
+    nbegin[u] = st[o];
+    ncount[u] = st[o + 1] - st[o];
+    nparent[u] = v;
+    nlevel[u] = level + 1;
+    nX[4 * u] = add_rn(X0, (o & 1) ? r : -r);
+    nX[4 * u + 1] = add_rn(X1, (o & 2) ? r : -r);
+    nX[4 * u + 2] = add_rn(X2, (o & 4) ? r : -r);
+    nX[4 * u + 3] = 0;
+  }
+}
+
+// leaf nodes: chain-less nodes at the deepest level of the last pass
+__global__ void k_finish_level(int lo, int hi, int* nchildn, int* nfirst) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi - lo) return;
+  nchildn[lo + t] = 0;
+  nfirst[lo + t] = -1;
+}
+
+// NNODE bottom-up (include/build_tree_tbb.h:215-217)
+__global__ void k_nnode(int lo, int hi, const int* __restrict__ nchildn,
+                        const int* __restrict__ nfirst, int* __restrict__ nnode) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi - lo) return;
+  int v = lo + t;
+  int s = 1;
+  for (int k = 0; k < nchildn[v]; k++) s += nnode[nfirst[v] + k];
+  nnode[v] = s;
+}
+
+// Cell slots top-down (Nodes2cells, include/build_tree_tbb.h:272-286): children at CN,
+// next free slot after the child block, each child's subtree after the previous child's.
+__global__ void k_pos(int lo, int hi, const int* __restrict__ nchildn,
+                      const int* __restrict__ nfirst, const int* __restrict__ nnode,
+                      int* __restrict__ npos, int* __restrict__ ncb) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi - lo) return;
+  int v = lo + t;
+  if (v == 0) {
+    npos[0] = 0;
+    ncb[0] = 1;
+  }
+  int nch = nchildn[v];
+  if (nch == 0) return;
+  int cb = ncb[v];
+  int acc = cb + nch;
+  for (int k = 0; k < nch; k++) {
+    int u = nfirst[v] + k;
+    npos[u] = cb + k;
+    ncb[u] = acc;
+    acc += nnode[u] - 1;
+  }
+}
+
+// Cell records (Nodes2cells::operator(), include/build_tree_tbb.h:250-262) with the
+// Morton index of getKey (:240-249) in 64-bit arithmetic.
+template <typename T>
+__global__ void k_cells(int nnodes, const T* __restrict__ box, const int* __restrict__ nbegin,
+                        const int* __restrict__ ncount, const int* __restrict__ nparent,
+                        const int* __restrict__ nchildn, const int* __restrict__ nlevel,
+                        const int* __restrict__ npos, const int* __restrict__ ncb,
+                        const T* __restrict__ nX, int* iparent, int* ichild, int* nchild,
+                        int* ibody, int* nbody, int* clevel, unsigned long long* icell,
+                        vec4<T>* cX) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nnodes) return;
+  int c = npos[v];
+  int lev = nlevel[v];
+  T R0 = box[3];
+  T R = div_rn(R0, (T)(1 << lev));
+  T X[3] = {nX[4 * v], nX[4 * v + 1], nX[4 * v + 2]};
+  iparent[c] = v == 0 ? 0 : npos[nparent[v]];
+  int nch = nchildn[v];
+  nchild[c] = nch;
+  ichild[c] = nch ? ncb[v] : 0;
+  ibody[c] = nbegin[v];
+  nbody[c] = ncount[v];
+  clevel[c] = lev;
+  T diam = mul_rn((T)2, R);
+  int iX[3];
+  for (int d = 0; d < 3; d++) iX[d] = (int)div_rn(sub_rn(X[d], sub_rn(box[d], R0)), diam);
+  unsigned long long index = ((1ULL << (3 * lev)) - 1) / 7;
+  for (int l = 0; l < lev; l++) {
+    for (int d = 0; d < 3; d++) index += (unsigned long long)(iX[d] & 1) << (3 * l + d);
+    for (int d = 0; d < 3; d++) iX[d] >>= 1;
+  }
+  icell[c] = index;
+  cX[c] = make_v4<T>(X[0], X[1], X[2], R);
+}
+
+// leaf level of every sorted body (leaves only; ranges partition the bodies)
+__global__ void k_leaf_levels(int nnodes, const int* __restrict__ nchildn,
+                              const int* __restrict__ nbegin, const int* __restrict__ ncount,
+                              const int* __restrict__ nlevel, int* __restrict__ blev) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nnodes || nchildn[v] != 0) return;
+  int lev = nlevel[v];
+  for (int b = nbegin[v]; b < nbegin[v] + ncount[v]; b++) blev[b] = lev;
+}
+
+// key truncated to the body's leaf, scattered back to input order
+__global__ void k_tkey(int n, const unsigned long long* __restrict__ skeys,
+                       const int* __restrict__ sidx, const int* __restrict__ blev,
+                       unsigned long long* __restrict__ tkey, int* __restrict__ iota) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int lev = blev[b];
+  unsigned long long mask = lev == 0 ? 0ULL : (~0ULL << (3 * (kMaxLevel - lev)));
+  tkey[sidx[b]] = skeys[b] & mask;
+  iota[b] = b;
+}
+
+template <typename T>
+__global__ void k_permute(int n, const vec4<T>* __restrict__ in, const int* __restrict__ order,
+                          vec4<T>* __restrict__ out) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) out[b] = in[order[b]];
+}
+
+__global__ void k_leaf_flags(int nnodes, const int* __restrict__ nchildn, int* __restrict__ f) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nnodes) f[v] = nchildn[v] == 0;
+  if (v == nnodes) f[v] = 0;
+}
+
+__global__ void k_leaf_scatter(int nnodes, const int* __restrict__ nchildn,
+                               const int* __restrict__ off, const int* __restrict__ npos,
+                               int* __restrict__ leaves) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nnodes && nchildn[v] == 0) leaves[off[v]] = npos[v];
+}
+
+// grow a node array keeping its contents
+template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
+  if (n <= a.cap) return;
+  DevArr<U> b;
+  b.ensure(n > 2 * a.cap ? n : 2 * a.cap);
+  if (a.p) FMM_CUDA(cudaMemcpyAsync(b.p, a.p, a.cap * sizeof(U), cudaMemcpyDeviceToDevice, s.stream));
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  a.release();
+  a = b;
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+template <typename T> void build_tree(Solver<T>& s) {
+  const int n = s.n;
+  const int TB = 256;
+  s.box.ensure(16);
+  s.level_lo.clear();
+  s.ncells = s.maxlevel = s.nleaves = 0;
+  if (n == 0) {
+    FMM_CUDA(cudaMemsetAsync(s.box.p, 0, 16 * sizeof(T), s.stream));
+    return;
+  }
+  // bounds and box
+  int nblk = std::min(ceil_div(n, TB), 148 * 4);
+  s.minmax_part.ensure(6 * nblk);
+  k_minmax_partial<T><<<nblk, TB, 0, s.stream>>>(s.bodies_in.p, n, s.minmax_part.p);
+  FMM_LAUNCH_CHECK();
+  k_box<T><<<1, 32, 0, s.stream>>>(s.minmax_part.p, nblk, s.box.p);
+  FMM_LAUNCH_CHECK();
+  phase_end(s, FMM_PHASE_BOUNDS);
+  phase_begin(s, FMM_PHASE_TREE);
+  // keys and first sort
+  s.keys.ensure(n);
+  s.keys2.ensure(n);
+  s.idx.ensure(n);
+  s.idx2.ensure(n);
+  k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, s.keys.p, s.idx.p);
+  FMM_LAUNCH_CHECK();
+  sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, 3 * kMaxLevel);
+  // nodes, level by level
+  size_t cap0 = (size_t)std::max(1024, 4 * (n / std::max(1, s.cfg.ncrit)) + 64);
+  DevArr<int>* narr[] = {&s.nbegin, &s.ncount, &s.nparent, &s.nchildn, &s.nfirst,
+                         &s.nnode, &s.npos, &s.ncb, &s.nlevel};
+  for (auto* a : narr) a->ensure(cap0);
+  s.nX.ensure(4 * cap0);
+  k_root<<<1, 1, 0, s.stream>>>(n, s.nbegin.p, s.ncount.p, s.nparent.p, s.nlevel.p);
+  FMM_LAUNCH_CHECK();
+  k_root_x<T><<<1, 1, 0, s.stream>>>(s.box.p, s.nX.p);
+  FMM_LAUNCH_CHECK();
+  s.level_lo.push_back(0);
+  s.level_lo.push_back(1);
+  for (int level = 0;; level++) {
+    int lo = s.level_lo[level], hi = s.level_lo[level + 1];
+    int m = hi - lo;
+    s.nsplit.ensure(9 * (size_t)m);
+    s.coff.ensure(m + 1);
+    s.idx.ensure(std::max((size_t)n, (size_t)m + 1));
+    int* cnt = s.idx.p;  // the input-order index array is free until the second sort
+    k_split<<<ceil_div(m + 1, TB), TB, 0, s.stream>>>(lo, hi, level, s.cfg.ncrit, s.keys2.p,
+                                                       s.nbegin.p, s.ncount.p, cnt, s.nsplit.p);
+    FMM_LAUNCH_CHECK();
+    exclusive_sum_int(s, cnt, s.coff.p, m + 1);
+    FMM_CUDA(cudaMemcpyAsync(s.scal_host, s.coff.p + m, sizeof(int), cudaMemcpyDeviceToHost,
+                             s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+    int total = s.scal_host[0];
+    if (total == 0) {
+      k_finish_level<<<ceil_div(m, TB), TB, 0, s.stream>>>(lo, hi, s.nchildn.p, s.nfirst.p);
+      FMM_LAUNCH_CHECK();
+      break;
+    }
+    size_t need = (size_t)hi + total;
+    for (auto* a : narr) grow(s, *a, need);
+    grow(s, s.nX, 4 * need);
+    k_emit<T><<<ceil_div(m, TB), TB, 0, s.stream>>>(lo, hi, level, cnt, s.coff.p, s.nsplit.p,
+                                                    s.box.p, s.nbegin.p, s.ncount.p,
+                                                    s.nparent.p, s.nchildn.p, s.nfirst.p,
+                                                    s.nlevel.p, s.nX.p);
+    FMM_LAUNCH_CHECK();
+    s.level_lo.push_back(hi + total);
+  }
+  const int nlev = (int)s.level_lo.size() - 1;
+  const int nnodes = s.level_lo.back();
+  s.maxlevel = nlev - 1;
+  s.ncells = nnodes;
+  for (int l = nlev - 1; l >= 0; l--) {
+    int lo = s.level_lo[l], hi = s.level_lo[l + 1];
+    k_nnode<<<ceil_div(hi - lo, TB), TB, 0, s.stream>>>(lo, hi, s.nchildn.p, s.nfirst.p,
+                                                        s.nnode.p);
+    FMM_LAUNCH_CHECK();
+  }
+  for (int l = 0; l < nlev; l++) {
+    int lo = s.level_lo[l], hi = s.level_lo[l + 1];
+    k_pos<<<ceil_div(hi - lo, TB), TB, 0, s.stream>>>(lo, hi, s.nchildn.p, s.nfirst.p,
+                                                      s.nnode.p, s.npos.p, s.ncb.p);
+    FMM_LAUNCH_CHECK();
+  }
+  // cells
+  s.c_iparent.ensure(nnodes); s.c_ichild.ensure(nnodes); s.c_nchild.ensure(nnodes);
+  s.c_ibody.ensure(nnodes); s.c_nbody.ensure(nnodes); s.c_level.ensure(nnodes);
+  s.c_icell.ensure(nnodes);
+  s.cX.ensure(nnodes);
+  k_cells<T><<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(
+      nnodes, s.box.p, s.nbegin.p, s.ncount.p, s.nparent.p, s.nchildn.p, s.nlevel.p, s.npos.p,
+      s.ncb.p, s.nX.p, s.c_iparent.p, s.c_ichild.p, s.c_nchild.p, s.c_ibody.p, s.c_nbody.p,
+      s.c_level.p, s.c_icell.p, s.cX.p);
+  FMM_LAUNCH_CHECK();
+  // bodies inside a leaf in input order: stable sort by leaf-truncated key
+  int* blev = s.idx.p;
+  k_leaf_levels<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, s.nbegin.p,
+                                                           s.ncount.p, s.nlevel.p, blev);
+  FMM_LAUNCH_CHECK();
+  s.order.ensure(n);
+  k_tkey<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.keys2.p, s.idx2.p, blev, s.keys.p, s.order.p);
+  FMM_LAUNCH_CHECK();
+  // s.order currently holds 0..n-1 (input order positions); sort them by truncated key
+  FMM_CUDA(cudaMemcpyAsync(s.idx.p, s.order.p, n * sizeof(int), cudaMemcpyDeviceToDevice,
+                           s.stream));
+  sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
+  s.bodies.ensure(n);
+  k_permute<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.bodies_in.p, s.order.p, s.bodies.p);
+  FMM_LAUNCH_CHECK();
+  // leaf cell list
+  int* flags = s.nsplit.p;
+  s.nsplit.ensure(nnodes + 1);
+  flags = s.nsplit.p;
+  s.coff.ensure(nnodes + 1);
+  k_leaf_flags<<<ceil_div(nnodes + 1, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, flags);
+  FMM_LAUNCH_CHECK();
+  exclusive_sum_int(s, flags, s.coff.p, nnodes + 1);
+  FMM_CUDA(cudaMemcpyAsync(s.scal_host, s.coff.p + nnodes, sizeof(int), cudaMemcpyDeviceToHost,
+                           s.stream));
+  s.leaves.ensure(nnodes);
+  k_leaf_scatter<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, s.coff.p,
+                                                            s.npos.p, s.leaves.p);
+  FMM_LAUNCH_CHECK();
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  s.nleaves = s.scal_host[0];
+}
+
+template void build_tree<float>(Solver<float>&);
+template void build_tree<double>(Solver<double>&);
+
+}  // namespace fmmb200

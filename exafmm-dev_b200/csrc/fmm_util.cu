@@ -1,0 +1,151 @@
+// Utilities behind the C ABI: FP64 direct summation on the GPU (Traversal::direct +
+// normalize, include/traversal.h:304-337, accumulated in double), the FP32 FMA throughput
+// probe used as the roofline denominator of the FP32-pipe kernels, and the count of this
+// library's kernel launches.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <string>
+
+#include "fmm_solver.cuh"
+
+namespace fmmb200 {
+std::atomic<long long> g_launches{0};
+}
+using namespace fmmb200;
+
+namespace {
+
+constexpr int kDirTile = 256;
+
+__global__ void __launch_bounds__(kDirTile)
+    k_direct(int nt, const double* __restrict__ xt, int ns, const double* __restrict__ xs,
+             const double* __restrict__ qs, double eps2, double* __restrict__ out) {
+  __shared__ double sh[kDirTile][4];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double x = 0, y = 0, z = 0;
+  if (i < nt) {
+    x = xt[3 * i];
+    y = xt[3 * i + 1];
+    z = xt[3 * i + 2];
+  }
+  double pot = 0, ax = 0, ay = 0, az = 0;
+  for (int j0 = 0; j0 < ns; j0 += kDirTile) {
+    const int j = j0 + threadIdx.x;
+    __syncthreads();
+    if (j < ns) {
+      sh[threadIdx.x][0] = xs[3 * j];
+      sh[threadIdx.x][1] = xs[3 * j + 1];
+      sh[threadIdx.x][2] = xs[3 * j + 2];
+      sh[threadIdx.x][3] = qs[j];
+    }
+    __syncthreads();
+    const int cnt = min(kDirTile, ns - j0);
+    for (int k = 0; k < cnt; k++) {
+      const double dx = sh[k][0] - x, dy = sh[k][1] - y, dz = sh[k][2] - z;
+      const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+      if (r2 != 0) {
+        const double inv = 1.0 / sqrt(r2);
+        const double qi = sh[k][3] * inv;
+        const double inv3 = qi * inv * inv;
+        pot += qi;
+        ax += dx * inv3;
+        ay += dy * inv3;
+        az += dz * inv3;
+      }
+    }
+  }
+  if (i < nt) {
+    out[4 * i] = pot;
+    out[4 * i + 1] = ax;
+    out[4 * i + 2] = ay;
+    out[4 * i + 3] = az;
+  }
+}
+
+// independent FMA chains: 8 per thread, ITER iterations, 2 flops each
+template <int ITER>
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, float s) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = threadIdx.x * 1e-7f + k;
+#pragma unroll 16
+  for (int i = 0; i < ITER; i++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = fmaf(a[k], s, 1e-7f);
+  float t = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) t += a[k];
+  if (t == 123.456f) out[0] = t;  // keeps the chains live
+}
+
+}  // namespace
+
+extern "C" {
+
+long long fmm_b200_kernel_launches(void) { return g_launches.load(); }
+
+int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
+                    const double* qs, double eps2, double* out) {
+  if (nt < 0 || ns < 0 || (nt > 0 && (!xt || !out)) || (ns > 0 && (!xs || !qs)))
+    return FMM_ERR_INVALID;
+  if (nt == 0) return FMM_OK;
+  try {
+    FMM_CUDA(cudaSetDevice(device));
+    DevArr<double> b;
+    b.ensure(3 * (size_t)nt + 4 * (size_t)ns + 4 * (size_t)nt);
+    double *dxt = b.p, *dxs = b.p + 3 * (size_t)nt, *dqs = dxs + 3 * (size_t)ns,
+           *dout = dqs + ns;
+    FMM_CUDA(cudaMemcpy(dxt, xt, 24 * (size_t)nt, cudaMemcpyHostToDevice));
+    if (ns) {
+      FMM_CUDA(cudaMemcpy(dxs, xs, 24 * (size_t)ns, cudaMemcpyHostToDevice));
+      FMM_CUDA(cudaMemcpy(dqs, qs, 8 * (size_t)ns, cudaMemcpyHostToDevice));
+    }
+    k_direct<<<ceil_div(nt, kDirTile), kDirTile>>>(nt, dxt, ns, dxs, dqs, eps2, dout);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpy(out, dout, 32 * (size_t)nt, cudaMemcpyDeviceToHost));
+    b.release();
+  } catch (const FmmError& e) {
+    return e.code;
+  }
+  return FMM_OK;
+}
+
+int fmm_b200_fp32_peak(int device, double* tflops) {
+  if (!tflops) return FMM_ERR_INVALID;
+  try {
+    FMM_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    FMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    DevArr<float> o;
+    o.ensure(1);
+    constexpr int ITER = 8192;
+    const int blocks = sms * 8, threads = 256;
+    k_fma_probe<ITER><<<blocks, threads>>>(o.p, 0.9999f);  // warm-up
+    FMM_LAUNCH_CHECK();
+    cudaEvent_t a, b;
+    FMM_CUDA(cudaEventCreate(&a));
+    FMM_CUDA(cudaEventCreate(&b));
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+      FMM_CUDA(cudaEventRecord(a));
+      k_fma_probe<ITER><<<blocks, threads>>>(o.p, 0.9999f);
+      FMM_LAUNCH_CHECK();
+      FMM_CUDA(cudaEventRecord(b));
+      FMM_CUDA(cudaEventSynchronize(b));
+      float ms = 0;
+      FMM_CUDA(cudaEventElapsedTime(&ms, a, b));
+      best = ms < best ? ms : best;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    o.release();
+    const double flops = 2.0 * 8 * ITER * (double)blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+  } catch (const FmmError& e) {
+    return e.code;
+  }
+  return FMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+/* exafmm_b200.h -- C ABI of the B200-native Laplace FMM (libexafmm_b200.so).
+ *
+ * Drop-in boundary for the exafmm-dev single-node FMM hot path.  Every entry point takes
+ * plain pointers and sizes, returns an int status (FMM_OK = 0), and is re-entrant per
+ * solver handle.  The reference has no return codes (assert/exit, include/macros.h:10-14);
+ * here failures come back as status codes with a message from fmm_b200_last_error().
+ *
+ * Reference interfaces each group replaces:
+ *   fmm_b200_build_tree     BoundBox::getBounds (include/bound_box.h:76-88) +
+ *                           BuildTree::buildTree (include/build_tree_tbb.h:365-374)
+ *   fmm_b200_upward_pass    UpDownPass::upwardPass (include/up_down_pass.h:119-132)
+ *   fmm_b200_traverse       Traversal::dualTreeTraversal (include/traversal.h:240-264),
+ *                           applying kernel::M2L / kernel::P2P (include/kernel.h:6-14)
+ *   fmm_b200_downward_pass  UpDownPass::downwardPass (include/up_down_pass.h:135-148)
+ *   fmm_b200_solve_*        the examples/serial.cxx:46-60 sequence in one call
+ *   FMM_Init/FMM_Partition/FMM_Coulomb/FMM_Finalize   wrappers/gromacs.cxx:28-162
+ *   fmm_init_/fmm_partition_/fmm_coulomb_/fmm_finalize_ wrappers/charmm.cxx:31-202
+ *
+ * Body and result arrays in the working precision are 4-vectors: bodies (x, y, z, q),
+ * results (phi, dphi/dx, dphi/dy, dphi/dz) per unit target charge, in the caller's body
+ * order (the reference's TRG after downwardPass, scattered back by IBODY).
+ */
+#ifndef EXAFMM_B200_H
+#define EXAFMM_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FMM_OK 0
+#define FMM_ERR_INVALID 1        /* bad argument or configuration */
+#define FMM_ERR_CUDA 2           /* CUDA runtime error (message in fmm_b200_last_error) */
+#define FMM_ERR_NOT_SUPPORTED 3  /* e.g. periodic images > 0 */
+#define FMM_ERR_NO_MEMORY 4      /* device allocation failed */
+#define FMM_ERR_STATE 5          /* stage called out of order */
+#define FMM_ERR_NO_DEVICE 6      /* no CUDA device / kernels not built for it */
+#define FMM_ERR_DEVICE 7         /* a device-side check failed (capacity, depth) */
+
+/* expansion basis: the reference's -DSpherical / -DCartesian (Makefile.include:37-41) */
+#define FMM_SPHERICAL 0
+#define FMM_CARTESIAN 1
+/* working precision: FP32 expansions with compensated potential/gradient accumulation
+ * (the reference's float real_t + -DKAHAN), or FP64 throughout (-DFP64) */
+#define FMM_FP32 0
+#define FMM_FP64 1
+
+typedef struct fmm_b200_config {
+  int basis;       /* FMM_SPHERICAL or FMM_CARTESIAN */
+  int P;           /* expansion order: EXPANSION (include/types.h:38) */
+  double theta;    /* opening angle (include/args.h:98, -t) */
+  int ncrit;       /* bodies per leaf (include/args.h:98, -c) */
+  int nspawn;      /* 2x2 split threshold of the traversal (include/args.h:98, -s) */
+  int use_rmax;    /* include/args.h:99 (-x) */
+  int use_ropt;    /* include/args.h:99 (-o) */
+  int precision;   /* FMM_FP32 or FMM_FP64 */
+  double eps2;     /* softening squared (Traversal::eps2; see fmm_b200_config note) */
+  int images;      /* periodic image levels; only 0 is supported */
+  int device;      /* CUDA device ordinal */
+} fmm_b200_config;
+
+typedef struct fmm_b200_solver fmm_b200_solver;
+
+/* phase timings (milliseconds of device time, CUDA events on the solver's stream), in the
+ * reference's logger phase order (include/logger.h:87-106 call sites) */
+#define FMM_PHASE_BOUNDS 0
+#define FMM_PHASE_TREE 1
+#define FMM_PHASE_UPWARD 2
+#define FMM_PHASE_TRAVERSE 3   /* list construction */
+#define FMM_PHASE_M2L 4
+#define FMM_PHASE_P2P 5
+#define FMM_PHASE_DOWNWARD 6
+#define FMM_PHASE_TOTAL 7
+#define FMM_NUM_PHASES 8
+
+/* ---- lifecycle --------------------------------------------------------------------- */
+/* Defaults: spherical, P = 10, theta = 0.4, ncrit = 64, nspawn = 1000, use_rmax = 1,
+ * use_ropt = 1, FP32, eps2 = 0, images = 0, device 0. */
+int fmm_b200_default_config(fmm_b200_config* cfg);
+int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out);
+int fmm_b200_destroy(fmm_b200_solver* s);
+/* Work is issued on this stream (a cudaStream_t; NULL = the legacy default stream). */
+int fmm_b200_set_stream(fmm_b200_solver* s, void* stream);
+/* Message of the last failure on this handle (or of the last failed create if s is NULL). */
+const char* fmm_b200_last_error(const fmm_b200_solver* s);
+/* Which P values were compiled for a basis: writes up to cap values, returns the count. */
+int fmm_b200_supported_orders(int basis, int* orders, int cap);
+
+/* ---- whole solve --------------------------------------------------------------------- */
+/* Bodies and results in device memory (4-vectors in the working precision, caller order).
+ * Stream-ordered; returns once the work is queued (plus the few host reads the level
+ * structure needs). */
+int fmm_b200_solve_device(fmm_b200_solver* s, int n, const void* d_bodies, void* d_trg);
+/* Host double arrays as in FMM_Coulomb (wrappers/gromacs.cxx:104-162): x interleaved
+ * (3n), q (n); p (n) and f (3n) receive phi and grad phi.  Copies in and out inside the
+ * call; synchronous. */
+int fmm_b200_solve_host(fmm_b200_solver* s, int n, const double* x, const double* q,
+                        double* p, double* f);
+
+/* ---- stages (the reference's class methods) ------------------------------------------ */
+int fmm_b200_set_bodies_host(fmm_b200_solver* s, int n, const double* x, const double* q);
+int fmm_b200_set_bodies_device(fmm_b200_solver* s, int n, const void* d_bodies);
+int fmm_b200_build_tree(fmm_b200_solver* s);
+int fmm_b200_upward_pass(fmm_b200_solver* s);
+int fmm_b200_traverse(fmm_b200_solver* s);
+int fmm_b200_downward_pass(fmm_b200_solver* s);
+int fmm_b200_get_trg_host(fmm_b200_solver* s, double* trg);   /* 4n, caller order */
+int fmm_b200_get_trg_device(fmm_b200_solver* s, void* d_trg); /* 4n working precision */
+
+/* ---- introspection (tree, lists, expansions; host copies) ----------------------------- */
+int fmm_b200_num_cells(fmm_b200_solver* s, int* num_cells, int* max_level);
+/* Cells in the reference layout (include/types.h:79-92, include/build_tree_tbb.h:250-294):
+ * X is 3 per cell; R is the current radius (after build: R0 / 2^level; after the upward
+ * pass: the MAC radius). */
+int fmm_b200_get_cells(fmm_b200_solver* s, int* iparent, int* ichild, int* nchild,
+                       int* ibody, int* nbody, unsigned long long* icell, int* level,
+                       double* X, double* R);
+/* Original index (IBODY) of each body in tree order. */
+int fmm_b200_get_order(fmm_b200_solver* s, int* ibody);
+/* Root box: X0[3], R0 (BuildTree::bounds2box, include/build_tree_tbb.h:298-310). */
+int fmm_b200_get_box(fmm_b200_solver* s, double* x0r0);
+/* which = 0: multipoles M, 1: locals L.  Spherical: NTERM (re, im) pairs per cell;
+ * Cartesian: NTERM reals per cell. */
+int fmm_b200_get_expansion(fmm_b200_solver* s, int which, double* out);
+/* Interaction lists of the last traversal: cell pairs packed (target << 32) | source,
+ * sorted; body-pair counts are the sum of target x source body counts. */
+int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2p,
+                       long long* p2p_body_pairs);
+int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
+int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
+
+/* ---- utilities ----------------------------------------------------------------------- */
+/* FP64 direct sum on the GPU: Traversal::direct + normalize (include/traversal.h:304-337)
+ * with double accumulation.  Targets xt (3 nt), sources xs (3 ns) with charges qs; out
+ * receives 4 nt values (phi, grad phi) per unit target charge; pairs with r^2 + eps2 == 0
+ * are skipped.  Synchronous. */
+int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
+                    const double* qs, double eps2, double* out);
+/* FP32 FMA throughput of the device in TFLOP/s (independent FMA chains on every SM): the
+ * roofline denominator of the FP32-pipe kernels (M2L, P2P).  No reference counterpart. */
+int fmm_b200_fp32_peak(int device, double* tflops);
+/* Number of this library's own kernel launches so far (library calls such as CUB sorts are
+ * not counted).  No reference counterpart. */
+long long fmm_b200_kernel_launches(void);
+
+/* ---- reference wrapper ABI (single GPU, single rank) ----------------------------------
+ * FMM_Init: the gromacs wrapper's fixed parameters (ncrit 32, nspawn 1000, theta 0.4,
+ * use_rmax, use_ropt, eps2 0, wrappers/gromacs.cxx:28-56) on the spherical basis at
+ * EXAFMM_B200_P (default 10) in FP32; images must be 0 (periodic boundaries are not
+ * supported: the call leaves the library uninitialised and FMM_Coulomb does nothing). */
+void FMM_Init(int images);
+void FMM_Finalize(void);
+#ifdef __cplusplus
+void FMM_Partition(int& n, int* index, double* x, double* q, double cycle);
+#else
+void FMM_Partition(int* n, int* index, double* x, double* q, double cycle);
+#endif
+void FMM_Coulomb(int n, double* x, double* q, double* p, double* f, double cycle);
+
+/* Fortran ABI of the CHARMM wrapper (wrappers/charmm.cxx:31-202), single rank: bodies
+ * with icpumap[i] == 1 are solved and p, f accumulate TRG * q * 332.0716. */
+void fmm_init_(int* images, double* theta, int* verbose);
+void fmm_finalize_(void);
+void fmm_partition_(int* nglobal, int* icpumap, double* x, double* q, double* xold,
+                    double* cycle);
+void fmm_coulomb_(int* nglobal, int* icpumap, double* x, double* q, double* p, double* f,
+                  double* cycle);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,238 @@
+"""Parity of the CUDA path (through the C ABI) against the oracle and the reference goldens.
+
+Bar: trees, body order and (for use_ropt = 0) interaction lists bit-exact; with the
+error-optimised radius (use_ropt = 1) the radii go through the GPU's powf / pow, which may
+differ from glibc's in the last bit, so a handful of borderline MAC decisions may flip
+(<= 1e-4 of the pairs).  Potentials and gradients: FP64 within 1e-10 of the FP64 oracle on
+the same tree; FP32 within 2e-5 rel-L2 of the FP32 oracle, and within the oracle's own FMM
+error (+ 2e-6) of an FP64 direct sum.
+"""
+import importlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import CARTESIAN, SPHERICAL, Oracle, rel_l2
+
+pytestmark = pytest.mark.gpu
+fmm = importlib.import_module("exafmm-dev_b200")
+
+CASES = {
+    "sph6_f64_cube": ("spherical", 6, "f64", "cube", 16384, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    "sph6_f32_cube": ("spherical", 6, "f32", "cube", 20000,
+                      dict(ncrit=32, theta=0.4, use_ropt=0, nspawn=500)),
+    "sph10_f32_plummer": ("spherical", 10, "f32", "plummer", 30000,
+                          dict(ncrit=64, theta=0.35, use_ropt=1)),
+    "sph8_f64_plummer": ("spherical", 8, "f64", "plummer", 12000,
+                         dict(ncrit=48, theta=0.4, use_ropt=1)),
+    "sph4_f32_sphere": ("spherical", 4, "f32", "sphere", 20000, dict(ncrit=16, theta=0.5, use_ropt=0)),
+    "cart5_f32_sphere": ("cartesian", 5, "f32", "sphere", 30000, dict(ncrit=32, theta=0.5, use_ropt=0)),
+    "cart4_f64_cube": ("cartesian", 4, "f64", "cube", 10000, dict(ncrit=16, theta=0.6, use_ropt=0)),
+}
+
+_oracle_cache = {}
+
+
+def oracle_run(name, datasets):
+    if name not in _oracle_cache:
+        basis, P, prec, dist, n, kw = CASES[name]
+        x, q = datasets.make(dist, n, seed=11, precision=prec)
+        o = Oracle(prec).run(x, q, basis=SPHERICAL if basis == "spherical" else CARTESIAN, P=P,
+                             kahan=int(prec == "f32"), **kw)
+        _oracle_cache[name] = (x, q, o)
+    return _oracle_cache[name]
+
+
+def gpu_solver(name):
+    basis, P, prec, dist, n, kw = CASES[name]
+    return fmm.Solver(basis=basis, P=P, precision=prec, **kw)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_tree_bit_exact(name, datasets):
+    x, q, o = oracle_run(name, datasets)
+    s = gpu_solver(name)
+    s.set_bodies(x, q)
+    s.build_tree()
+    g, r = s.cells(), o.cells()
+    assert np.array_equal(s.box(), o.box())
+    for k in ("iparent", "ichild", "nchild", "ibody", "nbody", "level", "icell", "X"):
+        assert np.array_equal(g[k], r[k]), k
+    assert np.array_equal(g["R"], r["R_built"])
+    assert np.array_equal(s.order(), o.order())
+    assert s.num_cells()[1] == o.maxlevel
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_upward_and_lists(name, datasets):
+    x, q, o = oracle_run(name, datasets)
+    basis, P, prec, dist, n, kw = CASES[name]
+    s = gpu_solver(name)
+    s.set_bodies(x, q)
+    s.build_tree()
+    s.upward_pass()
+    R = s.cells()["R"]
+    Mg, Mo = s.expansion(0), o.expansion(0)
+    scale = np.abs(Mo).max(axis=1, keepdims=True) + 1e-300
+    err = (np.abs(Mg - Mo) / scale).max()
+    assert err < (2e-5 if prec == "f32" else 1e-11), err
+    s.traverse()
+    m2l, p2p = s.lists()
+    om2l, op2p = np.sort(o.m2l()), np.sort(o.p2p())
+    if kw["use_ropt"] == 0:
+        assert np.array_equal(R, o.cells()["R"])
+        assert np.array_equal(m2l, om2l)
+        assert np.array_equal(p2p, op2p)
+    else:
+        assert np.allclose(R, o.cells()["R"], rtol=1e-5, atol=0)
+        diff = len(np.setxor1d(m2l, om2l)) + len(np.setxor1d(p2p, op2p))
+        assert diff <= max(2, 1e-4 * (len(om2l) + len(op2p))), diff
+    nm2l, np2p, pairs = s.list_counts()
+    assert (nm2l, np2p) == (len(m2l), len(p2p))
+    c = s.cells()
+    tgt, src = p2p >> 32, p2p & 0xffffffff
+    assert pairs == int((c["nbody"][tgt].astype(np.int64) * c["nbody"][src]).sum())
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_solve_matches_oracle_and_direct(name, datasets):
+    x, q, o = oracle_run(name, datasets)
+    basis, P, prec, dist, n, kw = CASES[name]
+    s = gpu_solver(name)
+    trg = s.solve(x, q)
+    ref = o.trg()
+    pot, acc = rel_l2(trg, ref)
+    tol = 2e-5 if prec == "f32" else 1e-10
+    assert pot < tol and acc < tol, (pot, acc)
+    idx = datasets.sample_targets(n, 256)
+    d = Oracle("f64").direct(x[idx], x, q)
+    gp, ga = rel_l2(trg[idx], d)
+    op, oa = rel_l2(ref[idx], d)
+    assert gp < op * 1.05 + 2e-6 and ga < oa * 1.05 + 2e-6, (gp, ga, op, oa)
+
+
+@pytest.mark.parametrize("case", ["sph_p6_f64_cube", "sph_p10_f32k_plummer",
+                                  "cart_p5_f32_sphere"])
+def test_golden_reference(case, golden_dir):
+    """Against the reference's own outputs (tests/golden, made by make_golden.py)."""
+    g = np.load(os.path.join(golden_dir, case + ".npz"))
+    p = json.loads(str(g["params"]))
+    basis = "spherical" if p["config"].startswith("sph") else "cartesian"
+    P = int(p["config"].split("_")[1][1:])
+    s = fmm.Solver(basis=basis, P=P, theta=p["theta"], ncrit=p["ncrit"],
+                   use_ropt=p["use_ropt"], precision=p["precision"])
+    s.set_bodies(g["x"], g["q"])
+    s.build_tree()
+    c = s.cells()
+    for k in ("iparent", "ichild", "nchild", "ibody", "nbody", "level"):
+        assert np.array_equal(c[k], g["cell_" + k]), k
+    assert np.array_equal(c["X"], g["cell_X"])
+    assert np.array_equal(s.order(), g["order"])
+    s.upward_pass()
+    s.traverse()
+    s.downward_pass()
+    m2l, p2p = s.lists()
+    diff = len(np.setxor1d(m2l, g["m2l"])) + len(np.setxor1d(p2p, g["p2p"]))
+    assert diff <= (0 if p["use_ropt"] == 0 else 2), diff
+    pot, acc = rel_l2(s.trg(), g["trg"])
+    tol = 5e-5 if p["precision"] == "f32" else 5e-7
+    assert pot < tol and acc < tol, (pot, acc)
+
+
+def test_edge_cases(datasets):
+    s = fmm.Solver(basis="spherical", P=6, theta=0.4, ncrit=16, use_ropt=0, precision="f64")
+    # no bodies
+    out = s.solve(np.zeros((0, 3)), np.zeros(0))
+    assert out.shape == (0, 4)
+    # one body: potential 0; the gradient is the reference's 0/0 at the cell centre
+    out = s.solve(np.array([[0.1, 0.2, 0.3]]), np.array([1.0]))
+    assert out[0, 0] == 0 and np.all(np.isnan(out[0, 1:]))
+    # two bodies: exact
+    x = np.array([[0.5, 0.25, -0.5], [0.1, 0.2, 0.3]])
+    qq = np.array([1.0, 2.0])
+    o = Oracle("f64")
+    assert np.allclose(s.solve(x, qq), o.direct(x, x, qq), rtol=1e-12)
+    # coincident bodies beyond the depth cap, plus a random cloud
+    xr, qr = datasets.make("cube", 2000, seed=5, precision="f64")
+    xs = np.concatenate([xr, np.tile([[0.25, -0.125, 0.5]], (100, 1))])
+    qs = np.concatenate([qr, np.full(100, 0.01)])
+    trg = s.solve(xs, qs)
+    ref = o.run(xs, qs, P=6, theta=0.4, ncrit=16).trg()
+    ok = np.isfinite(ref).all(axis=1)
+    assert np.allclose(trg[ok], ref[ok], rtol=1e-9, atol=1e-9)
+    assert np.array_equal(np.isfinite(trg), np.isfinite(ref))
+
+
+def test_ncrit_one_and_reuse(datasets):
+    """ncrit = 1 (one body per leaf) and a handle reused across sizes."""
+    s = fmm.Solver(basis="spherical", P=4, theta=0.5, ncrit=1, use_ropt=0, precision="f64")
+    o = Oracle("f64")
+    for n in (50, 3000, 700):
+        x, q = datasets.make("plummer", n, seed=n, precision="f64")
+        trg = s.solve(x, q)
+        ref = o.run(x, q, P=4, theta=0.5, ncrit=1).trg()
+        ok = np.isfinite(ref).all(axis=1)
+        assert np.allclose(trg[ok], ref[ok], rtol=1e-9, atol=1e-12)
+
+
+def test_deterministic(datasets):
+    x, q = datasets.make("plummer", 50000, precision="f32")
+    s = fmm.Solver(P=8, theta=0.4, ncrit=64)
+    a = s.solve(x, q)
+    b = s.solve(x, q)
+    assert np.array_equal(a, b)
+
+
+def test_device_entry_matches_host(datasets):
+    torch = pytest.importorskip("torch")
+    x, q = datasets.make("cube", 40000, precision="f32")
+    s = fmm.Solver(P=6, theta=0.4, ncrit=64, use_ropt=0)
+    ref = s.solve(x, q)
+    bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1), dtype=torch.float32,
+                          device="cuda")
+    out = torch.empty_like(bodies)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    s.solve_device(len(q), bodies.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().astype(np.float64), ref.astype(np.float32).astype(np.float64))
+
+
+def test_gromacs_wrapper(datasets):
+    """FMM_Coulomb (wrappers/gromacs.cxx:104-162) on one rank: p, f are phi and grad phi
+    minus the dipole correction the reference applies with the given cycle."""
+    lib = fmm.load_library()
+    x, q = datasets.make("cube", 5000, seed=3, precision="f64")
+    x = np.ascontiguousarray(x * 0.9)
+    n = len(q)
+    cycle = 2 * np.pi
+    lib.FMM_Init(0)
+    p = np.zeros(n)
+    f = np.zeros(3 * n)
+    xf = np.ascontiguousarray(x.reshape(-1))
+    lib.FMM_Coulomb(n, fmm._p(xf), fmm._p(q), fmm._p(p), fmm._p(f), cycle)
+    lib.FMM_Finalize()
+    d = Oracle("f64").direct(x, x, q)
+    dip = (x * q[:, None]).sum(0)
+    coef = 4 * np.pi / (3 * cycle ** 3)
+    ep = d[:, 0] - coef * (dip ** 2).sum() / n / q
+    ef = d[:, 1:] - coef * dip
+    assert np.sqrt(((p - ep) ** 2).sum() / (ep ** 2).sum()) < 1e-3
+    assert np.sqrt(((f.reshape(-1, 3) - ef) ** 2).sum() / (ef ** 2).sum()) < 1e-3
+
+
+def test_timings_and_errors(datasets):
+    s = fmm.Solver(P=6)
+    with pytest.raises(fmm.FmmError) as e:
+        s.upward_pass()
+    assert e.value.code == fmm.FMM_ERR_STATE
+    x, q = datasets.make("cube", 20000, precision="f32")
+    s.solve(x, q)
+    t = s.timings()
+    assert t["total"] > 0 and t["m2l"] > 0 and t["p2p"] > 0
+    with pytest.raises(fmm.FmmError) as e:
+        fmm.Solver(P=6, images=1)
+    assert e.value.code == fmm.FMM_ERR_NOT_SUPPORTED
+    with pytest.raises(fmm.FmmError):
+        fmm.Solver(P=3)

@@ -58,7 +58,7 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -70,7 +70,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -180,6 +180,9 @@ def main():
     ap.add_argument("--ref-n", type=int, default=REF_SAMPLE_N)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-ups, then one solve between cudaProfilerStart/Stop (for ncu "
+                         "--profile-from-start off), then exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     datasets = importlib.import_module("exafmm-dev_b200.datasets")
@@ -217,6 +220,15 @@ def main():
     for _ in range(args.warmup):
         step(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     torch.cuda.synchronize()
+    if args.profile:
+        torch.cuda.profiler.start()
+        step(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        if rank == 0:
+            print(json.dumps({"profile": WORKLOAD_NAME, "n_bodies": n,
+                              "phases_ms": solver.timings(), "lists": solver.list_counts()}))
+        return
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -231,6 +243,11 @@ def main():
         t = solver.timings()
         phase_sum = t if phase_sum is None else {k: phase_sum[k] + t[k] for k in t}
     torch.cuda.synchronize()
+    # keep the GPU under the same load until the sampler has a few readings
+    t_extra = time.perf_counter()
+    while len(clocks.rows) < 5 and time.perf_counter() - t_extra < 3.0:
+        step(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        torch.cuda.synchronize()
     clk = clocks.stop()
     launches = (fmm.kernel_launches() - launches0) // args.steps
     step_ms = [a.elapsed_time(b) for a, b in evs]

@@ -1,0 +1,319 @@
+// exafmm_b200.hpp -- C++ facade with the reference's single-node class API, backed by the
+// GPU solver of libexafmm_b200.so (C ABI in exafmm_b200.h).
+//
+// The reference drives one solve as (examples/serial.cxx:46-60)
+//     bounds = boundBox.getBounds(bodies);
+//     cells  = buildTree.buildTree(bodies, buffer, bounds);
+//     upDownPass.upwardPass(cells);
+//     traversal.dualTreeTraversal(cells, cells, cycle, mutual);
+//     upDownPass.downwardPass(cells);
+// and the same calls compile against this header.  The work runs on the device; Bodies
+// and Cells are host mirrors, refreshed after each stage:
+//   * buildTree permutes `bodies` into tree order in place, as the reference does
+//     (include/build_tree_tbb.h:365-374), and returns the cells in the reference layout;
+//   * upwardPass refreshes each Cell's R and M; downwardPass its L and every Body's TRG
+//     (phi, grad phi per unit charge, include/types.h:71 and kernels/*CPU.cxx L2P).
+// Run-time parameters replace the reference's compile-time ones (EXPANSION, Spherical /
+// Cartesian, FP64, include/types.h:12-45): set them in a Context before building.
+// Only the non-periodic, non-mutual path exists (images = 0); Traversal::direct runs the
+// FP64 direct sum on the GPU.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "exafmm_b200.h"
+
+namespace exafmm_b200 {
+
+typedef double real_t;
+typedef std::complex<double> complex_t;
+
+struct vec3 {
+  real_t v[3] = {0, 0, 0};
+  real_t& operator[](int i) { return v[i]; }
+  const real_t& operator[](int i) const { return v[i]; }
+};
+struct vec4 {
+  real_t v[4] = {0, 0, 0, 0};
+  real_t& operator[](int i) { return v[i]; }
+  const real_t& operator[](int i) const { return v[i]; }
+};
+
+struct Bounds {  // include/types.h:54-57
+  vec3 Xmin, Xmax;
+};
+
+struct Body {  // include/types.h:60-72
+  vec3 X;
+  real_t SRC = 0;
+  int IBODY = 0;
+  int IRANK = 0;
+  uint64_t ICELL = 0;
+  real_t WEIGHT = 1;
+  vec4 TRG;
+};
+typedef std::vector<Body> Bodies;
+typedef Bodies::iterator B_iter;
+
+struct Cell {  // include/types.h:79-92 (BODY is an index-based iterator here)
+  int IPARENT = 0, ICHILD = 0, NCHILD = 0, IBODY = 0, NBODY = 0;
+  B_iter BODY;
+  uint64_t ICELL = 0;
+  real_t WEIGHT = 0;
+  vec3 X;
+  real_t R = 0;
+  std::vector<complex_t> M, L;  // spherical: NTERM complex; Cartesian: NTERM real parts
+};
+typedef std::vector<Cell> Cells;
+typedef Cells::iterator C_iter;
+
+class Error : public std::runtime_error {
+ public:
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Solver parameters the reference fixes at compile time, plus the device.
+struct Context {
+  fmm_b200_config cfg;
+  std::shared_ptr<fmm_b200_solver> solver;
+  Bodies* bodies = nullptr;
+  Context() { fmm_b200_default_config(&cfg); }
+  static Context& global() {
+    static Context c;
+    return c;
+  }
+  void check(int rc) const {
+    if (rc != FMM_OK)
+      throw Error(rc, fmm_b200_last_error(solver ? solver.get() : nullptr));
+  }
+  fmm_b200_solver* get() {
+    if (!solver) {
+      fmm_b200_solver* s = nullptr;
+      int rc = fmm_b200_create(&cfg, &s);
+      if (rc != FMM_OK) throw Error(rc, fmm_b200_last_error(nullptr));
+      solver.reset(s, [](fmm_b200_solver* p) { fmm_b200_destroy(p); });
+    }
+    return solver.get();
+  }
+  void reset() { solver.reset(); }
+};
+
+inline int nterm(const fmm_b200_config& c) {
+  return c.basis == FMM_SPHERICAL ? c.P * (c.P + 1) / 2 : c.P * (c.P + 1) * (c.P + 2) / 6;
+}
+
+// BoundBox (include/bound_box.h:73-121)
+class BoundBox {
+ public:
+  explicit BoundBox(int nspawn = 1000) : nspawn_(nspawn) {}
+  Bounds getBounds(Bodies& bodies) {
+    Bounds b;
+    if (bodies.empty()) return b;
+    b.Xmin = b.Xmax = bodies.front().X;
+    return getBounds(bodies, b);
+  }
+  Bounds getBounds(const Bodies& bodies, Bounds b) {
+    for (const Body& B : bodies)
+      for (int d = 0; d < 3; d++) {
+        b.Xmin[d] = B.X[d] < b.Xmin[d] ? B.X[d] : b.Xmin[d];
+        b.Xmax[d] = B.X[d] > b.Xmax[d] ? B.X[d] : b.Xmax[d];
+      }
+    return b;
+  }
+
+ private:
+  int nspawn_;
+};
+
+// BuildTree (include/build_tree_tbb.h:362-387).  The tree is built from the bodies'
+// own bounds on the device (the bounds argument is accepted for API compatibility).
+class BuildTree {
+ public:
+  BuildTree(int ncrit, int nspawn, Context& ctx = Context::global()) : ctx_(ctx) {
+    ctx_.cfg.ncrit = ncrit;
+    ctx_.cfg.nspawn = nspawn;
+  }
+  Cells buildTree(Bodies& bodies, Bodies& buffer, Bounds) {
+    ctx_.reset();  // parameters may have changed
+    fmm_b200_solver* s = ctx_.get();
+    const int n = (int)bodies.size();
+    std::vector<double> x(3 * (size_t)n), q(n);
+    for (int i = 0; i < n; i++) {
+      for (int d = 0; d < 3; d++) x[3 * i + d] = bodies[i].X[d];
+      q[i] = bodies[i].SRC;
+    }
+    ctx_.check(fmm_b200_set_bodies_host(s, n, x.data(), q.data()));
+    ctx_.check(fmm_b200_build_tree(s));
+    std::vector<int> order(n);
+    if (n) ctx_.check(fmm_b200_get_order(s, order.data()));
+    buffer = bodies;
+    for (int i = 0; i < n; i++) bodies[i] = buffer[order[i]];
+    ctx_.bodies = &bodies;
+    maxlevel_ = 0;
+    return fetch_cells(ctx_, bodies, false, false);
+  }
+  void printTreeData(Cells& cells) { (void)cells; }
+
+  static Cells fetch_cells(Context& ctx, Bodies& bodies, bool M, bool L) {
+    fmm_b200_solver* s = ctx.get();
+    int nc = 0, ml = 0;
+    ctx.check(fmm_b200_num_cells(s, &nc, &ml));
+    std::vector<int> ip(nc), ic(nc), nch(nc), ib(nc), nb(nc), lev(nc);
+    std::vector<unsigned long long> key(nc);
+    std::vector<double> X(3 * (size_t)nc), R(nc);
+    if (nc)
+      ctx.check(fmm_b200_get_cells(s, ip.data(), ic.data(), nch.data(), ib.data(), nb.data(),
+                                   key.data(), lev.data(), X.data(), R.data()));
+    const int nt = nterm(ctx.cfg);
+    const int w = ctx.cfg.basis == FMM_SPHERICAL ? 2 : 1;
+    std::vector<double> em, el;
+    if (M && nc) {
+      em.resize((size_t)nc * nt * w);
+      ctx.check(fmm_b200_get_expansion(s, 0, em.data()));
+    }
+    if (L && nc) {
+      el.resize((size_t)nc * nt * w);
+      ctx.check(fmm_b200_get_expansion(s, 1, el.data()));
+    }
+    Cells cells(nc);
+    for (int c = 0; c < nc; c++) {
+      Cell& C = cells[c];
+      C.IPARENT = ip[c];
+      C.ICHILD = ic[c];
+      C.NCHILD = nch[c];
+      C.IBODY = ib[c];
+      C.NBODY = nb[c];
+      C.BODY = bodies.begin() + ib[c];
+      C.ICELL = key[c];
+      for (int d = 0; d < 3; d++) C.X[d] = X[3 * c + d];
+      C.R = R[c];
+      auto unpack = [&](const std::vector<double>& e, std::vector<complex_t>& out) {
+        if (e.empty()) return;
+        out.resize(nt);
+        for (int t = 0; t < nt; t++)
+          out[t] = w == 2 ? complex_t(e[((size_t)c * nt + t) * 2], e[((size_t)c * nt + t) * 2 + 1])
+                          : complex_t(e[(size_t)c * nt + t], 0);
+      };
+      unpack(em, C.M);
+      unpack(el, C.L);
+    }
+    return cells;
+  }
+
+ private:
+  Context& ctx_;
+  int maxlevel_ = 0;
+};
+
+// UpDownPass (include/up_down_pass.h:113-148)
+class UpDownPass {
+ public:
+  UpDownPass(real_t theta, bool useRmax, bool useRopt, Context& ctx = Context::global())
+      : ctx_(ctx) {
+    ctx_.cfg.theta = theta;
+    ctx_.cfg.use_rmax = useRmax;
+    ctx_.cfg.use_ropt = useRopt;
+  }
+  void upwardPass(Cells& cells) {
+    if (cells.empty()) return;
+    ctx_.check(fmm_b200_upward_pass(ctx_.get()));
+    cells = BuildTree::fetch_cells(ctx_, *ctx_.bodies, true, false);
+  }
+  void downwardPass(Cells& cells) {
+    if (cells.empty()) return;
+    fmm_b200_solver* s = ctx_.get();
+    ctx_.check(fmm_b200_downward_pass(s));
+    Bodies& bodies = *ctx_.bodies;
+    const int n = (int)bodies.size();
+    std::vector<double> trg(4 * (size_t)n);
+    std::vector<int> order(n);
+    if (n) {
+      ctx_.check(fmm_b200_get_trg_host(s, trg.data()));  // caller (pre-sort) order
+      ctx_.check(fmm_b200_get_order(s, order.data()));
+    }
+    for (int b = 0; b < n; b++)
+      for (int d = 0; d < 4; d++) bodies[b].TRG[d] = trg[4 * (size_t)order[b] + d];
+    cells = BuildTree::fetch_cells(ctx_, bodies, true, true);
+  }
+
+ private:
+  Context& ctx_;
+};
+
+// Traversal (include/traversal.h:214-337); images = 0, mutual = false only.
+class Traversal {
+ public:
+  Traversal(int nspawn, int images, real_t eps2, Context& ctx = Context::global()) : ctx_(ctx) {
+    ctx_.cfg.nspawn = nspawn;
+    ctx_.cfg.images = images;
+    ctx_.cfg.eps2 = (double)(int)eps2;  // the reference stores eps2 as const int (:17)
+  }
+  void dualTreeTraversal(Cells& icells, Cells& jcells, real_t cycle, bool mutual,
+                         real_t remote = 1) {
+    (void)jcells;
+    (void)cycle;
+    (void)remote;
+    if (mutual) throw Error(FMM_ERR_NOT_SUPPORTED, "mutual traversal is not supported");
+    if (icells.empty()) return;
+    ctx_.check(fmm_b200_traverse(ctx_.get()));
+  }
+  // direct sum on the GPU in FP64: TRG of ibodies += contributions of jbodies
+  // (times the target's own charge, as kernel::P2P leaves it before normalize)
+  void direct(Bodies& ibodies, Bodies& jbodies, real_t cycle) {
+    (void)cycle;
+    const int nt = (int)ibodies.size(), ns = (int)jbodies.size();
+    std::vector<double> xt(3 * (size_t)nt), xs(3 * (size_t)ns), qs(ns), out(4 * (size_t)nt);
+    for (int i = 0; i < nt; i++)
+      for (int d = 0; d < 3; d++) xt[3 * i + d] = ibodies[i].X[d];
+    for (int j = 0; j < ns; j++) {
+      for (int d = 0; d < 3; d++) xs[3 * j + d] = jbodies[j].X[d];
+      qs[j] = jbodies[j].SRC;
+    }
+    int rc = fmm_b200_direct(ctx_.cfg.device, nt, xt.data(), ns, xs.data(), qs.data(),
+                             (double)(int)ctx_.cfg.eps2, out.data());
+    if (rc != FMM_OK) throw Error(rc, "direct sum failed");
+    for (int i = 0; i < nt; i++)
+      for (int d = 0; d < 4; d++) ibodies[i].TRG[d] += ibodies[i].SRC * out[4 * (size_t)i + d];
+  }
+  void normalize(Bodies& bodies) {  // include/traversal.h:333-337
+    for (Body& B : bodies)
+      for (int d = 0; d < 4; d++) B.TRG[d] /= B.SRC;
+  }
+  void printTraversalData() {}
+
+ private:
+  Context& ctx_;
+};
+
+// Verify (include/verify.h:18-83)
+struct Verify {
+  double getDifScalar(const Bodies& a, const Bodies& b) const {
+    double v = 0;
+    for (size_t i = 0; i < a.size(); i++) v += (a[i].TRG[0] - b[i].TRG[0]) * (a[i].TRG[0] - b[i].TRG[0]);
+    return v;
+  }
+  double getNrmScalar(const Bodies& a) const {
+    double v = 0;
+    for (const Body& B : a) v += B.TRG[0] * B.TRG[0];
+    return v;
+  }
+  double getDifVector(const Bodies& a, const Bodies& b) const {
+    double v = 0;
+    for (size_t i = 0; i < a.size(); i++)
+      for (int d = 1; d < 4; d++) v += (a[i].TRG[d] - b[i].TRG[d]) * (a[i].TRG[d] - b[i].TRG[d]);
+    return v;
+  }
+  double getNrmVector(const Bodies& a) const {
+    double v = 0;
+    for (const Body& B : a)
+      for (int d = 1; d < 4; d++) v += B.TRG[d] * B.TRG[d];
+    return v;
+  }
+};
+
+}  // namespace exafmm_b200

@@ -1155,3 +1155,99 @@ double oracle_kernel_chain(int basis, int P, int mass, long seed) {
   oracle_free(o);
   return sqrt(diff / norm);
 }
+
+/* ------------------------------------------------------------------ single operators */
+/* One kernel::P2M / M2M / M2L / L2L / L2P application (include/kernel.h:6-14) on cells set
+ * up by hand, as examples/kernel.cxx does; expansions as ncoef doubles, accumulating into
+ * the output.  Unnormalised (non-MASS) multipoles. */
+static Oracle* op_setup(int basis, int P, int nb, const double* xq) {
+  double zx[3] = {0, 0, 0}, zq[1] = {1};
+  double* x = nb ? (double*)malloc(sizeof(double) * 3 * nb) : zx;
+  double* q = nb ? (double*)malloc(sizeof(double) * nb) : zq;
+  for (int b = 0; b < nb; b++) {
+    for (int d = 0; d < 3; d++) x[3 * b + d] = xq[4 * b + d];
+    q[b] = xq[4 * b + 3];
+  }
+  oracle_params prm = {basis, P, 0.5, 16, 1000, 0, 0, 0, 0, 0.0};
+  Oracle* o = (Oracle*)oracle_new(nb, x, q, &prm);
+  if (nb) { free(x); free(q); }
+  o->nc = 2;
+  o->iparent = (int*)calloc(2, sizeof(int));
+  o->ichild = (int*)calloc(2, sizeof(int));
+  o->nchild = (int*)calloc(2, sizeof(int));
+  o->cibody = (int*)calloc(2, sizeof(int));
+  o->cnbody = (int*)calloc(2, sizeof(int));
+  o->cX = (real*)calloc(6, sizeof(real));
+  o->M = (real*)calloc(2 * o->ncoef, sizeof(real));
+  o->L = (real*)calloc(2 * o->ncoef, sizeof(real));
+  o->cnbody[0] = nb;
+  return o;
+}
+static void op_set(Oracle* o, int c, const double* X, const double* M, const double* L) {
+  for (int d = 0; d < 3; d++) o->cX[3 * c + d] = (real)X[d];
+  for (int i = 0; i < o->ncoef; i++) {
+    if (M) o->M[(size_t)c * o->ncoef + i] = (real)M[i];
+    if (L) o->L[(size_t)c * o->ncoef + i] = (real)L[i];
+  }
+}
+static void op_get(Oracle* o, const real* src, double* out) {
+  for (int i = 0; i < o->ncoef; i++) out[i] += src[i];
+}
+
+void oracle_op_m2l(int basis, int P, const double* Xi, const double* Xj, const double* Mj,
+                   double* Li) {
+  Oracle* o = op_setup(basis, P, 0, NULL);
+  op_set(o, 0, Xi, NULL, NULL);
+  op_set(o, 1, Xj, Mj, NULL);
+  if (basis == ORACLE_SPHERICAL) sph_m2l(o, 0, 1); else cart_m2l(o, 0, 1);
+  op_get(o, o->L, Li);
+  oracle_free(o);
+}
+
+void oracle_op_m2m(int basis, int P, const double* Xp, const double* Xc, const double* Mc,
+                   double* Mp) {
+  Oracle* o = op_setup(basis, P, 0, NULL);
+  op_set(o, 0, Xp, NULL, NULL);
+  op_set(o, 1, Xc, Mc, NULL);
+  o->ichild[0] = 1;
+  o->nchild[0] = 1;
+  if (basis == ORACLE_SPHERICAL) sph_m2m(o, 0); else cart_m2m(o, 0);
+  op_get(o, o->M, Mp);
+  oracle_free(o);
+}
+
+void oracle_op_l2l(int basis, int P, const double* Xc, const double* Xp, const double* Lp,
+                   double* Lc) {
+  Oracle* o = op_setup(basis, P, 0, NULL);
+  op_set(o, 0, Xc, NULL, NULL);
+  op_set(o, 1, Xp, NULL, Lp);
+  o->iparent[0] = 1;
+  if (basis == ORACLE_SPHERICAL) sph_l2l(o, 0); else cart_l2l(o, 0);
+  op_get(o, o->L, Lc);
+  oracle_free(o);
+}
+
+void oracle_op_p2m(int basis, int P, const double* Xc, int nb, const double* xq, double* M) {
+  Oracle* o = op_setup(basis, P, nb, xq);
+  op_set(o, 0, Xc, NULL, NULL);
+  if (basis == ORACLE_SPHERICAL) sph_p2m(o, 0); else cart_p2m(o, 0);
+  op_get(o, o->M, M);
+  oracle_free(o);
+}
+
+/* potential and gradient of the local expansion L at the bodies (unit charges) */
+void oracle_op_l2p(int basis, int P, const double* Xc, const double* L, int nb,
+                   const double* x, double* trg) {
+  double* xq = (double*)malloc(sizeof(double) * 4 * (nb ? nb : 1));
+  for (int b = 0; b < nb; b++) {
+    for (int d = 0; d < 3; d++) xq[4 * b + d] = x[3 * b + d];
+    xq[4 * b + 3] = 1;
+  }
+  Oracle* o = op_setup(basis, P, nb, xq);
+  free(xq);
+  op_set(o, 0, Xc, NULL, L);
+  if (basis == ORACLE_SPHERICAL) sph_l2p(o, 0); else cart_l2p(o, 0);
+  for (int b = 0; b < nb; b++)
+    for (int d = 0; d < 4; d++) trg[4 * b + d] = o->trg[4 * b + d];
+  oracle_free(o);
+}

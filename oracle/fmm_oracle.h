@@ -65,6 +65,18 @@ void oracle_rel_l2(int n, const double* trg, const double* ref, double* pot_acc)
 double oracle_kernel_chain(int basis, int P, int mass, long seed);
 int oracle_real_bytes(void);
 
+/* single operators (include/kernel.h:6-14) on hand-made cells, accumulating outputs;
+ * expansions as ncoef doubles (2 NTERM spherical, NTERM Cartesian), unnormalised */
+void oracle_op_m2l(int basis, int P, const double* Xi, const double* Xj, const double* Mj,
+                   double* Li);
+void oracle_op_m2m(int basis, int P, const double* Xp, const double* Xc, const double* Mc,
+                   double* Mp);
+void oracle_op_l2l(int basis, int P, const double* Xc, const double* Xp, const double* Lp,
+                   double* Lc);
+void oracle_op_p2m(int basis, int P, const double* Xc, int nb, const double* xq, double* M);
+void oracle_op_l2p(int basis, int P, const double* Xc, const double* L, int nb,
+                   const double* x, double* trg);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,10 @@ template <typename T> struct V4;
 template <> struct V4<float> { using type = float4; };
 template <> struct V4<double> { using type = double4; };
 template <typename T> using vec4 = typename V4<T>::type;
+template <typename T> struct V2;
+template <> struct V2<float> { using type = float2; };
+template <> struct V2<double> { using type = double2; };
+template <typename T> using vec2 = typename V2<T>::type;
 
 template <typename T> __host__ __device__ __forceinline__ vec4<T> make_v4(T a, T b, T c, T d) {
   vec4<T> v;

@@ -124,17 +124,20 @@ __host__ __device__ __forceinline__ void local(const Angles<T>& a, T* yr, T* yi)
 }
 
 // M2L of one source multipole into a register local expansion (:149-191, mutual = false,
-// unnormalised multipoles).  Mj holds NT (re, im) pairs.
-template <typename T, int P>
+// unnormalised multipoles), for the output degrees j in [J0, J1) only (the FP32 kernel
+// splits the outputs into passes).  Mj holds NT (re, im) pairs.  The loop bounds are
+// compile-time after unrolling, so the whole contraction resolves to register operands.
+template <typename T, int P, int J0 = 0, int J1 = P>
 __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, const T* Mj, T* Lr,
                                                   T* Li) {
 #pragma unroll
-  for (int n = 0; n < P; n++) {
+  for (int n = 0; n < P - J0; n++) {
 #pragma unroll
     for (int mu = 0; mu <= n; mu++) {
       const T mr = Mj[2 * sidx(n, mu)], mi = Mj[2 * sidx(n, mu) + 1];
 #pragma unroll
-      for (int j = 0; j < P - n; j++) {
+      for (int j = J0; j < J1; j++) {
+        if (j + n >= P) break;
         const int a = j + n;
 #pragma unroll
         for (int k = 0; k <= j; k++) {
@@ -183,48 +186,54 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, cons
   }
 }
 
-// Y[a, b] for any sign of b from an interleaved (re, im) m >= 0 store
+// Y[a, b] for any sign of b from the m >= 0 store (real parts yr, imaginary parts yi)
 template <typename T>
-__host__ __device__ __forceinline__ void yget(const T* y, int a, int b, T& r, T& i) {
+__host__ __device__ __forceinline__ void yget(const T* yr, const T* yi, int a, int b, T& r,
+                                              T& i) {
   if (b >= 0) {
-    r = y[2 * sidx(a, b)];
-    i = y[2 * sidx(a, b) + 1];
+    r = yr[sidx(a, b)];
+    i = yi[sidx(a, b)];
   } else {
-    r = y[2 * sidx(a, -b)];
-    i = -y[2 * sidx(a, -b) + 1];
+    r = yr[sidx(a, -b)];
+    i = -yi[sidx(a, -b)];
   }
 }
 
-// M2M output coefficient (j, k) from one child (:127-144); Y from multipole() at
-// Xparent - Xchild as interleaved (re, im) pairs, Mc the child's NT (re, im) pairs.
-// Runtime indices (shared memory).
+// M2M output coefficient (j, k) from one child (:127-144); Y (yr, yi) from multipole() at
+// Xparent - Xchild, Mc the child's NT (re, im) pairs.  Runtime indices when (j, k) are
+// runtime values, register operands when they are unrolled constants.
 template <typename T>
-__host__ __device__ __forceinline__ void m2m_term(int j, int k, const T* y, const T* Mc,
-                                                  T& outr, T& outi) {
+__host__ __device__ __forceinline__ void m2m_term(int j, int k, const T* yr, const T* yi,
+                                                  const T* Mc, T& outr, T& outi) {
   T sr = 0, si = 0;
+#pragma unroll
   for (int n = 0; n <= j; n++) {
-    int mlo = -n > -j + k + n ? -n : -j + k + n;
-    int mhi = k - 1 < n ? k - 1 : n;
-    for (int m = mlo; m <= mhi; m++) {
+    // m in [max(-n, -j+k+n), min(k-1, n)]
+#pragma unroll
+    for (int m = -n; m <= n; m++) {
+      if (m < -j + k + n) continue;
+      if (m > k - 1) break;
       // Cj->M[(j-n)(j-n+1)/2 + k - m] * Ynm[n*n+n-m] * IPOW2N(m) * ODDEVEN(n)
-      int q = (j - n) * (j - n + 1) / 2 + k - m;
-      T Mr = Mc[2 * q], Mi = Mc[2 * q + 1];
+      const int q = (j - n) * (j - n + 1) / 2 + k - m;
+      const T Mr = Mc[2 * q], Mi = Mc[2 * q + 1];
       T ur, ui;
-      yget(y, n, -m, ur, ui);
-      T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
-      int sgn = ((m < 0 && (m & 1)) ? -1 : 1) * ((n & 1) ? -1 : 1);
+      yget(yr, yi, n, -m, ur, ui);
+      const T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
+      const int sgn = ((m < 0 && (m & 1)) ? -1 : 1) * ((n & 1) ? -1 : 1);
       sr += sgn * pr;
       si += sgn * pi;
     }
-    int mhi2 = n < j + k - n ? n : j + k - n;
-    for (int m = k; m <= mhi2; m++) {
+    // m in [k, min(n, j+k-n)]
+#pragma unroll
+    for (int m = k; m <= n; m++) {
+      if (m > j + k - n) break;
       // conj(Cj->M[(j-n)(j-n+1)/2 - k + m]) * Ynm[n*n+n-m] * ODDEVEN(k+n+m)
-      int q = (j - n) * (j - n + 1) / 2 - k + m;
-      T Mr = Mc[2 * q], Mi = -Mc[2 * q + 1];
+      const int q = (j - n) * (j - n + 1) / 2 - k + m;
+      const T Mr = Mc[2 * q], Mi = -Mc[2 * q + 1];
       T ur, ui;
-      yget(y, n, -m, ur, ui);
-      T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
-      int sgn = ((k + n + m) & 1) ? -1 : 1;
+      yget(yr, yi, n, -m, ur, ui);
+      const T pr = Mr * ur - Mi * ui, pi = Mr * ui + Mi * ur;
+      const int sgn = ((k + n + m) & 1) ? -1 : 1;
       sr += sgn * pr;
       si += sgn * pi;
     }
@@ -233,41 +242,74 @@ __host__ __device__ __forceinline__ void m2m_term(int j, int k, const T* y, cons
   outi = si;
 }
 
-// L2L output coefficient (j, k) from the parent (:203-222); Y from multipole() at
-// Xchild - Xparent as interleaved (re, im) pairs, Lp the parent's NT (re, im) pairs.
+// L2L output coefficient (j, k) from the parent (:203-222); Y (yr, yi) from multipole() at
+// Xchild - Xparent, Lp the parent's NT (re, im) pairs.
 template <typename T>
-__host__ __device__ __forceinline__ void l2l_term(int P, int j, int k, const T* y,
-                                                  const T* Lp, T& outr, T& outi) {
+__host__ __device__ __forceinline__ void l2l_term(int P, int j, int k, const T* yr,
+                                                  const T* yi, const T* Lp, T& outr, T& outi) {
   T sr = 0, si = 0;
+#pragma unroll
   for (int n = j; n < P; n++) {
-    for (int m = j + k - n; m < 0; m++) {
+    // m in [j+k-n, -1]
+#pragma unroll
+    for (int m = -n; m < 0; m++) {
+      if (m < j + k - n) continue;
       // conj(Cj->L[n(n+1)/2 - m]) * Ynm[(n-j)^2 + n-j + m-k] * ODDEVEN(k)
-      int q = n * (n + 1) / 2 - m;
-      T Lr = Lp[2 * q], Li = -Lp[2 * q + 1];
+      const int q = n * (n + 1) / 2 - m;
+      const T Lr = Lp[2 * q], Li = -Lp[2 * q + 1];
       T ur, ui;
-      yget(y, n - j, m - k, ur, ui);
-      T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
-      int sgn = (k & 1) ? -1 : 1;
+      yget(yr, yi, n - j, m - k, ur, ui);
+      const T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
+      const int sgn = (k & 1) ? -1 : 1;
       sr += sgn * pr;
       si += sgn * pi;
     }
+#pragma unroll
     for (int m = 0; m <= n; m++) {
-      int d = m - k;
-      if (n - j >= (d < 0 ? -d : d)) {
-        // Cj->L[n(n+1)/2 + m] * Ynm[(n-j)^2 + n-j + m-k] * ODDEVEN((m-k)(m<k))
-        int q = n * (n + 1) / 2 + m;
-        T Lr = Lp[2 * q], Li = Lp[2 * q + 1];
-        T ur, ui;
-        yget(y, n - j, d, ur, ui);
-        T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
-        int sgn = (d < 0 && (d & 1)) ? -1 : 1;
-        sr += sgn * pr;
-        si += sgn * pi;
-      }
+      const int d = m - k;
+      if (n - j < (d < 0 ? -d : d)) continue;
+      // Cj->L[n(n+1)/2 + m] * Ynm[(n-j)^2 + n-j + m-k] * ODDEVEN((m-k)(m<k))
+      const int q = n * (n + 1) / 2 + m;
+      const T Lr = Lp[2 * q], Li = Lp[2 * q + 1];
+      T ur, ui;
+      yget(yr, yi, n - j, d, ur, ui);
+      const T pr = Lr * ur - Li * ui, pi = Lr * ui + Li * ur;
+      const int sgn = (d < 0 && (d & 1)) ? -1 : 1;
+      sr += sgn * pr;
+      si += sgn * pi;
     }
   }
   outr = sr;
   outi = si;
+}
+
+// Whole M2M / L2L translations for the output degrees j in [J0, J1) with compile-time
+// indices (register operands); out[t - sidx(J0, 0)] holds output t as (re, im).
+template <typename T, int P, int J0 = 0, int J1 = P>
+__host__ __device__ __forceinline__ void m2m_range(const T* yr, const T* yi, const T* Mc,
+                                                   T* out) {
+#pragma unroll
+  for (int j = J0; j < J1; j++)
+#pragma unroll
+    for (int k = 0; k <= j; k++) {
+      T r, i;
+      m2m_term<T>(j, k, yr, yi, Mc, r, i);
+      out[2 * (sidx(j, k) - sidx(J0, 0))] += r;
+      out[2 * (sidx(j, k) - sidx(J0, 0)) + 1] += i;
+    }
+}
+template <typename T, int P, int J0 = 0, int J1 = P>
+__host__ __device__ __forceinline__ void l2l_range(const T* yr, const T* yi, const T* Lp,
+                                                   T* out) {
+#pragma unroll
+  for (int j = J0; j < J1; j++)
+#pragma unroll
+    for (int k = 0; k <= j; k++) {
+      T r, i;
+      l2l_term<T>(P, j, k, yr, yi, Lp, r, i);
+      out[2 * (sidx(j, k) - sidx(J0, 0))] += r;
+      out[2 * (sidx(j, k) - sidx(J0, 0)) + 1] += i;
+    }
 }
 
 // L2P of one body (:226-256): potential and gradient of the local expansion L (NT (re, im)

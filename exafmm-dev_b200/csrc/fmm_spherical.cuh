@@ -99,8 +99,8 @@ __device__ __forceinline__ void spread_y(const T* yr, const T* yi, T* sy, int la
 #pragma unroll
   for (int t = 0; t < NT; t++)
     if ((t & 31) == lane) {
-      sy[2 * t] = yr[t];
-      sy[2 * t + 1] = yi[t];
+      sy[t] = yr[t];
+      sy[NT + t] = yi[t];
     }
 }
 
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     for (int i = 0; i < KO; i++) {
       if (lane + 32 * i < NT) {
         T r, im;
-        sph::m2m_term<T>(oj[i], ok[i], sy[wl], sm[wl], r, im);
+        sph::m2m_term<T>(oj[i], ok[i], sy[wl], sy[wl] + NT, sm[wl], r, im);
         ar[i] += r;
         ai[i] += im;
       }
@@ -181,10 +181,141 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
   }
 }
 
-// ---------------------------------------------------------------- M2L
-// FP32: lane per source, Y and L in registers.
+// output degrees per FP32 M2M / L2L pass: at most 24 complex outputs per pass
+__host__ __device__ constexpr int tr_pass_end(int P, int J0) {
+  int j = J0 + 1;
+  while (j < P && sph::NT(j + 1) - sph::NT(J0) <= 24) j++;
+  return j;
+}
+
+// M2M passes for one child lane; outputs summed over the 8-lane group and written.
+template <typename T, int P, int J0>
+__device__ __forceinline__ void m2m_passes(const T* yr, const T* yi, const T* Mc, bool has,
+                                           int slot, T* Mp, T m0) {
+  if constexpr (J0 < P) {
+    constexpr int J1 = tr_pass_end(P, J0);
+    constexpr int NO = 2 * (sph::sidx(J1, 0) - sph::sidx(J0, 0));
+    T acc[NO];
+#pragma unroll
+    for (int t = 0; t < NO; t++) acc[t] = 0;
+    if (has) sph::m2m_range<T, P, J0, J1>(yr, yi, Mc, acc);
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+      for (int t = 0; t < NO; t++) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], o);
+    if (J0 == 0) acc[0] = m0;
+    if (Mp) {
+#pragma unroll
+      for (int t = 0; t < NO; t++)
+        if ((t & 7) == slot) Mp[2 * sph::sidx(J0, 0) + t] = acc[t];
+    }
+    m2m_passes<T, P, J1>(yr, yi, Mc, has, slot, Mp, m0);
+  }
+}
+
+// FP32 M2M: 8 lanes per parent (one per child slot), 4 parents per warp; each lane
+// translates its child with compile-time indices, the group sums in a fixed order, and the
+// monopole is re-summed in child order (the reference's sequence) so that the radii of the
+// error-optimised MAC see the same M[0] bits.
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
+    k_m2m_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
+              const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
+              int ncoef, int use_rmax, T theta) {
+  constexpr int NT = sph::NT(P);
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = lo + (gt >> 3);
+  const int slot = gt & 7;
+  int c = 0, nch = 0, c0 = 0;
+  if (v < hi) {
+    c = npos[v];
+    nch = nchild[c];
+    c0 = ichild[c];
+  }
+  const bool has = slot < nch;
+  T rr = 0;
+  vec4<T> Xp = make_v4<T>(0, 0, 0, 0);
+  if (v < hi) Xp = cX[c];
+  T yr[NT], yi[NT];
+  const T* Mc = M;
+  if (has) {
+    const int cc = c0 + slot;
+    const vec4<T> Xc = cX[cc];
+    sph::Angles<T> a = sph::angles(Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
+    sph::multipole<T, P>(a, a.r, yr, yi);
+    Mc = M + (size_t)cc * ncoef;
+    rr = add_rn(sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z))), Xc.w);
+  }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const T x = __shfl_xor_sync(0xffffffffu, rr, o);
+    rr = x > rr ? x : rr;
+  }
+  T m0 = 0;
+  if (slot == 0)
+    for (int k = 0; k < nch; k++) m0 = add_rn(m0, M[(size_t)(c0 + k) * ncoef]);
+  const bool write = v < hi && nch > 0;
+  m2m_passes<T, P, 0>(yr, yi, Mc, has, slot, write ? M + (size_t)c * ncoef : nullptr, m0);
+  if (write && slot == 0) {
+    T R = Xp.w;
+    if (use_rmax) R = rr < R ? rr : R;
+    cX[c].w = div_rn(R, theta);
+  }
+}
+
+template <typename T, int P, int J0>
+__device__ __forceinline__ void l2l_passes(const T* yr, const T* yi, const T* Lp, T* Lc) {
+  if constexpr (J0 < P) {
+    constexpr int J1 = tr_pass_end(P, J0);
+    constexpr int NO = 2 * (sph::sidx(J1, 0) - sph::sidx(J0, 0));
+    T acc[NO];
+#pragma unroll
+    for (int t = 0; t < NO; t++) acc[t] = Lc[2 * sph::sidx(J0, 0) + t];
+    sph::l2l_range<T, P, J0, J1>(yr, yi, Lp, acc);
+#pragma unroll
+    for (int t = 0; t < NO; t++) Lc[2 * sph::sidx(J0, 0) + t] = acc[t];
+    l2l_passes<T, P, J1>(yr, yi, Lp, Lc);
+  }
+}
+
+// FP32 L2L: thread per cell, compile-time indices.
+template <typename T, int P>
+__global__ void __launch_bounds__(128)
+    k_l2l_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
+              const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
+  constexpr int NT = sph::NT(P);
+  const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= hi) return;
+  const int c = npos[v];
+  const int p = iparent[c];
+  const vec4<T> Xc = cX[c], Xp = cX[p];
+  T yr[NT], yi[NT];
+  sph::Angles<T> a = sph::angles(Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
+  sph::multipole<T, P>(a, a.r, yr, yi);
+  l2l_passes<T, P, 0>(yr, yi, L + (size_t)p * ncoef, L + (size_t)c * ncoef);
+}
+
+// ---------------------------------------------------------------- M2L
+// FP32: warp per target, lane per source cell, harmonics and local expansion in registers,
+// one warp reduction per target cell at the end.  The outputs are split into passes over
+// their degree (separate launches) so that each unrolled contraction stays small: the
+// kernel is bound by instruction fetch when one pass holds all of P = 10.
+constexpr int kM2LWarps = 4;
+// output degrees per FP32 M2L pass: add degrees while the pass stays under ~600 complex
+// multiply-adds (the unrolled code of one pass, and its registers, stay moderate)
+__host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
+  int cost = 0, j = J0;
+  while (j < P) {
+    const int c = (j + 1) * (P - j) * (P - j);
+    if (j > J0 && cost + c > 600) break;
+    cost += c;
+    j++;
+  }
+  return j;
+}
+
+template <typename T, int P, int J0, int J1>
+__global__ void __launch_bounds__(32 * kM2LWarps)
     k_m2l_reg(int ncells, const int* __restrict__ off, const unsigned long long* __restrict__ pairs,
               const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L,
               int ncoef) {
@@ -204,10 +335,10 @@ __global__ void __launch_bounds__(128)
     T yr[NT], yi[NT];
     sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
     sph::local<T, P>(a, yr, yi);
-    sph::m2l_pair<T, P>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
+    sph::m2l_pair<T, P, J0, J1>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
   }
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
+  for (int t = sph::sidx(J0, 0); t < sph::sidx(J1, 0); t++) {
     const T r = warp_sum(Lr[t]);
     const T i = warp_sum(Li[t]);
     if (lane == (t & 31)) {
@@ -217,16 +348,28 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+template <typename T, int P, int J0>
+static void launch_m2l_passes(Solver<T>& s) {
+  if constexpr (J0 < P) {
+    constexpr int J1 = m2l_pass_end(P, J0);
+    k_m2l_reg<T, P, J0, J1><<<ceil_div(s.ncells, kM2LWarps), 32 * kM2LWarps, 0, s.stream>>>(
+        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+    launch_m2l_passes<T, P, J1>(s);
+  }
+}
+
 // M2L output coefficient (j, k) from one source (:156-189), runtime indices
 template <typename T>
 __device__ __forceinline__ void m2l_term(int P, int j, int k, const T* y, const T* Mj, T& outr,
                                          T& outi) {
+  const int NTy = P * (P + 1) / 2;  // y holds NT real parts, then NT imaginary parts
   T sr = 0, si = 0;
   for (int n = 0; n < P - j; n++) {
     const int a = j + n;
     for (int mu = 1; mu <= n; mu++) {
       const T mr = Mj[2 * sph::sidx(n, mu)], mi = Mj[2 * sph::sidx(n, mu) + 1];
-      const T ur = y[2 * sph::sidx(a, k + mu)], ui = y[2 * sph::sidx(a, k + mu) + 1];
+      const T ur = y[sph::sidx(a, k + mu)], ui = y[NTy + sph::sidx(a, k + mu)];
       sr += mr * ur - mi * ui;
       si -= mr * ui + mi * ur;
     }
@@ -234,11 +377,11 @@ __device__ __forceinline__ void m2l_term(int P, int j, int k, const T* y, const 
       const T mr = Mj[2 * sph::sidx(n, m)], mi = Mj[2 * sph::sidx(n, m) + 1];
       T vr, vi;
       if (m >= k) {
-        const T wr = y[2 * sph::sidx(a, m - k)], wi = y[2 * sph::sidx(a, m - k) + 1];
+        const T wr = y[sph::sidx(a, m - k)], wi = y[NTy + sph::sidx(a, m - k)];
         vr = mr * wr - mi * wi;
         vi = mr * wi + mi * wr;
       } else {
-        const T wr = y[2 * sph::sidx(a, k - m)], wi = y[2 * sph::sidx(a, k - m) + 1];
+        const T wr = y[sph::sidx(a, k - m)], wi = y[NTy + sph::sidx(a, k - m)];
         vr = mr * wr + mi * wi;
         vi = mi * wr - mr * wi;
       }
@@ -344,7 +487,7 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
       int j, k;
       jk_of(t, j, k);
       T r, im;
-      sph::l2l_term<T>(P, j, k, sy[wl], sl[wl], r, im);
+      sph::l2l_term<T>(P, j, k, sy[wl], sy[wl] + NT, sl[wl], r, im);
       L[(size_t)c * ncoef + 2 * t] += r;
       L[(size_t)c * ncoef + 2 * t + 1] += im;
     }
@@ -394,17 +537,22 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
-  constexpr int W = SphCfg<T>::W;
-  k_m2m<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(
-      lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
-      (T)s.cfg.theta);
-  FMM_LAUNCH_CHECK();
+  if constexpr (sizeof(T) == 4) {
+    k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), 128), 128, 0, s.stream>>>(
+        lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
+        (T)s.cfg.theta);
+    FMM_LAUNCH_CHECK();
+  } else {
+    constexpr int W = SphCfg<T>::W;
+    k_m2m<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(
+        lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
+        (T)s.cfg.theta);
+    FMM_LAUNCH_CHECK();
+  }
 }
 template <typename T, int P> static void m2l_(Solver<T>& s) {
   if constexpr (sizeof(T) == 4) {
-    k_m2l_reg<T, P><<<ceil_div(s.ncells, 4), 128, 0, s.stream>>>(
-        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
-    FMM_LAUNCH_CHECK();
+    launch_m2l_passes<T, P, 0>(s);
   } else {
     constexpr int W = SphCfg<T>::W;
     k_m2l_lanes<T, P><<<ceil_div(s.ncells, W), 32 * W, 0, s.stream>>>(
@@ -413,10 +561,16 @@ template <typename T, int P> static void m2l_(Solver<T>& s) {
   }
 }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
-  constexpr int W = SphCfg<T>::W;
-  k_l2l<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
-                                                              s.cX.p, s.L.p, s.ncoef);
-  FMM_LAUNCH_CHECK();
+  if constexpr (sizeof(T) == 4) {
+    k_l2l_reg<T, P><<<ceil_div(hi - lo, 128), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
+                                                                  s.cX.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+  } else {
+    constexpr int W = SphCfg<T>::W;
+    k_l2l<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
+                                                                s.cX.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+  }
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   constexpr int W = SphCfg<T>::W;

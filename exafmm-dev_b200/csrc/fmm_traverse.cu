@@ -72,8 +72,25 @@ __global__ void k_trav_count(const int2* __restrict__ front, int nfront,
   }
 }
 
-// pass 2: write.  Output slots come from atomics (the final lists are sorted afterwards, so
-// their order does not depend on scheduling).
+// pass 2: write.  Output slots come from one atomic per warp and output kind (the lanes'
+// offsets from a warp prefix sum); the final lists are sorted afterwards, so their order
+// does not depend on scheduling.
+__device__ __forceinline__ unsigned long long warp_alloc(unsigned long long* counter,
+                                                         unsigned k) {
+  const int lane = lane_id();
+  unsigned incl = k;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total) base = atomicAdd(counter, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + (incl - k);
+}
+
 template <typename T>
 __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
@@ -81,28 +98,36 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
                              int nspawn, unsigned long long* __restrict__ counters,
                              unsigned long long* __restrict__ m2l,
                              unsigned long long* __restrict__ p2p, int2* __restrict__ next) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
-    int2 p = front[t];
-    int k;
-    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
-    unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+  const int stride = gridDim.x * blockDim.x;
+  // every lane of a warp runs the same number of iterations (warp-uniform trip count)
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int wbase = t0 - lane_id();
+  for (int w = wbase; w < nfront; w += stride) {
+    const int t = w + lane_id();
+    int ty = -1, k = 0;
+    int2 p = make_int2(0, 0);
+    if (t < nfront) {
+      p = front[t];
+      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+    }
+    const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+    const unsigned long long om = warp_alloc(&counters[0], ty == PAIR_M2L ? 1u : 0u);
+    const unsigned long long op = warp_alloc(&counters[1], ty == PAIR_P2P ? 1u : 0u);
+    const unsigned long long o = warp_alloc(&counters[2], ty >= PAIR_SPLIT_I ? (unsigned)k : 0u);
     if (ty == PAIR_M2L) {
-      m2l[atomicAdd(&counters[0], 1ULL)] = packed;
+      m2l[om] = packed;
     } else if (ty == PAIR_P2P) {
-      p2p[atomicAdd(&counters[1], 1ULL)] = packed;
-    } else {
-      unsigned long long o = atomicAdd(&counters[2], (unsigned long long)k);
-      if (ty == PAIR_SPLIT_I) {
-        int c0 = ichild[p.x];
-        for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
-      } else if (ty == PAIR_SPLIT_J) {
-        int c0 = ichild[p.y];
-        for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, c0 + j);
-      } else {
-        int ci0 = ichild[p.x], cj0 = ichild[p.y];
-        int nj = nchild[p.y];
-        for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
-      }
+      p2p[op] = packed;
+    } else if (ty == PAIR_SPLIT_I) {
+      int c0 = ichild[p.x];
+      for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
+    } else if (ty == PAIR_SPLIT_J) {
+      int c0 = ichild[p.y];
+      for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, c0 + j);
+    } else if (ty == PAIR_SPLIT_IJ) {
+      int ci0 = ichild[p.x], cj0 = ichild[p.y];
+      int nj = nchild[p.y];
+      for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
     }
   }
 }
@@ -134,6 +159,16 @@ __global__ void k_p2p_bodypairs(const unsigned long long* __restrict__ pairs, lo
   }
   s = warp_sum(s);
   if (lane_id() == 0 && s) atomicAdd(out, s);
+}
+
+// (target << 32 | source) <-> (target << b | source)
+__global__ void k_pack_pairs(unsigned long long* __restrict__ a, long long n, int b, int pack) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long v = a[t];
+    if (pack) a[t] = ((v >> 32) << b) | (v & 0xffffffffULL);
+    else a[t] = ((v >> b) << 32) | (v & ((1ULL << b) - 1));
+  }
 }
 
 static int bits_for(int n) {
@@ -196,13 +231,22 @@ template <typename T> void build_lists(Solver<T>& s) {
   FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
   s.nm2l = nm2l;
   s.np2p = np2p;
-  const int endbit = 32 + bits_for(s.ncells);
+  // sort on (target << b | source) with b = bits(ncells): 2b key bits instead of 32 + b
+  const int b = bits_for(s.ncells);
   s.list_tmp.ensure(std::max<long long>(std::max(nm2l, np2p), 1));
-  sort_keys_u64(s, s.m2l.p, s.list_tmp.p, (int)nm2l, endbit);
-  std::swap(s.m2l, s.list_tmp);
-  s.list_tmp.ensure(std::max<long long>(np2p, 1));
-  sort_keys_u64(s, s.p2p.p, s.list_tmp.p, (int)np2p, endbit);
-  std::swap(s.p2p, s.list_tmp);
+  for (int which = 0; which < 2; which++) {
+    DevArr<unsigned long long>& lst = which ? s.p2p : s.m2l;
+    const long long cnt = which ? np2p : nm2l;
+    if (cnt == 0) continue;
+    const int grid = std::min(ceil_div(cnt, TB), 148 * 16);
+    k_pack_pairs<<<grid, TB, 0, s.stream>>>(lst.p, cnt, b, 1);
+    FMM_LAUNCH_CHECK();
+    s.list_tmp.ensure(cnt);
+    sort_keys_u64(s, lst.p, s.list_tmp.p, (int)cnt, 2 * b);
+    k_pack_pairs<<<grid, TB, 0, s.stream>>>(s.list_tmp.p, cnt, b, 0);
+    FMM_LAUNCH_CHECK();
+    std::swap(lst, s.list_tmp);
+  }
   s.m2l_off.ensure(s.ncells + 1);
   s.p2p_off.ensure(s.ncells + 1);
   k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.m2l.p, nm2l, s.ncells, s.m2l_off.p);

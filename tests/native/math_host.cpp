@@ -15,7 +15,9 @@ template <int P> void sph_m2l(const double* Xi, const double* Xj, const double* 
   double yr[NT], yi[NT], Lr[NT] = {}, Lm[NT] = {};
   sph::Angles<double> a = sph::angles(Xi[0] - Xj[0], Xi[1] - Xj[1], Xi[2] - Xj[2]);
   sph::local<double, P>(a, yr, yi);
-  sph::m2l_pair<double, P>(yr, yi, Mj, Lr, Lm);
+  // two output ranges, as the FP32 kernel's passes split them
+  sph::m2l_pair<double, P, 0, P / 2>(yr, yi, Mj, Lr, Lm);
+  sph::m2l_pair<double, P, P / 2, P>(yr, yi, Mj, Lr, Lm);
   for (int t = 0; t < NT; t++) Li[2 * t] += Lr[t], Li[2 * t + 1] += Lm[t];
 }
 template <int P> void sph_mult(const double* d, double* y) {
@@ -25,26 +27,40 @@ template <int P> void sph_mult(const double* d, double* y) {
   sph::multipole<double, P>(a, a.r, yr, yi);
   for (int t = 0; t < NT; t++) y[2 * t] = yr[t], y[2 * t + 1] = yi[t];
 }
+template <int P> void split(const double* y, double* yr, double* yi) {
+  for (int t = 0; t < sph::NT(P); t++) yr[t] = y[2 * t], yi[t] = y[2 * t + 1];
+}
+// runtime-index terms (the FP64 kernels) and the unrolled ranges (the FP32 kernels) agree
 template <int P> void sph_m2m(const double* Xp, const double* Xc, const double* Mc, double* Mp) {
   double d[3] = {Xp[0] - Xc[0], Xp[1] - Xc[1], Xp[2] - Xc[2]}, y[2 * sph::NT(P)];
+  double yr[sph::NT(P)], yi[sph::NT(P)], rng[2 * sph::NT(P)] = {};
   sph_mult<P>(d, y);
+  split<P>(y, yr, yi);
+  sph::m2m_range<double, P>(yr, yi, Mc, rng);
   for (int j = 0; j < P; j++)
     for (int k = 0; k <= j; k++) {
       double r, i;
-      sph::m2m_term<double>(j, k, y, Mc, r, i);
-      Mp[2 * sph::sidx(j, k)] += r;
-      Mp[2 * sph::sidx(j, k) + 1] += i;
+      sph::m2m_term<double>(j, k, yr, yi, Mc, r, i);
+      const int t = sph::sidx(j, k);
+      Mp[2 * t] += (r + rng[2 * t]) / 2;
+      Mp[2 * t + 1] += (i + rng[2 * t + 1]) / 2;
+      if (r != rng[2 * t] || i != rng[2 * t + 1]) Mp[2 * t] += 1e300;  // must agree exactly
     }
 }
 template <int P> void sph_l2l(const double* Xc, const double* Xp, const double* Lp, double* Lc) {
   double d[3] = {Xc[0] - Xp[0], Xc[1] - Xp[1], Xc[2] - Xp[2]}, y[2 * sph::NT(P)];
+  double yr[sph::NT(P)], yi[sph::NT(P)], rng[2 * sph::NT(P)] = {};
   sph_mult<P>(d, y);
+  split<P>(y, yr, yi);
+  sph::l2l_range<double, P>(yr, yi, Lp, rng);
   for (int j = 0; j < P; j++)
     for (int k = 0; k <= j; k++) {
       double r, i;
-      sph::l2l_term<double>(P, j, k, y, Lp, r, i);
-      Lc[2 * sph::sidx(j, k)] += r;
-      Lc[2 * sph::sidx(j, k) + 1] += i;
+      sph::l2l_term<double>(P, j, k, yr, yi, Lp, r, i);
+      const int t = sph::sidx(j, k);
+      Lc[2 * t] += (r + rng[2 * t]) / 2;
+      Lc[2 * t + 1] += (i + rng[2 * t + 1]) / 2;
+      if (r != rng[2 * t] || i != rng[2 * t + 1]) Lc[2 * t] += 1e300;  // must agree exactly
     }
 }
 template <int P> void sph_p2m(const double* Xc, int nb, const double* xq, double* M) {

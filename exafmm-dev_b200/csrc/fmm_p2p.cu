@@ -3,7 +3,8 @@
 //
 // One warp owns one target leaf.  Its lanes split into groups of G (1, 2 or 4) so that a
 // small leaf still keeps the warp busy: each group holds one target body and its G lanes
-// take every G-th source.  Source leaves stream through shared memory 32 bodies at a time
+// take every G-th source; a leaf of 33..64 bodies gives each lane two targets that share
+// every staged source.  Source leaves stream through shared memory 32 bodies at a time
 // (one coalesced 16-byte load per lane, read back as a broadcast), the inner loop is
 // FP32 FMA + one rsqrt per pair, and each source leaf's plain FP32 partial sum is folded
 // into a compensated (TwoSum) accumulator, so the accumulation error does not grow with
@@ -17,6 +18,108 @@
 namespace fmmb200 {
 
 constexpr int kP2PWarps = 4;
+
+template <typename T>
+__device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, T eps2, T& pot,
+                                          T& ax, T& ay, T& az) {
+  const T dx = sj.x - xi.x, dy = sj.y - xi.y, dz = sj.z - xi.z;
+  const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+  const T inv = r2 > T(0) ? rsqrt_(r2) : T(0);
+  const T qinv = sj.w * inv;
+  const T inv3 = qinv * inv * inv;
+  pot += qinv;
+  ax = fma(dx, inv3, ax);
+  ay = fma(dy, inv3, ay);
+  az = fma(dz, inv3, az);
+}
+
+// TPL targets per lane (1 or 2): a lane holds targets ti and ti + 32 / G and reuses every
+// staged source for both.
+template <typename T, bool COMP, int TPL>
+__device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], int b0, int nb,
+                                         int base, int G, int s0, int s1,
+                                         const unsigned long long* __restrict__ pairs,
+                                         const int* __restrict__ ibody,
+                                         const int* __restrict__ nbody,
+                                         const vec4<T>* __restrict__ bodies, T eps2,
+                                         vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+  const int tpp = 32 / G;
+  const int sub = lane % G;
+  int ti[TPL];
+  bool act[TPL];
+  vec4<T> xi[TPL];
+  Comp<T> acc[TPL][4];
+#pragma unroll
+  for (int u = 0; u < TPL; u++) {
+    ti[u] = base + u * tpp + lane / G;
+    act[u] = ti[u] < nb;
+    xi[u] = act[u] ? bodies[b0 + ti[u]] : make_v4<T>(0, 0, 0, 0);
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[u][d] = Comp<T>{0, 0};
+  }
+  // source leaf s: (first body, count), the next one prefetched
+  int cj = s0 < s1 ? (int)(pairs[s0] & 0xffffffffULL) : 0;
+  int j0 = s0 < s1 ? ibody[cj] : 0, nj = s0 < s1 ? nbody[cj] : 0;
+  for (int s = s0; s < s1; s++) {
+    int j0n = 0, njn = 0;
+    if (s + 1 < s1) {
+      const int cn = (int)(pairs[s + 1] & 0xffffffffULL);
+      j0n = ibody[cn];
+      njn = nbody[cn];
+    }
+    T pot[TPL], ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+    for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
+    for (int jb = 0; jb < nj; jb += 32) {
+      const int cnt = min(32, nj - jb);
+      __syncwarp();
+      if (lane < cnt) sh[wl][lane] = bodies[j0 + jb + lane];
+      __syncwarp();
+#pragma unroll 4
+      for (int k = sub; k < cnt; k += G) {
+        const vec4<T> sj = sh[wl][k];
+#pragma unroll
+        for (int u = 0; u < TPL; u++) p2p_accum(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TPL; u++) {
+      if (COMP) {
+        comp_add(acc[u][0], pot[u]);
+        comp_add(acc[u][1], ax[u]);
+        comp_add(acc[u][2], ay[u]);
+        comp_add(acc[u][3], az[u]);
+      } else {
+        acc[u][0].s += pot[u];
+        acc[u][1].s += ax[u];
+        acc[u][2].s += ay[u];
+        acc[u][3].s += az[u];
+      }
+    }
+    j0 = j0n;
+    nj = njn;
+  }
+  for (int o = 1; o < G; o <<= 1) {
+#pragma unroll
+    for (int u = 0; u < TPL; u++)
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        Comp<T> r;
+        r.s = __shfl_xor_sync(0xffffffffu, acc[u][d].s, o);
+        r.e = __shfl_xor_sync(0xffffffffu, acc[u][d].e, o);
+        if (COMP) comp_merge(acc[u][d], r);
+        else acc[u][d].s += r.s;
+      }
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int u = 0; u < TPL; u++)
+      if (act[u]) {
+        trg_s[b0 + ti[u]] = make_v4<T>(acc[u][0].s, acc[u][1].s, acc[u][2].s, acc[u][3].s);
+        trg_e[b0 + ti[u]] = make_v4<T>(acc[u][0].e, acc[u][1].e, acc[u][2].e, acc[u][3].e);
+      }
+  }
+}
 
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(32 * kP2PWarps)
@@ -32,63 +135,14 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
   const int c = leaves[w];
   const int b0 = ibody[c], nb = nbody[c];
   const int G = nb <= 8 ? 4 : (nb <= 16 ? 2 : 1);
-  const int tpp = 32 / G;
   const int s0 = off[c], s1 = off[c + 1];
-  for (int base = 0; base < nb; base += tpp) {
-    const int ti = base + lane / G;
-    const int sub = lane % G;
-    const bool active = ti < nb;
-    vec4<T> xi = active ? bodies[b0 + ti] : make_v4<T>(0, 0, 0, 0);
-    Comp<T> acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    for (int s = s0; s < s1; s++) {
-      const int cj = (int)(pairs[s] & 0xffffffffULL);
-      const int j0 = ibody[cj], nj = nbody[cj];
-      T pot = 0, ax = 0, ay = 0, az = 0;
-      for (int jb = 0; jb < nj; jb += 32) {
-        const int cnt = min(32, nj - jb);
-        __syncwarp();
-        if (lane < cnt) sh[wl][lane] = bodies[j0 + jb + lane];
-        __syncwarp();
-#pragma unroll 4
-        for (int k = sub; k < cnt; k += G) {
-          const vec4<T> sj = sh[wl][k];
-          const T dx = sj.x - xi.x, dy = sj.y - xi.y, dz = sj.z - xi.z;
-          const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-          const T inv = r2 > T(0) ? rsqrt_(r2) : T(0);
-          const T qinv = sj.w * inv;
-          const T inv3 = qinv * inv * inv;
-          pot += qinv;
-          ax = fma(dx, inv3, ax);
-          ay = fma(dy, inv3, ay);
-          az = fma(dz, inv3, az);
-        }
-      }
-      if (COMP) {
-        comp_add(acc[0], pot);
-        comp_add(acc[1], ax);
-        comp_add(acc[2], ay);
-        comp_add(acc[3], az);
-      } else {
-        acc[0].s += pot;
-        acc[1].s += ax;
-        acc[2].s += ay;
-        acc[3].s += az;
-      }
-    }
-    for (int o = 1; o < G; o <<= 1) {
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        Comp<T> r;
-        r.s = __shfl_xor_sync(0xffffffffu, acc[d].s, o);
-        r.e = __shfl_xor_sync(0xffffffffu, acc[d].e, o);
-        if (COMP) comp_merge(acc[d], r);
-        else acc[d].s += r.s;
-      }
-    }
-    if (active && sub == 0) {
-      trg_s[b0 + ti] = make_v4<T>(acc[0].s, acc[1].s, acc[2].s, acc[3].s);
-      trg_e[b0 + ti] = make_v4<T>(acc[0].e, acc[1].e, acc[2].e, acc[3].e);
-    }
+  if (nb <= 32) {
+    p2p_leaf<T, COMP, 1>(lane, wl, sh, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
+                         trg_s, trg_e);
+  } else {
+    for (int base = 0; base < nb; base += 64)
+      p2p_leaf<T, COMP, 2>(lane, wl, sh, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
+                           eps2, trg_s, trg_e);
   }
 }
 

@@ -76,6 +76,8 @@ struct SolverBase {
   DevArr<int2> front, front2;
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
+  DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches
+  int m2l_ntgt = 0;
   DevArr<unsigned long long> p2p_pairs_count;
   DevArr<double> dtmp;  // host <-> device conversion scratch
   // phase timing

@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(128)
 // one warp reduction per target cell at the end.  The outputs are split into passes over
 // their degree (separate launches) so that each unrolled contraction stays small: the
 // kernel is bound by instruction fetch when one pass holds all of P = 10.
-constexpr int kM2LWarps = 4;
+constexpr int kM2LWarps = 12;
 // output degrees per FP32 M2L pass: add degrees while the pass stays under ~600 complex
 // multiply-adds (the unrolled code of one pass, and its registers, stay moderate)
 __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
@@ -314,29 +314,44 @@ __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
   return j;
 }
 
+// Warps of a block run in lockstep (a block barrier per batch of 32 sources) so that they
+// execute the same unrolled instructions together and share the fetched instruction lines;
+// targets arrive ordered by their number of batches, so the warps of a block have about
+// the same amount of work.
 template <typename T, int P, int J0, int J1>
 __global__ void __launch_bounds__(32 * kM2LWarps)
-    k_m2l_reg(int ncells, const int* __restrict__ off, const unsigned long long* __restrict__ pairs,
-              const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L,
-              int ncoef) {
+    k_m2l_reg(int ntgt, const int* __restrict__ tgt, const int* __restrict__ off,
+              const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
+              const T* __restrict__ M, T* __restrict__ L, int ncoef) {
   constexpr int NT = sph::NT(P);
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = lane_id();
-  if (c >= ncells) return;
-  const int s0 = off[c], s1 = off[c + 1];
-  if (s0 == s1) return;
+  __shared__ int smax;
+  const int wl = threadIdx.x >> 5, lane = lane_id();
+  const int w = blockIdx.x * kM2LWarps + wl;
+  const int c = w < ntgt ? tgt[w] : 0;
+  const int s0 = w < ntgt ? off[c] : 0, s1 = w < ntgt ? off[c + 1] : 0;
+  const int nbat = (s1 - s0 + 31) >> 5;
+  if (threadIdx.x == 0) smax = 0;
+  __syncthreads();
+  if (lane == 0) atomicMax(&smax, nbat);
+  __syncthreads();
+  const int maxbat = smax;
   const vec4<T> Xi = cX[c];
   T Lr[NT], Li[NT];
 #pragma unroll
   for (int t = 0; t < NT; t++) Lr[t] = Li[t] = 0;
-  for (int s = s0 + lane; s < s1; s += 32) {
-    const int j = (int)(pairs[s] & 0xffffffffULL);
-    const vec4<T> Xj = cX[j];
-    T yr[NT], yi[NT];
-    sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
-    sph::local<T, P>(a, yr, yi);
-    sph::m2l_pair<T, P, J0, J1>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
+  for (int bt = 0; bt < maxbat; bt++) {
+    const int s = s0 + bt * 32 + lane;
+    if (s < s1) {
+      const int j = (int)(pairs[s] & 0xffffffffULL);
+      const vec4<T> Xj = cX[j];
+      T yr[NT], yi[NT];
+      sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
+      sph::local<T, P>(a, yr, yi);
+      sph::m2l_pair<T, P, J0, J1>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
+    }
+    __syncthreads();
   }
+  if (nbat == 0) return;
 #pragma unroll
   for (int t = sph::sidx(J0, 0); t < sph::sidx(J1, 0); t++) {
     const T r = warp_sum(Lr[t]);
@@ -352,8 +367,8 @@ template <typename T, int P, int J0>
 static void launch_m2l_passes(Solver<T>& s) {
   if constexpr (J0 < P) {
     constexpr int J1 = m2l_pass_end(P, J0);
-    k_m2l_reg<T, P, J0, J1><<<ceil_div(s.ncells, kM2LWarps), 32 * kM2LWarps, 0, s.stream>>>(
-        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+    k_m2l_reg<T, P, J0, J1><<<ceil_div(s.m2l_ntgt, kM2LWarps), 32 * kM2LWarps, 0, s.stream>>>(
+        s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
     FMM_LAUNCH_CHECK();
     launch_m2l_passes<T, P, J1>(s);
   }

@@ -147,6 +147,19 @@ __global__ void k_csr(const unsigned long long* __restrict__ pairs, long long n,
   off[c] = (int)a;
 }
 
+// M2L targets (cells with at least one source) keyed by their number of 32-source batches,
+// largest first, for the lockstep M2L kernels
+__global__ void k_m2l_targets(int ncells, const int* __restrict__ off,
+                              unsigned long long* __restrict__ key, int* __restrict__ cell,
+                              int* __restrict__ count) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int n = off[c + 1] - off[c];
+  key[c] = n ? (unsigned long long)(1023 - min(1023, (n + 31) >> 5)) : 1023ULL;
+  cell[c] = c;
+  if (n) atomicAdd(count, 1);
+}
+
 // body-pair count of the P2P list: sum over pairs of nbody(target) * nbody(source)
 __global__ void k_p2p_bodypairs(const unsigned long long* __restrict__ pairs, long long n,
                                 const int* __restrict__ nbody,
@@ -253,6 +266,20 @@ template <typename T> void build_lists(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
   k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.p2p.p, np2p, s.ncells, s.p2p_off.p);
   FMM_LAUNCH_CHECK();
+  // M2L target order: by descending batch count (stable in cell index)
+  {
+    int* ntgt = (int*)(cnt + 4);
+    FMM_CUDA(cudaMemsetAsync(ntgt, 0, sizeof(int), s.stream));
+    s.keys.ensure(s.ncells);
+    s.keys2.ensure(s.ncells);
+    s.idx.ensure(s.ncells);
+    s.m2l_tgt.ensure(s.ncells);
+    k_m2l_targets<<<ceil_div(s.ncells, TB), TB, 0, s.stream>>>(s.ncells, s.m2l_off.p, s.keys.p,
+                                                               s.idx.p, ntgt);
+    FMM_LAUNCH_CHECK();
+    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.m2l_tgt.p, s.ncells, 10);
+    FMM_CUDA(cudaMemcpyAsync(s.scal_host + 12, ntgt, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  }
   FMM_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned long long), s.stream));
   k_p2p_bodypairs<<<std::max(1, std::min(ceil_div(np2p, TB), 148 * 8)), TB, 0, s.stream>>>(
       s.p2p.p, np2p, s.c_nbody.p, cnt + 3);
@@ -261,6 +288,7 @@ template <typename T> void build_lists(Solver<T>& s) {
                            s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
   s.p2p_body_pairs = (long long)hc[3];
+  s.m2l_ntgt = s.scal_host[12];
 }
 
 template void build_lists<float>(Solver<float>&);

@@ -289,6 +289,27 @@ __global__ void k_tkey(int n, const unsigned long long* __restrict__ skeys,
   iota[b] = b;
 }
 
+// Input order inside every leaf of at most 64 bodies (warp per leaf node): the bodies'
+// original indices, currently in full-key order, are ranked and written back ascending.
+__global__ void k_leaf_reorder(int nnodes, const int* __restrict__ nchildn,
+                               const int* __restrict__ nbegin, const int* __restrict__ ncount,
+                               const int* __restrict__ sidx, int* __restrict__ order) {
+  const int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = lane_id();
+  if (v >= nnodes || nchildn[v] != 0) return;
+  const int b0 = nbegin[v], n = ncount[v];
+  const int a = lane < n ? sidx[b0 + lane] : 0x7fffffff;
+  const int b = lane + 32 < n ? sidx[b0 + 32 + lane] : 0x7fffffff;
+  int ra = 0, rb = 0;
+  for (int k = 0; k < n; k++) {
+    const int u = k < 32 ? __shfl_sync(0xffffffffu, a, k) : __shfl_sync(0xffffffffu, b, k - 32);
+    ra += u < a;
+    rb += u < b;
+  }
+  if (lane < n) order[b0 + ra] = a;
+  if (lane + 32 < n) order[b0 + rb] = b;
+}
+
 template <typename T>
 __global__ void k_permute(int n, const vec4<T>* __restrict__ in, const int* __restrict__ order,
                           vec4<T>* __restrict__ out) {
@@ -417,25 +438,32 @@ template <typename T> void build_tree(Solver<T>& s) {
       s.ncb.p, s.nX.p, s.c_iparent.p, s.c_ichild.p, s.c_nchild.p, s.c_ibody.p, s.c_nbody.p,
       s.c_level.p, s.c_icell.p, s.cX.p);
   FMM_LAUNCH_CHECK();
-  // bodies inside a leaf in input order: stable sort by leaf-truncated key
-  int* blev = s.idx.p;
-  k_leaf_levels<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, s.nbegin.p,
-                                                           s.ncount.p, s.nlevel.p, blev);
-  FMM_LAUNCH_CHECK();
+  // bodies inside a leaf in input order (the stable partitions of the reference keep it)
   s.order.ensure(n);
-  k_tkey<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.keys2.p, s.idx2.p, blev, s.keys.p, s.order.p);
-  FMM_LAUNCH_CHECK();
-  // s.order currently holds 0..n-1 (input order positions); sort them by truncated key
-  FMM_CUDA(cudaMemcpyAsync(s.idx.p, s.order.p, n * sizeof(int), cudaMemcpyDeviceToDevice,
-                           s.stream));
-  sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
+  if (s.cfg.ncrit <= 64 && s.maxlevel < kMaxLevel) {
+    // every leaf holds at most ncrit <= 64 bodies: rank them per leaf
+    k_leaf_reorder<<<ceil_div(32LL * nnodes, TB), TB, 0, s.stream>>>(
+        nnodes, s.nchildn.p, s.nbegin.p, s.ncount.p, s.idx2.p, s.order.p);
+    FMM_LAUNCH_CHECK();
+  } else {
+    // general case: stable sort by leaf-truncated key from input order
+    int* blev = s.idx.p;
+    k_leaf_levels<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, s.nbegin.p,
+                                                             s.ncount.p, s.nlevel.p, blev);
+    FMM_LAUNCH_CHECK();
+    k_tkey<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.keys2.p, s.idx2.p, blev, s.keys.p, s.order.p);
+    FMM_LAUNCH_CHECK();
+    // s.order holds 0..n-1 (input positions); sort them by truncated key
+    FMM_CUDA(cudaMemcpyAsync(s.idx.p, s.order.p, n * sizeof(int), cudaMemcpyDeviceToDevice,
+                             s.stream));
+    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
+  }
   s.bodies.ensure(n);
   k_permute<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.bodies_in.p, s.order.p, s.bodies.p);
   FMM_LAUNCH_CHECK();
   // leaf cell list
-  int* flags = s.nsplit.p;
   s.nsplit.ensure(nnodes + 1);
-  flags = s.nsplit.p;
+  int* flags = s.nsplit.p;
   s.coff.ensure(nnodes + 1);
   k_leaf_flags<<<ceil_div(nnodes + 1, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, flags);
   FMM_LAUNCH_CHECK();

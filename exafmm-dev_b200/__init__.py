@@ -56,6 +56,10 @@ SIGNATURES = {
     "fmm_b200_solve_device": (_i, [_vp, _i, _vp, _vp]),
     "fmm_b200_solve_host": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "fmm_b200_set_bodies_host": (_i, [_vp, _i, _vp, _vp]),
+    "fmm_b200_solve_batch_device": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "fmm_b200_solve_batch_host": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "fmm_b200_set_bodies_batch_device": (_i, [_vp, _i, _vp, _vp]),
+    "fmm_b200_get_roots": (_i, [_vp, _vp, _vp, _vp]),
     "fmm_b200_set_bodies_device": (_i, [_vp, _i, _vp]),
     "fmm_b200_build_tree": (_i, [_vp]),
     "fmm_b200_upward_pass": (_i, [_vp]),
@@ -71,6 +75,12 @@ SIGNATURES = {
     "fmm_b200_num_lists": (_i, [_vp, _vp, _vp, _vp]),
     "fmm_b200_get_lists": (_i, [_vp, _vp, _vp]),
     "fmm_b200_get_timings": (_i, [_vp, _vp]),
+    "fmm_b200_server_create": (_i, [_vp, _d, _i, _i, _vp]),
+    "fmm_b200_server_submit": (_i, [_vp, _i, _vp, _vp, _i, _vp]),
+    "fmm_b200_server_poll": (_i, [_vp, _ll, _vp]),
+    "fmm_b200_server_wait": (_i, [_vp, _ll, _vp, _vp, _vp, _vp]),
+    "fmm_b200_server_stats": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "fmm_b200_server_destroy": (_i, [_vp]),
     "fmm_b200_direct": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_fp32_peak": (_i, [_i, _vp]),
     "fmm_b200_kernel_launches": (_ll, []),
@@ -231,6 +241,36 @@ class Solver:
         self.n = n
         return np.concatenate([p[:, None], f], axis=1)
 
+    def solve_batch(self, xs, qs):
+        """Several independent solves in one batch: lists of (n_s, 3) positions and (n_s,)
+        charges; returns a list of (n_s, 4) results."""
+        counts = np.array([len(q) for q in qs], np.int32)
+        x = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64).reshape(-1, 3) for a in xs]))
+        q = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64).reshape(-1) for a in qs]))
+        n = len(q)
+        p = np.zeros(n)
+        f = np.zeros((n, 3))
+        self._check(self.lib.fmm_b200_solve_batch_host(self.h, len(counts), _p(counts), _p(x),
+                                                       _p(q), _p(p), _p(f)))
+        self.n = n
+        out = np.concatenate([p[:, None], f], axis=1)
+        return np.split(out, np.cumsum(counts)[:-1])
+
+    def solve_batch_device(self, counts, bodies_ptr, trg_ptr):
+        counts = np.ascontiguousarray(counts, np.int32)
+        self.n = int(counts.sum())
+        self._check(self.lib.fmm_b200_solve_batch_device(self.h, len(counts), _p(counts),
+                                                         C.c_void_p(bodies_ptr),
+                                                         C.c_void_p(trg_ptr)))
+
+    def roots(self):
+        nr = C.c_int()
+        self._check(self.lib.fmm_b200_get_roots(self.h, C.byref(nr), None, None))
+        cells = np.zeros(nr.value, np.int32)
+        solves = np.zeros(nr.value, np.int32)
+        self._check(self.lib.fmm_b200_get_roots(self.h, C.byref(nr), _p(cells), _p(solves)))
+        return cells, solves
+
     def solve_host_ptrs(self, n, x_ptr, q_ptr, p_ptr, f_ptr):
         """solve_host on raw host pointers (pinned buffers for end-to-end timing)."""
         self.n = n
@@ -300,3 +340,64 @@ class Solver:
         t = np.zeros(len(PHASES))
         self._check(self.lib.fmm_b200_get_timings(self.h, _p(t)))
         return dict(zip(PHASES, t))
+
+
+class Server:
+    """Continuous-batching serving loop (fmm_b200_server_*): submit solves of any size and
+    order P from any thread; results come back per request with their latency."""
+
+    def __init__(self, basis="spherical", theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
+                 use_ropt=1, precision="f32", hbm_budget_gb=32.0, workers=2, max_batch=256,
+                 device=0):
+        self.lib = load_library()
+        cfg = Config()
+        self.lib.fmm_b200_default_config(C.byref(cfg))
+        cfg.basis, cfg.theta, cfg.ncrit, cfg.nspawn = _basis(basis), theta, ncrit, nspawn
+        cfg.use_rmax, cfg.use_ropt, cfg.precision, cfg.device = use_rmax, use_ropt, _prec(precision), device
+        self.h = C.c_void_p()
+        rc = self.lib.fmm_b200_server_create(C.byref(cfg), hbm_budget_gb * 1e9, workers, max_batch,
+                                             C.byref(self.h))
+        if rc != FMM_OK:
+            raise FmmError(rc, self.lib.fmm_b200_last_error(None).decode())
+        self._n = {}
+
+    def submit(self, x, q, P):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, np.float64).reshape(-1)
+        rid = C.c_longlong()
+        rc = self.lib.fmm_b200_server_submit(self.h, len(q), _p(x), _p(q), P, C.byref(rid))
+        if rc != FMM_OK:
+            raise FmmError(rc, "submit rejected")
+        self._n[rid.value] = len(q)
+        return rid.value
+
+    def done(self, rid):
+        d = C.c_int()
+        rc = self.lib.fmm_b200_server_poll(self.h, rid, C.byref(d))
+        if rc != FMM_OK:
+            raise FmmError(rc, "unknown request")
+        return bool(d.value)
+
+    def wait(self, rid):
+        """(n, 4) result, latency seconds, queueing seconds."""
+        n = self._n.pop(rid)
+        p = np.zeros(n)
+        f = np.zeros((n, 3))
+        lat, que = C.c_double(), C.c_double()
+        rc = self.lib.fmm_b200_server_wait(self.h, rid, _p(p), _p(f), C.byref(lat), C.byref(que))
+        if rc != FMM_OK:
+            raise FmmError(rc, "request failed")
+        return np.concatenate([p[:, None], f], axis=1), lat.value, que.value
+
+    def stats(self):
+        a, b, c, d = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_int()
+        self.lib.fmm_b200_server_stats(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return dict(completed=a.value, bodies=b.value, batches=c.value, pending=d.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fmm_b200_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

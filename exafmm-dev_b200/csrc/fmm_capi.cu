@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include <string>
 
 #include "fmm_solver.cuh"
@@ -97,6 +98,21 @@ template <typename F> int guarded(fmm_b200_solver* h, F&& f) {
     h->base->err = e.what();
     return FMM_ERR_INVALID;
   }
+}
+
+// body ranges of a batch of solves from their counts (host); false on a bad count
+bool set_segments(SolverBase& s, int nsolves, const int* counts, int* total) {
+  if (nsolves < 1 || !counts) return false;
+  s.seg.assign(nsolves + 1, 0);
+  long long acc = 0;
+  for (int q = 0; q < nsolves; q++) {
+    if (counts[q] < 0) return false;
+    acc += counts[q];
+    if (acc > 0x7fffffffLL) return false;
+    s.seg[q + 1] = (int)acc;
+  }
+  *total = (int)acc;
+  return true;
 }
 
 template <typename T> void set_bodies_host_t(Solver<T>& s, int n, const double* x, const double* q,
@@ -319,11 +335,15 @@ const char* fmm_b200_last_error(const fmm_b200_solver* h) {
 
 int fmm_b200_set_bodies_host(fmm_b200_solver* h, int n, const double* x, const double* q) {
   if (n < 0 || (n > 0 && (!x || !q))) return FMM_ERR_INVALID;
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  h->base->seg = {0, n};
   return FMM_DISPATCH(h, set_bodies_host_t(s, n, x, q, h->base->dtmp));
 }
 
 int fmm_b200_set_bodies_device(fmm_b200_solver* h, int n, const void* d_bodies) {
   if (n < 0 || (n > 0 && !d_bodies)) return FMM_ERR_INVALID;
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  h->base->seg = {0, n};
   return FMM_DISPATCH(h, {
     s.n = n;
     s.bodies_in.ensure(std::max(n, 1));
@@ -341,6 +361,8 @@ int fmm_b200_downward_pass(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_do
 
 int fmm_b200_solve_device(fmm_b200_solver* h, int n, const void* d_bodies, void* d_trg) {
   if (n < 0 || (n > 0 && (!d_bodies || !d_trg))) return FMM_ERR_INVALID;
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  h->base->seg = {0, n};
   return FMM_DISPATCH(h, {
     s.n = n;
     s.bodies_in.ensure(std::max(n, 1));
@@ -358,6 +380,8 @@ int fmm_b200_solve_device(fmm_b200_solver* h, int n, const void* d_bodies, void*
 int fmm_b200_solve_host(fmm_b200_solver* h, int n, const double* x, const double* q, double* p,
                         double* f) {
   if (n < 0 || (n > 0 && (!x || !q || !p || !f))) return FMM_ERR_INVALID;
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  h->base->seg = {0, n};
   return FMM_DISPATCH(h, {
     DevArr<double>& tmp = h->base->dtmp;
     set_bodies_host_t(s, n, x, q, tmp);
@@ -371,6 +395,78 @@ int fmm_b200_solve_host(fmm_b200_solver* h, int n, const double* x, const double
                                s.stream));
     }
     FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_solve_batch_device(fmm_b200_solver* h, int nsolves, const int* counts,
+                                const void* d_bodies, void* d_trg) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  int n = 0;
+  if (!set_segments(*h->base, nsolves, counts, &n)) return FMM_ERR_INVALID;
+  if (n > 0 && (!d_bodies || !d_trg)) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    s.n = n;
+    s.bodies_in.ensure(std::max(n, 1));
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p, d_bodies, sizeof(s.bodies_in.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+    s.stage = ST_BODIES;
+    solve_all(s);
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(d_trg, s.trg_out.p, sizeof(s.trg_out.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+  });
+}
+
+int fmm_b200_solve_batch_host(fmm_b200_solver* h, int nsolves, const int* counts,
+                              const double* x, const double* q, double* p, double* f) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  int n = 0;
+  if (!set_segments(*h->base, nsolves, counts, &n)) return FMM_ERR_INVALID;
+  if (n > 0 && (!x || !q || !p || !f)) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    DevArr<double>& tmp = h->base->dtmp;
+    std::vector<int> seg = s.seg;
+    set_bodies_host_t(s, n, x, q, tmp);
+    s.seg = seg;
+    solve_all(s);
+    if (n > 0) {
+      tmp.ensure(4 * (size_t)n);
+      k_unpack_pf<T><<<ceil_div(n, 256), 256, 0, s.stream>>>(n, s.trg_out.p, tmp.p, tmp.p + n);
+      FMM_LAUNCH_CHECK();
+      FMM_CUDA(cudaMemcpyAsync(p, tmp.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s.stream));
+      FMM_CUDA(cudaMemcpyAsync(f, tmp.p + n, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               s.stream));
+    }
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_set_bodies_batch_device(fmm_b200_solver* h, int nsolves, const int* counts,
+                                     const void* d_bodies) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  int n = 0;
+  if (!set_segments(*h->base, nsolves, counts, &n)) return FMM_ERR_INVALID;
+  if (n > 0 && !d_bodies) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, {
+    s.n = n;
+    s.bodies_in.ensure(std::max(n, 1));
+    if (n > 0)
+      FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p, d_bodies, sizeof(s.bodies_in.p[0]) * n,
+                               cudaMemcpyDeviceToDevice, s.stream));
+    s.stage = ST_BODIES;
+  });
+}
+
+int fmm_b200_get_roots(fmm_b200_solver* h, int* nroots, int* root_cells, int* root_solves) {
+  return guarded(h, [&] {
+    SolverBase& s = *h->base;
+    if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "tree not built");
+    if (nroots) *nroots = s.nroots;
+    for (int r = 0; r < s.nroots; r++) {
+      if (root_cells) root_cells[r] = s.root_cell[r];
+      if (root_solves) root_solves[r] = s.root_solve[r];
+    }
   });
 }
 

@@ -17,10 +17,10 @@ namespace fmmb200 {
 // M2L / L2L of the MASS build undo again), so only |M[0]| enters.
 template <typename T>
 __global__ void k_ropt(int ncells, vec4<T>* __restrict__ cX, const T* __restrict__ M,
-                       int ncoef, int P, T theta) {
+                       const int* __restrict__ croot, int ncoef, int P, T theta) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
-  const T m0root = fabs(M[0]);
+  const T m0root = fabs(M[(size_t)croot[c] * ncoef]);  // the monopole of this cell's root
   const T omt = sub_rn((T)1, theta);
   const T cc = (T)__ddiv_rn(__ddiv_rn((double)mul_rn(omt, omt), pow((double)theta, (double)(P + 2))),
                            (double)powf((float)m0root, (float)(1.0 / 3)));
@@ -64,8 +64,8 @@ template <typename T> void upward_pass(Solver<T>& s) {
   ops.p2m(s);
   for (int l = s.maxlevel - 1; l >= 0; l--) ops.m2m_level(s, s.level_lo[l], s.level_lo[l + 1]);
   if (s.cfg.use_ropt) {
-    k_ropt<T><<<ceil_div(s.ncells, 256), 256, 0, s.stream>>>(s.ncells, s.cX.p, s.M.p, s.ncoef,
-                                                            s.cfg.P, (T)s.cfg.theta);
+    k_ropt<T><<<ceil_div(s.ncells, 256), 256, 0, s.stream>>>(s.ncells, s.cX.p, s.M.p, s.c_root.p,
+                                                            s.ncoef, s.cfg.P, (T)s.cfg.theta);
     FMM_LAUNCH_CHECK();
   }
 }

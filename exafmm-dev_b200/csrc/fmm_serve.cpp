@@ -1,0 +1,314 @@
+// Serving loop over the batched solver: continuous batching of independent FMM solves.
+//
+// Requests (bodies + expansion order) are copied in at submit and queued.  A scheduler
+// thread forms batches from whatever is pending whenever a worker is free: the oldest
+// request decides the order P, later requests of the same P join in arrival order while the
+// batch fits the free part of the device-memory budget and the batch-size limit.  Each
+// worker owns a CUDA stream and one solver handle per order, so batches on different
+// workers overlap on the GPU; requests that arrive while batches run are admitted into the
+// next batch as soon as a worker and budget free up.  A request's result does not depend on
+// which batch it rode in (fmm_b200_solve_batch_*: every solve is computed as it is alone).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/exafmm_b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  long long id = 0;
+  int n = 0, P = 0;
+  std::vector<double> x, q, p, f;
+  size_t bytes = 0;
+  int status = FMM_OK;
+  bool done = false;
+  Clock::time_point t_submit, t_start, t_done;
+};
+
+struct Worker {
+  int index = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, fmm_b200_solver*> handles;  // per expansion order
+  std::vector<std::shared_ptr<Request>> batch;
+  bool busy = false;
+  std::thread thread;
+  // pinned staging for the batch's inputs / outputs
+  double* pin = nullptr;
+  size_t pin_cap = 0;
+};
+
+}  // namespace
+
+struct fmm_b200_server {
+  fmm_b200_config cfg;
+  size_t budget = 0, in_flight = 0;
+  int max_batch = 256;
+  std::mutex mu;
+  std::condition_variable cv;   // scheduler wakes on submit / worker done
+  std::condition_variable done_cv;
+  std::deque<std::shared_ptr<Request>> pending;
+  std::unordered_map<long long, std::shared_ptr<Request>> all;
+  std::vector<std::unique_ptr<Worker>> workers;
+  std::thread scheduler;
+  bool stop = false;
+  long long next_id = 1;
+  long long completed = 0, bodies_done = 0, batches = 0;
+  std::string err;
+};
+
+namespace {
+
+// device memory of one solve in the batched solver (bodies, sort scratch, tree, expansions,
+// interaction lists), an upper-end estimate used for admission
+size_t estimate_bytes(const fmm_b200_config& c, int n, int P) {
+  const size_t ncoef = c.basis == FMM_SPHERICAL ? (size_t)P * (P + 1) : (size_t)P * (P + 1) * (P + 2) / 6;
+  const size_t real = c.precision == FMM_FP64 ? 8 : 4;
+  const size_t cells = 2 * (size_t)n / std::max(1, c.ncrit) + 64;
+  return (size_t)n * (8 * real + 48) + cells * (2 * ncoef * real + 160) + cells * 400 * 8;
+}
+
+void worker_loop(fmm_b200_server* S, Worker* W) {
+  cudaSetDevice(S->cfg.device);
+  cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking);
+  for (;;) {
+    std::vector<std::shared_ptr<Request>> batch;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv.wait(lk, [&] { return S->stop || !W->batch.empty(); });
+      if (W->batch.empty() && S->stop) break;
+      batch.swap(W->batch);
+    }
+    const int P = batch.front()->P;
+    int rc = FMM_OK;
+    fmm_b200_solver*& h = W->handles[P];
+    if (!h) {
+      fmm_b200_config c = S->cfg;
+      c.P = P;
+      rc = fmm_b200_create(&c, &h);
+      if (rc == FMM_OK) rc = fmm_b200_set_stream(h, W->stream);
+      if (rc != FMM_OK) h = nullptr;
+    }
+    std::vector<int> counts;
+    size_t n = 0;
+    for (auto& r : batch) {
+      counts.push_back(r->n);
+      n += r->n;
+    }
+    if (rc == FMM_OK) {
+      if (W->pin_cap < 8 * n) {
+        if (W->pin) cudaFreeHost(W->pin);
+        W->pin_cap = 8 * n + 1024;
+        if (cudaMallocHost((void**)&W->pin, W->pin_cap * sizeof(double)) != cudaSuccess) {
+          W->pin = nullptr;
+          W->pin_cap = 0;
+          rc = FMM_ERR_NO_MEMORY;
+        }
+      }
+    }
+    const auto t_start = Clock::now();
+    if (rc == FMM_OK) {
+      double *x = W->pin, *q = x + 3 * n, *p = q + n, *f = p + n;
+      size_t o = 0;
+      for (auto& r : batch) {
+        std::memcpy(x + 3 * o, r->x.data(), sizeof(double) * 3 * r->n);
+        std::memcpy(q + o, r->q.data(), sizeof(double) * r->n);
+        o += r->n;
+      }
+      rc = fmm_b200_solve_batch_host(h, (int)counts.size(), counts.data(), x, q, p, f);
+      if (rc == FMM_OK) {
+        o = 0;
+        for (auto& r : batch) {
+          r->p.assign(p + o, p + o + r->n);
+          r->f.assign(f + 3 * o, f + 3 * (o + r->n));
+          o += r->n;
+        }
+      }
+    }
+    const auto t_done = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (auto& r : batch) {
+        r->status = rc;
+        r->done = true;
+        r->t_start = t_start;
+        r->t_done = t_done;
+        S->in_flight -= r->bytes;
+        S->completed++;
+        S->bodies_done += r->n;
+      }
+      S->batches++;
+      W->busy = false;
+      if (rc != FMM_OK && h) S->err = fmm_b200_last_error(h);
+    }
+    S->cv.notify_all();
+    S->done_cv.notify_all();
+  }
+  for (auto& kv : W->handles)
+    if (kv.second) fmm_b200_destroy(kv.second);
+  if (W->pin) cudaFreeHost(W->pin);
+  cudaStreamDestroy(W->stream);
+}
+
+void scheduler_loop(fmm_b200_server* S) {
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    Worker* free_w = nullptr;
+    S->cv.wait(lk, [&] {
+      if (S->stop) return true;
+      if (S->pending.empty()) return false;
+      free_w = nullptr;
+      for (auto& w : S->workers)
+        if (!w->busy) {
+          free_w = w.get();
+          break;
+        }
+      return free_w && S->in_flight + S->pending.front()->bytes <= S->budget;
+    });
+    if (S->stop) break;
+    // batch: the oldest request's order, later ones of the same order in arrival order
+    const int P = S->pending.front()->P;
+    std::vector<std::shared_ptr<Request>> batch;
+    for (auto it = S->pending.begin(); it != S->pending.end() && (int)batch.size() < S->max_batch;) {
+      if ((*it)->P == P && S->in_flight + (*it)->bytes <= S->budget) {
+        S->in_flight += (*it)->bytes;
+        batch.push_back(*it);
+        it = S->pending.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    free_w->busy = true;
+    free_w->batch = std::move(batch);
+    S->cv.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmm_b200_server_create(const fmm_b200_config* cfg, double hbm_budget_bytes, int nworkers,
+                           int max_batch, fmm_b200_server** out) {
+  if (!cfg || !out || nworkers < 1 || max_batch < 1 || !(hbm_budget_bytes > 0))
+    return FMM_ERR_INVALID;
+  // validate the configuration (and the device) once up front
+  fmm_b200_solver* probe = nullptr;
+  int rc = fmm_b200_create(cfg, &probe);
+  if (rc != FMM_OK) return rc;
+  fmm_b200_destroy(probe);
+  fmm_b200_server* S = new fmm_b200_server();
+  S->cfg = *cfg;
+  S->budget = (size_t)hbm_budget_bytes;
+  S->max_batch = max_batch;
+  for (int i = 0; i < nworkers; i++) {
+    S->workers.emplace_back(new Worker());
+    S->workers.back()->index = i;
+  }
+  for (auto& w : S->workers) w->thread = std::thread(worker_loop, S, w.get());
+  S->scheduler = std::thread(scheduler_loop, S);
+  *out = S;
+  return FMM_OK;
+}
+
+int fmm_b200_server_submit(fmm_b200_server* S, int n, const double* x, const double* q, int P,
+                           long long* id) {
+  if (!S || n < 1 || !x || !q || !id) return FMM_ERR_INVALID;
+  auto r = std::make_shared<Request>();
+  r->n = n;
+  r->P = P;
+  r->bytes = estimate_bytes(S->cfg, n, P);
+  if (r->bytes > S->budget) return FMM_ERR_NO_MEMORY;  // never fits: reject, do not queue
+  int buf[64];
+  const int nord = fmm_b200_supported_orders(S->cfg.basis, buf, 64);
+  if (std::find(buf, buf + std::min(nord, 64), P) == buf + std::min(nord, 64)) return FMM_ERR_INVALID;
+  r->x.assign(x, x + 3 * (size_t)n);
+  r->q.assign(q, q + n);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return FMM_ERR_STATE;
+    r->id = S->next_id++;
+    S->pending.push_back(r);
+    S->all[r->id] = r;
+    *id = r->id;
+  }
+  S->cv.notify_all();
+  return FMM_OK;
+}
+
+int fmm_b200_server_poll(fmm_b200_server* S, long long id, int* done) {
+  if (!S || !done) return FMM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(id);
+  if (it == S->all.end()) return FMM_ERR_INVALID;
+  *done = it->second->done ? 1 : 0;
+  return FMM_OK;
+}
+
+int fmm_b200_server_wait(fmm_b200_server* S, long long id, double* p, double* f,
+                         double* latency_s, double* queue_s) {
+  if (!S) return FMM_ERR_INVALID;
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->all.find(id);
+    if (it == S->all.end()) return FMM_ERR_INVALID;
+    r = it->second;
+    S->done_cv.wait(lk, [&] { return r->done; });
+    S->all.erase(it);
+  }
+  if (r->status != FMM_OK) return r->status;
+  if (p) std::memcpy(p, r->p.data(), sizeof(double) * r->n);
+  if (f) std::memcpy(f, r->f.data(), sizeof(double) * 3 * r->n);
+  if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  if (queue_s) *queue_s = std::chrono::duration<double>(r->t_start - r->t_submit).count();
+  return FMM_OK;
+}
+
+int fmm_b200_server_stats(fmm_b200_server* S, long long* completed, long long* bodies,
+                          long long* batches, int* pending) {
+  if (!S) return FMM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (completed) *completed = S->completed;
+  if (bodies) *bodies = S->bodies_done;
+  if (batches) *batches = S->batches;
+  if (pending) *pending = (int)S->pending.size();
+  return FMM_OK;
+}
+
+int fmm_b200_server_destroy(fmm_b200_server* S) {
+  if (!S) return FMM_ERR_INVALID;
+  {
+    // drain: let queued requests finish first
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->done_cv.wait(lk, [&] {
+      if (!S->pending.empty()) return false;
+      for (auto& w : S->workers)
+        if (w->busy) return false;
+      return true;
+    });
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  S->scheduler.join();
+  for (auto& w : S->workers) w->thread.join();
+  delete S;
+  return FMM_OK;
+}
+
+}  // extern "C"

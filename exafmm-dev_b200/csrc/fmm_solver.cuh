@@ -51,6 +51,13 @@ struct SolverBase {
   fmm_b200_config cfg;
   cudaStream_t stream = nullptr;
   int n = 0;
+  // a batch of independent solves ("forest"): body ranges [seg[s], seg[s+1]) per solve;
+  // every non-empty solve gets one root (roots in solve order), cells of a root contiguous
+  std::vector<int> seg{0, 0};
+  std::vector<int> root_solve;  // solve of each root
+  std::vector<int> root_cell;   // first cell of each root (host copy)
+  int nroots = 0;
+  DevArr<int> d_seg, d_root_first, d_root_count, nsid, c_root, cbase;
   int ncoef = 0, nterm = 0;
   Stage stage = ST_NONE;
   std::string err;
@@ -88,7 +95,7 @@ struct SolverBase {
 
 template <typename T> struct Solver : SolverBase {
   DevArr<vec4<T>> bodies_in, bodies, trg_s, trg_e, trg_out, cX;
-  DevArr<T> box;  // X0[3], R0, Xmin[3], Xmax[3]
+  DevArr<T> box;  // per root, 16 values: X0[3], R0, Xmin[3], Xmax[3]
   DevArr<T> M, L, nX;
   DevArr<T> minmax_part;
 };
@@ -125,6 +132,9 @@ void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long 
 void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
                    int n, int end_bit);
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n);
+void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
+                              unsigned long long* kout, const int* vin, int* vout, int n,
+                              int nseg, const int* begin, const int* end, int end_bit);
 void sum_u64(SolverBase& s, const unsigned long long* in, unsigned long long* out, int n);
 
 }  // namespace fmmb200

@@ -27,6 +27,18 @@ void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long l
                                           s.stream));
 }
 
+void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
+                              unsigned long long* kout, const int* vin, int* vout, int n,
+                              int nseg, const int* begin, const int* end, int end_bit) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  FMM_CUDA(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, nseg,
+                                                    begin, end, 0, end_bit, s.stream));
+  s.cub_tmp.ensure(bytes);
+  FMM_CUDA(cub::DeviceSegmentedRadixSort::SortPairs(s.cub_tmp.p, bytes, kin, kout, vin, vout, n,
+                                                    nseg, begin, end, 0, end_bit, s.stream));
+}
+
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n) {
   if (n <= 0) return;
   size_t bytes = 0;

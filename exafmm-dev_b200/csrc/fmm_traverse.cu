@@ -10,6 +10,7 @@
 // sizes, no overflow) and emits M2L pairs, P2P pairs and the next frontier.  Lists are
 // then sorted by (target, source) into per-target CSR for the M2L and P2P kernels.
 #include <algorithm>
+#include <vector>
 
 #include "fmm_solver.cuh"
 
@@ -196,10 +197,13 @@ template <typename T> void build_lists(Solver<T>& s) {
   if (s.ncells == 0) return;
   unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
   unsigned long long* hc = (unsigned long long*)s.scal_host;
-  s.front.ensure(1);
-  int2 root = make_int2(0, 0);
-  FMM_CUDA(cudaMemcpyAsync(s.front.p, &root, sizeof(int2), cudaMemcpyHostToDevice, s.stream));
-  long long nfront = 1;
+  // one (root, root) pair per solve of the batch: lists never cross solves
+  std::vector<int2> roots(s.nroots);
+  for (int r = 0; r < s.nroots; r++) roots[r] = make_int2(s.root_cell[r], s.root_cell[r]);
+  s.front.ensure(std::max(s.nroots, 1));
+  FMM_CUDA(cudaMemcpyAsync(s.front.p, roots.data(), sizeof(int2) * s.nroots,
+                           cudaMemcpyHostToDevice, s.stream));
+  long long nfront = s.nroots;
   long long nm2l = 0, np2p = 0;
   s.m2l.ensure(1024);
   s.p2p.ensure(1024);

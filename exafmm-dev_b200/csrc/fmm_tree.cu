@@ -21,12 +21,15 @@ template <> __device__ __forceinline__ float tmax<float>() { return FLT_MAX; }
 template <> __device__ __forceinline__ double tmax<double>() { return DBL_MAX; }
 
 // ---------------------------------------------------------------- bounds
-// BoundBox::getBounds (include/bound_box.h:76-88): elementwise min / max of positions.
+// BoundBox::getBounds (include/bound_box.h:76-88): elementwise min / max of positions, per
+// chunk of one root's bodies (one block per chunk), then per root.
 template <typename T>
-__global__ void k_minmax_partial(const vec4<T>* __restrict__ b, int n, T* __restrict__ part) {
+__global__ void k_minmax_chunks(const vec4<T>* __restrict__ b, const int* __restrict__ cb,
+                                const int* __restrict__ ce, T* __restrict__ part) {
   T mn[3] = {tmax<T>(), tmax<T>(), tmax<T>()};
   T mx[3] = {-tmax<T>(), -tmax<T>(), -tmax<T>()};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int e = ce[blockIdx.x];
+  for (int i = cb[blockIdx.x] + threadIdx.x; i < e; i += blockDim.x) {
     vec4<T> p = b[i];
     mn[0] = p.x < mn[0] ? p.x : mn[0];
     mn[1] = p.y < mn[1] ? p.y : mn[1];
@@ -59,13 +62,17 @@ __global__ void k_minmax_partial(const vec4<T>* __restrict__ b, int n, T* __rest
   }
 }
 
-// BuildTree::bounds2box (include/build_tree_tbb.h:298-310); box = X0[3], R0, Xmin[3], Xmax[3]
+// BuildTree::bounds2box (include/build_tree_tbb.h:298-310), one thread per root;
+// box[16 r ..] = X0[3], R0, Xmin[3], Xmax[3]
 template <typename T>
-__global__ void k_box(const T* __restrict__ part, int nblk, T* __restrict__ box) {
-  if (threadIdx.x != 0) return;
+__global__ void k_box(int nroots, const int* __restrict__ chunk_lo, const T* __restrict__ part,
+                      T* __restrict__ box) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nroots) return;
+  const int c0 = chunk_lo[r], c1 = chunk_lo[r + 1];
   T mn[3], mx[3];
-  for (int d = 0; d < 3; d++) mn[d] = part[d], mx[d] = part[3 + d];
-  for (int k = 1; k < nblk; k++)
+  for (int d = 0; d < 3; d++) mn[d] = part[6 * c0 + d], mx[d] = part[6 * c0 + 3 + d];
+  for (int k = c0 + 1; k < c1; k++)
     for (int d = 0; d < 3; d++) {
       T a = part[6 * k + d], c = part[6 * k + 3 + d];
       mn[d] = a < mn[d] ? a : mn[d];
@@ -79,18 +86,28 @@ __global__ void k_box(const T* __restrict__ part, int nblk, T* __restrict__ box)
     T c = sub_rn(mx[d], X[d]);
     R = R < c ? c : R;
   }
-  for (int d = 0; d < 3; d++) box[d] = X[d], box[4 + d] = mn[d], box[7 + d] = mx[d];
-  box[3] = (T)__dmul_rn((double)R, 1.00001);
+  T* bx = box + 16 * r;
+  for (int d = 0; d < 3; d++) bx[d] = X[d], bx[4 + d] = mn[d], bx[7 + d] = mx[d];
+  bx[3] = (T)__dmul_rn((double)R, 1.00001);
 }
 
 // ---------------------------------------------------------------- path keys
 template <typename T>
 __global__ void k_keys(const vec4<T>* __restrict__ b, int n, const T* __restrict__ box,
+                       const int* __restrict__ root_first, int nroots,
                        unsigned long long* __restrict__ keys, int* __restrict__ idx) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  // root of body i: last r with root_first[r] <= i
+  int lo = 0, hi = nroots - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (root_first[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const T* bx = box + 16 * lo;
   vec4<T> p = b[i];
-  T c0 = box[0], c1 = box[1], c2 = box[2], R0 = box[3];
+  T c0 = bx[0], c1 = bx[1], c2 = bx[2], R0 = bx[3];
   unsigned long long key = 0;
 #pragma unroll 1
   for (int l = 0; l < kMaxLevel; l++) {
@@ -109,16 +126,19 @@ __device__ __forceinline__ int digit_at(unsigned long long key, int level) {
   return (int)((key >> (3 * (kMaxLevel - 1 - level))) & 7ULL);
 }
 
-__global__ void k_root(int n, int* nbegin, int* ncount, int* nparent, int* nlevel) {
-  nbegin[0] = 0;
-  ncount[0] = n;
-  nparent[0] = -1;
-  nlevel[0] = 0;
-}
-
-template <typename T> __global__ void k_root_x(const T* __restrict__ box, T* __restrict__ nX) {
-  for (int d = 0; d < 3; d++) nX[d] = box[d];
-  nX[3] = 0;
+// one root node per non-empty solve, in solve order
+template <typename T>
+__global__ void k_roots(int nroots, const int* __restrict__ root_first, const T* __restrict__ box,
+                        int* nbegin, int* ncount, int* nparent, int* nlevel, int* nsid, T* nX) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nroots) return;
+  nbegin[r] = root_first[r];
+  ncount[r] = root_first[r + 1] - root_first[r];
+  nparent[r] = -1;
+  nlevel[r] = 0;
+  nsid[r] = r;
+  for (int d = 0; d < 3; d++) nX[4 * r + d] = box[16 * r + d];
+  nX[4 * r + 3] = 0;
 }
 
 // One level of BuildNodes (include/build_tree_tbb.h:165-218): a node with more than ncrit
@@ -158,7 +178,7 @@ __global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
                        const T* __restrict__ box, int* __restrict__ nbegin,
                        int* __restrict__ ncount, int* __restrict__ nparent,
                        int* __restrict__ nchildn, int* __restrict__ nfirst,
-                       int* __restrict__ nlevel, T* __restrict__ nX) {
+                       int* __restrict__ nlevel, int* __restrict__ nsid, T* __restrict__ nX) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= hi - lo) return;
   int v = lo + t;
@@ -171,7 +191,8 @@ __global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
   int first = hi + coff[t];
   nfirst[v] = first;
   const int* st = starts + 9 * t;
-  T r = div_rn(box[3], (T)(1 << (level + 1)));
+  const int root = nsid[v];
+  T r = div_rn(box[16 * root + 3], (T)(1 << (level + 1)));
   T X0 = nX[4 * v], X1 = nX[4 * v + 1], X2 = nX[4 * v + 2];
   int k = 0;
   for (int o = 0; o < 8; o++) {
@@ -181,6 +202,7 @@ __global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
     ncount[u] = st[o + 1] - st[o];
     nparent[u] = v;
     nlevel[u] = level + 1;
+    nsid[u] = root;
     nX[4 * u] = add_rn(X0, (o & 1) ? r : -r);
     nX[4 * u + 1] = add_rn(X1, (o & 2) ? r : -r);
     nX[4 * u + 2] = add_rn(X2, (o & 4) ? r : -r);
@@ -211,13 +233,14 @@ __global__ void k_nnode(int lo, int hi, const int* __restrict__ nchildn,
 // next free slot after the child block, each child's subtree after the previous child's.
 __global__ void k_pos(int lo, int hi, const int* __restrict__ nchildn,
                       const int* __restrict__ nfirst, const int* __restrict__ nnode,
-                      int* __restrict__ npos, int* __restrict__ ncb) {
+                      const int* __restrict__ cbase, int* __restrict__ npos,
+                      int* __restrict__ ncb) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= hi - lo) return;
   int v = lo + t;
-  if (v == 0) {
-    npos[0] = 0;
-    ncb[0] = 1;
+  if (lo == 0) {  // roots: each root's cells start after the previous root's subtree
+    npos[v] = cbase[v];
+    ncb[v] = cbase[v] + 1;
   }
   int nch = nchildn[v];
   if (nch == 0) return;
@@ -234,21 +257,24 @@ __global__ void k_pos(int lo, int hi, const int* __restrict__ nchildn,
 // Cell records (Nodes2cells::operator(), include/build_tree_tbb.h:250-262) with the
 // Morton index of getKey (:240-249) in 64-bit arithmetic.
 template <typename T>
-__global__ void k_cells(int nnodes, const T* __restrict__ box, const int* __restrict__ nbegin,
+__global__ void k_cells(int nnodes, const T* __restrict__ boxes, const int* __restrict__ nbegin,
                         const int* __restrict__ ncount, const int* __restrict__ nparent,
                         const int* __restrict__ nchildn, const int* __restrict__ nlevel,
+                        const int* __restrict__ nsid, const int* __restrict__ cbase,
                         const int* __restrict__ npos, const int* __restrict__ ncb,
                         const T* __restrict__ nX, int* iparent, int* ichild, int* nchild,
                         int* ibody, int* nbody, int* clevel, unsigned long long* icell,
-                        vec4<T>* cX) {
+                        vec4<T>* cX, int* croot) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nnodes) return;
   int c = npos[v];
   int lev = nlevel[v];
+  const T* box = boxes + 16 * nsid[v];
+  croot[c] = cbase[nsid[v]];
   T R0 = box[3];
   T R = div_rn(R0, (T)(1 << lev));
   T X[3] = {nX[4 * v], nX[4 * v + 1], nX[4 * v + 2]};
-  iparent[c] = v == 0 ? 0 : npos[nparent[v]];
+  iparent[c] = nparent[v] < 0 ? c : npos[nparent[v]];
   int nch = nchildn[v];
   nchild[c] = nch;
   ichild[c] = nch ? ncb[v] : 0;
@@ -346,42 +372,80 @@ template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
 template <typename T> void build_tree(Solver<T>& s) {
   const int n = s.n;
   const int TB = 256;
-  s.box.ensure(16);
   s.level_lo.clear();
   s.ncells = s.maxlevel = s.nleaves = 0;
-  if (n == 0) {
+  // roots: non-empty solves in order
+  const int nsolves = (int)s.seg.size() - 1;
+  s.root_solve.clear();
+  std::vector<int> rfirst;
+  for (int q = 0; q < nsolves; q++)
+    if (s.seg[q + 1] > s.seg[q]) {
+      s.root_solve.push_back(q);
+      rfirst.push_back(s.seg[q]);
+    }
+  rfirst.push_back(n);
+  const int nroots = (int)s.root_solve.size();
+  s.nroots = nroots;
+  s.box.ensure(16 * (size_t)std::max(nroots, 1));
+  if (nroots == 0) {
     FMM_CUDA(cudaMemsetAsync(s.box.p, 0, 16 * sizeof(T), s.stream));
+    s.root_cell.clear();
     return;
   }
-  // bounds and box
-  int nblk = std::min(ceil_div(n, TB), 148 * 4);
-  s.minmax_part.ensure(6 * nblk);
-  k_minmax_partial<T><<<nblk, TB, 0, s.stream>>>(s.bodies_in.p, n, s.minmax_part.p);
+  // bounds per root over chunks of at most 16384 bodies
+  const int CH = 16384;
+  std::vector<int> hb, he, hlo{0};
+  for (int r = 0; r < nroots; r++) {
+    for (int b0 = rfirst[r]; b0 < rfirst[r + 1]; b0 += CH) {
+      hb.push_back(b0);
+      he.push_back(std::min(b0 + CH, rfirst[r + 1]));
+    }
+    hlo.push_back((int)hb.size());
+  }
+  const int nch = (int)hb.size();
+  s.d_root_first.ensure(nroots + 1);
+  s.d_seg.ensure(2 * (size_t)nch + nroots + 1);
+  int* dcb = s.d_seg.p;
+  int* dce = dcb + nch;
+  int* dlo = dce + nch;
+  FMM_CUDA(cudaMemcpyAsync(s.d_root_first.p, rfirst.data(), sizeof(int) * (nroots + 1),
+                           cudaMemcpyHostToDevice, s.stream));
+  FMM_CUDA(cudaMemcpyAsync(dcb, hb.data(), sizeof(int) * nch, cudaMemcpyHostToDevice, s.stream));
+  FMM_CUDA(cudaMemcpyAsync(dce, he.data(), sizeof(int) * nch, cudaMemcpyHostToDevice, s.stream));
+  FMM_CUDA(cudaMemcpyAsync(dlo, hlo.data(), sizeof(int) * (nroots + 1), cudaMemcpyHostToDevice,
+                           s.stream));
+  s.minmax_part.ensure(6 * (size_t)nch);
+  k_minmax_chunks<T><<<nch, TB, 0, s.stream>>>(s.bodies_in.p, dcb, dce, s.minmax_part.p);
   FMM_LAUNCH_CHECK();
-  k_box<T><<<1, 32, 0, s.stream>>>(s.minmax_part.p, nblk, s.box.p);
+  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, dlo, s.minmax_part.p, s.box.p);
   FMM_LAUNCH_CHECK();
   phase_end(s, FMM_PHASE_BOUNDS);
   phase_begin(s, FMM_PHASE_TREE);
-  // keys and first sort
+  // keys and first sort (within each root's range)
   s.keys.ensure(n);
   s.keys2.ensure(n);
   s.idx.ensure(n);
   s.idx2.ensure(n);
-  k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, s.keys.p, s.idx.p);
+  k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, s.d_root_first.p,
+                                                  nroots, s.keys.p, s.idx.p);
   FMM_LAUNCH_CHECK();
-  sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, 3 * kMaxLevel);
+  if (nroots == 1)
+    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, 3 * kMaxLevel);
+  else
+    segmented_sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots,
+                             s.d_root_first.p, s.d_root_first.p + 1, 3 * kMaxLevel);
   // nodes, level by level
-  size_t cap0 = (size_t)std::max(1024, 4 * (n / std::max(1, s.cfg.ncrit)) + 64);
+  size_t cap0 = (size_t)std::max(1024, 4 * (n / std::max(1, s.cfg.ncrit)) + 64 + nroots);
   DevArr<int>* narr[] = {&s.nbegin, &s.ncount, &s.nparent, &s.nchildn, &s.nfirst,
-                         &s.nnode, &s.npos, &s.ncb, &s.nlevel};
+                         &s.nnode, &s.npos, &s.ncb, &s.nlevel, &s.nsid};
   for (auto* a : narr) a->ensure(cap0);
   s.nX.ensure(4 * cap0);
-  k_root<<<1, 1, 0, s.stream>>>(n, s.nbegin.p, s.ncount.p, s.nparent.p, s.nlevel.p);
-  FMM_LAUNCH_CHECK();
-  k_root_x<T><<<1, 1, 0, s.stream>>>(s.box.p, s.nX.p);
+  k_roots<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, s.d_root_first.p, s.box.p,
+                                                        s.nbegin.p, s.ncount.p, s.nparent.p,
+                                                        s.nlevel.p, s.nsid.p, s.nX.p);
   FMM_LAUNCH_CHECK();
   s.level_lo.push_back(0);
-  s.level_lo.push_back(1);
+  s.level_lo.push_back(nroots);
   for (int level = 0;; level++) {
     int lo = s.level_lo[level], hi = s.level_lo[level + 1];
     int m = hi - lo;
@@ -408,7 +472,7 @@ template <typename T> void build_tree(Solver<T>& s) {
     k_emit<T><<<ceil_div(m, TB), TB, 0, s.stream>>>(lo, hi, level, cnt, s.coff.p, s.nsplit.p,
                                                     s.box.p, s.nbegin.p, s.ncount.p,
                                                     s.nparent.p, s.nchildn.p, s.nfirst.p,
-                                                    s.nlevel.p, s.nX.p);
+                                                    s.nlevel.p, s.nsid.p, s.nX.p);
     FMM_LAUNCH_CHECK();
     s.level_lo.push_back(hi + total);
   }
@@ -422,10 +486,17 @@ template <typename T> void build_tree(Solver<T>& s) {
                                                         s.nnode.p);
     FMM_LAUNCH_CHECK();
   }
+  // first cell of each root: exclusive scan of the roots' subtree sizes
+  s.cbase.ensure(nroots + 1);
+  s.coff.ensure(nroots + 1);
+  FMM_CUDA(cudaMemsetAsync(s.coff.p + nroots, 0, sizeof(int), s.stream));
+  FMM_CUDA(cudaMemcpyAsync(s.coff.p, s.nnode.p, sizeof(int) * nroots, cudaMemcpyDeviceToDevice,
+                           s.stream));
+  exclusive_sum_int(s, s.coff.p, s.cbase.p, nroots + 1);
   for (int l = 0; l < nlev; l++) {
     int lo = s.level_lo[l], hi = s.level_lo[l + 1];
     k_pos<<<ceil_div(hi - lo, TB), TB, 0, s.stream>>>(lo, hi, s.nchildn.p, s.nfirst.p,
-                                                      s.nnode.p, s.npos.p, s.ncb.p);
+                                                      s.nnode.p, s.cbase.p, s.npos.p, s.ncb.p);
     FMM_LAUNCH_CHECK();
   }
   // cells
@@ -433,10 +504,11 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.c_ibody.ensure(nnodes); s.c_nbody.ensure(nnodes); s.c_level.ensure(nnodes);
   s.c_icell.ensure(nnodes);
   s.cX.ensure(nnodes);
+  s.c_root.ensure(nnodes);
   k_cells<T><<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(
-      nnodes, s.box.p, s.nbegin.p, s.ncount.p, s.nparent.p, s.nchildn.p, s.nlevel.p, s.npos.p,
-      s.ncb.p, s.nX.p, s.c_iparent.p, s.c_ichild.p, s.c_nchild.p, s.c_ibody.p, s.c_nbody.p,
-      s.c_level.p, s.c_icell.p, s.cX.p);
+      nnodes, s.box.p, s.nbegin.p, s.ncount.p, s.nparent.p, s.nchildn.p, s.nlevel.p, s.nsid.p,
+      s.cbase.p, s.npos.p, s.ncb.p, s.nX.p, s.c_iparent.p, s.c_ichild.p, s.c_nchild.p,
+      s.c_ibody.p, s.c_nbody.p, s.c_level.p, s.c_icell.p, s.cX.p, s.c_root.p);
   FMM_LAUNCH_CHECK();
   // bodies inside a leaf in input order (the stable partitions of the reference keep it)
   s.order.ensure(n);
@@ -453,10 +525,14 @@ template <typename T> void build_tree(Solver<T>& s) {
     FMM_LAUNCH_CHECK();
     k_tkey<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.keys2.p, s.idx2.p, blev, s.keys.p, s.order.p);
     FMM_LAUNCH_CHECK();
-    // s.order holds 0..n-1 (input positions); sort them by truncated key
+    // s.order holds 0..n-1 (input positions); sort them by truncated key within each root
     FMM_CUDA(cudaMemcpyAsync(s.idx.p, s.order.p, n * sizeof(int), cudaMemcpyDeviceToDevice,
                              s.stream));
-    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
+    if (nroots == 1)
+      sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
+    else
+      segmented_sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, nroots,
+                               s.d_root_first.p, s.d_root_first.p + 1, 3 * kMaxLevel);
   }
   s.bodies.ensure(n);
   k_permute<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.bodies_in.p, s.order.p, s.bodies.p);
@@ -474,6 +550,9 @@ template <typename T> void build_tree(Solver<T>& s) {
   k_leaf_scatter<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.nchildn.p, s.coff.p,
                                                             s.npos.p, s.leaves.p);
   FMM_LAUNCH_CHECK();
+  s.root_cell.resize(nroots);
+  FMM_CUDA(cudaMemcpyAsync(s.root_cell.data(), s.cbase.p, sizeof(int) * nroots,
+                           cudaMemcpyDeviceToHost, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
   s.nleaves = s.scal_host[0];
 }

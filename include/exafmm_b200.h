@@ -98,6 +98,22 @@ int fmm_b200_solve_device(fmm_b200_solver* s, int n, const void* d_bodies, void*
 int fmm_b200_solve_host(fmm_b200_solver* s, int n, const double* x, const double* q,
                         double* p, double* f);
 
+/* ---- batches of independent solves --------------------------------------------------- *
+ * nsolves solves with counts[s] bodies each, bodies concatenated in solve order (device
+ * 4-vectors or host doubles as above), results in the same layout.  The solves share one
+ * tree build, traversal and set of kernel launches ("forest": one root per non-empty
+ * solve, cells of a solve contiguous, no interaction across solves); every solve's result
+ * is bitwise the one it gets alone.  All solves use the handle's configuration.
+ * No reference counterpart: the reference solves one system per call. */
+int fmm_b200_solve_batch_device(fmm_b200_solver* s, int nsolves, const int* counts,
+                                const void* d_bodies, void* d_trg);
+int fmm_b200_solve_batch_host(fmm_b200_solver* s, int nsolves, const int* counts,
+                              const double* x, const double* q, double* p, double* f);
+int fmm_b200_set_bodies_batch_device(fmm_b200_solver* s, int nsolves, const int* counts,
+                                     const void* d_bodies);
+/* Roots after the tree build: their count, first cell, and solve index. */
+int fmm_b200_get_roots(fmm_b200_solver* s, int* nroots, int* root_cells, int* root_solves);
+
 /* ---- stages (the reference's class methods) ------------------------------------------ */
 int fmm_b200_set_bodies_host(fmm_b200_solver* s, int n, const double* x, const double* q);
 int fmm_b200_set_bodies_device(fmm_b200_solver* s, int n, const void* d_bodies);
@@ -129,6 +145,29 @@ int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2
                        long long* p2p_body_pairs);
 int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
 int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
+
+/* ---- serving: continuous batching of independent solves ------------------------------ *
+ * A server owns nworkers worker threads (one CUDA stream and one solver handle per order
+ * each) and a scheduler that batches pending requests of equal order P, in arrival order,
+ * within hbm_budget_bytes of estimated device memory and max_batch solves per batch.
+ * Batches on different workers overlap on the device; a request arriving while batches
+ * run joins the next batch a worker takes.  cfg supplies basis, theta, ncrit, nspawn,
+ * precision and device; P comes with each request.  submit copies the inputs; wait blocks
+ * until the request is done, copies p (n) and f (3n), and reports its latency (submit to
+ * done) and queueing time (submit to batch start) in seconds.  A request whose estimate
+ * exceeds the whole budget is rejected with FMM_ERR_NO_MEMORY.  destroy drains the queue.
+ * No reference counterpart. */
+typedef struct fmm_b200_server fmm_b200_server;
+int fmm_b200_server_create(const fmm_b200_config* cfg, double hbm_budget_bytes, int nworkers,
+                           int max_batch, fmm_b200_server** out);
+int fmm_b200_server_submit(fmm_b200_server* srv, int n, const double* x, const double* q,
+                           int P, long long* request_id);
+int fmm_b200_server_poll(fmm_b200_server* srv, long long request_id, int* done);
+int fmm_b200_server_wait(fmm_b200_server* srv, long long request_id, double* p, double* f,
+                         double* latency_s, double* queue_s);
+int fmm_b200_server_stats(fmm_b200_server* srv, long long* completed, long long* bodies,
+                          long long* batches, int* pending);
+int fmm_b200_server_destroy(fmm_b200_server* srv);
 
 /* ---- utilities ----------------------------------------------------------------------- */
 /* FP64 direct sum on the GPU: Traversal::direct + normalize (include/traversal.h:304-337)

@@ -82,6 +82,7 @@ SIGNATURES = {
     "fmm_b200_server_stats": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "fmm_b200_server_destroy": (_i, [_vp]),
     "fmm_b200_direct": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
+    "fmm_b200_direct_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_fp32_peak": (_i, [_i, _vp]),
     "fmm_b200_kernel_launches": (_ll, []),
     "FMM_Init": (None, [_i]),
@@ -128,6 +129,27 @@ def direct(xt, xs, qs, eps2=0.0, device=0):
     rc = lib.fmm_b200_direct(device, len(xt), _p(xt), len(xs), _p(xs), _p(qs), eps2, _p(out))
     if rc != FMM_OK:
         raise FmmError(rc, "direct sum failed")
+    return out
+
+
+DIRECT_NOALLOC_MAX_TARGETS = 32768
+DIRECT_NOALLOC_MAX_SOURCES = 65536
+
+
+def direct_noalloc(xt, xs, qs, eps2=0.0, device=0):
+    """direct() for callers that cannot allocate device memory (fmm_b200_direct_noalloc):
+    the same result, staged through a static 3.75 MiB device array instead of per-call
+    allocations.  At most DIRECT_NOALLOC_MAX_TARGETS targets and DIRECT_NOALLOC_MAX_SOURCES
+    sources; calls on one device share the array and must not overlap."""
+    lib = load_library()
+    xt = np.ascontiguousarray(xt, np.float64).reshape(-1, 3)
+    xs = np.ascontiguousarray(xs, np.float64).reshape(-1, 3)
+    qs = np.ascontiguousarray(qs, np.float64).reshape(-1)
+    out = np.zeros((len(xt), 4))
+    rc = lib.fmm_b200_direct_noalloc(device, len(xt), _p(xt), len(xs), _p(xs), _p(qs), eps2,
+                                     _p(out))
+    if rc != FMM_OK:
+        raise FmmError(rc, lib.fmm_b200_last_error(None).decode())
     return out
 
 

@@ -22,6 +22,9 @@ static thread_local std::string g_create_error;
 
 namespace fmmb200 {
 
+// message of a failed call that has no solver handle (read through fmm_b200_last_error(NULL))
+void set_call_error(const char* msg) { g_create_error = msg; }
+
 void phase_begin(SolverBase& s, int ph) {
   FMM_CUDA(cudaEventRecord(s.ev[2 * ph], s.stream));
 }

@@ -125,6 +125,8 @@ std::vector<int> cartesian_orders();
 // phase timing helpers (fmm_capi.cu)
 void phase_begin(SolverBase& s, int phase);
 void phase_end(SolverBase& s, int phase);
+// message of a failed call without a solver handle, read by fmm_b200_last_error(NULL)
+void set_call_error(const char* msg);
 
 // CUB wrappers compiled once (fmm_sort.cu)
 void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,

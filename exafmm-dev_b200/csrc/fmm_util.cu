@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "fmm_solver.cuh"
@@ -79,11 +81,77 @@ __global__ void __launch_bounds__(256) k_fma_probe(float* out, float s) {
   if (t == 123.456f) out[0] = t;  // keeps the chains live
 }
 
+// ---- FP64 direct sum without allocation (fmm_b200_direct_noalloc) ---------------------
+// The staging buffers of fmm_b200_direct (targets, sources, charges, output) live in one
+// fixed array in device memory instead of per-call cudaMalloc/cudaFree.  Layout for a call
+// (nt, ns), in doubles: targets [0, 3 nt), sources [3 nt, 3 nt + 3 ns), charges next (ns),
+// output next (4 nt): 7 nt + 4 ns doubles, at most 7 * 32768 + 4 * 65536 = 491,520
+// doubles (3.75 MiB) per device.  No part of it has to start at zero: a call copies in
+// every input it reads and the kernel writes every output that is copied back.
+constexpr int kNoAllocMaxTargets = FMM_DIRECT_NOALLOC_MAX_TARGETS;
+constexpr int kNoAllocMaxSources = FMM_DIRECT_NOALLOC_MAX_SOURCES;
+constexpr size_t kNoAllocDoubles =
+    7 * (size_t)kNoAllocMaxTargets + 4 * (size_t)kNoAllocMaxSources;
+static __device__ __align__(256) double g_direct_scratch[kNoAllocDoubles];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// device address of the array on `device` (which must be current), looked up once per
+// device: host code only sees a host-side stand-in under the array's name
+double* noalloc_scratch(int device) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_base[device]) {
+    void* p = nullptr;
+    FMM_CUDA(cudaGetSymbolAddress(&p, g_direct_scratch));
+    g_noalloc_base[device] = static_cast<double*>(p);
+  }
+  return g_noalloc_base[device];
+}
+
 }  // namespace
 
 extern "C" {
 
 long long fmm_b200_kernel_launches(void) { return g_launches.load(); }
+
+int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const double* xs,
+                            const double* qs, double eps2, double* out) {
+  if (nt < 0 || ns < 0 || (nt > 0 && (!xt || !out)) || (ns > 0 && (!xs || !qs)) ||
+      device < 0 || device >= kNoAllocMaxDevices) {
+    fmmb200::set_call_error("fmm_b200_direct_noalloc: invalid argument");
+    return FMM_ERR_INVALID;
+  }
+  if (nt > kNoAllocMaxTargets || ns > kNoAllocMaxSources) {
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "fmm_b200_direct_noalloc: %d targets / %d sources exceed the static scratch "
+                  "limits of %d targets / %d sources (fmm_b200_direct has none)",
+                  nt, ns, kNoAllocMaxTargets, kNoAllocMaxSources);
+    fmmb200::set_call_error(msg);
+    return FMM_ERR_INVALID;
+  }
+  if (nt == 0) return FMM_OK;
+  try {
+    FMM_CUDA(cudaSetDevice(device));
+    double* base = noalloc_scratch(device);
+    double *dxt = base, *dxs = base + 3 * (size_t)nt, *dqs = dxs + 3 * (size_t)ns,
+           *dout = dqs + ns;
+    FMM_CUDA(cudaMemcpy(dxt, xt, 24 * (size_t)nt, cudaMemcpyHostToDevice));
+    if (ns) {
+      FMM_CUDA(cudaMemcpy(dxs, xs, 24 * (size_t)ns, cudaMemcpyHostToDevice));
+      FMM_CUDA(cudaMemcpy(dqs, qs, 8 * (size_t)ns, cudaMemcpyHostToDevice));
+    }
+    k_direct<<<ceil_div(nt, kDirTile), kDirTile>>>(nt, dxt, ns, dxs, dqs, eps2, dout);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpy(out, dout, 32 * (size_t)nt, cudaMemcpyDeviceToHost));
+  } catch (const FmmError& e) {
+    fmmb200::set_call_error(e.what());
+    return e.code;
+  }
+  return FMM_OK;
+}
 
 int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
                     const double* qs, double eps2, double* out) {

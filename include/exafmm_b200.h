@@ -176,6 +176,27 @@ int fmm_b200_server_destroy(fmm_b200_server* srv);
  * are skipped.  Synchronous. */
 int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
                     const double* qs, double eps2, double* out);
+/* fmm_b200_direct without any device allocation: same arguments, kernel and (bitwise)
+ * result, with the device staging buffers in a static device array of 3.75 MiB (7 nt + 4 ns
+ * doubles), which every GPU that loads this library holds until the process exits, instead
+ * of a cudaMalloc/cudaFree per call.  For callers that cannot allocate device memory while
+ * they run: those whose device memory is all held by their own pool allocator, and those
+ * that must not take the device-wide synchronisation that cudaMalloc/cudaFree imply while
+ * other streams of theirs are busy.  No counterpart in the reference.
+ * Limits: nt <= FMM_DIRECT_NOALLOC_MAX_TARGETS and ns <= FMM_DIRECT_NOALLOC_MAX_SOURCES;
+ * larger sizes return FMM_ERR_INVALID, with the limits in fmm_b200_last_error(NULL), before
+ * the device is touched.  The first call on each device does the set-up: it looks up the
+ * array's address (cudaGetSymbolAddress, with that device current), which may load the
+ * library's device code; make that first call before any stream capture begins on the
+ * device.  Nothing in the array has to start at zero: a call copies in every input it reads
+ * and writes every output it returns.  All calls on one device share the array and it keeps
+ * the last call's contents: calls that overlap on the same GPU (from several host threads)
+ * race on it, and the caller must serialise them.  Synchronous: the result is in `out` when
+ * the call returns. */
+#define FMM_DIRECT_NOALLOC_MAX_TARGETS 32768
+#define FMM_DIRECT_NOALLOC_MAX_SOURCES 65536
+int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const double* xs,
+                            const double* qs, double eps2, double* out);
 /* FP32 FMA throughput of the device in TFLOP/s (independent FMA chains on every SM): the
  * roofline denominator of the FP32-pipe kernels (M2L, P2P).  No reference counterpart. */
 int fmm_b200_fp32_peak(int device, double* tflops);

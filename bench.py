@@ -19,6 +19,10 @@ use_rmax = use_ropt = 1, FP32 expansions with compensated potential/gradient sum
 * --impl reference: that reference CPU FMM as the timed arm (rank 0 only).
 * multi-GPU (torchrun): replicas only; every rank solves its own instance, no collective
   on the data path (a barrier and a max-reduction of the timings only).
+* batched (rank 0): 256 independent solves of uneven N in one batched call (a forest of
+  trees in one set of launches), against the same solves one call each.
+* serving (rank 0): the continuous-batching server under Poisson arrivals at three loads,
+  with p50/p99 latency, throughput and accuracy per expansion order.
 """
 import argparse
 import importlib
@@ -123,6 +127,175 @@ def run_reference_sample(ref, datasets, n, threads, seed=43):
     return wall, run.times()
 
 
+BATCH = dict(solves=256, n_min=1000, n_max=200000, P=8, theta=0.4, ncrit=64, nspawn=1000)
+SERVE = dict(requests=48, n_min=1000, n_max=1000000, orders=(6, 8, 10), theta=0.4, ncrit=64,
+             workers=3, max_batch=64, hbm_budget_gb=60.0, load=(0.3, 0.6, 0.9))
+
+
+def log_uniform_sizes(rng, count, lo, hi):
+    return np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), count))).astype(int)
+
+
+def rel_err(got, ref):
+    pot = float(np.sqrt(((got[:, 0] - ref[:, 0]) ** 2).sum() / (ref[:, 0] ** 2).sum()))
+    acc = float(np.sqrt(((got[:, 1:] - ref[:, 1:]) ** 2).sum() / (ref[:, 1:] ** 2).sum()))
+    return pot, acc
+
+
+def bench_batched(fmm, datasets, torch, dev, stream, flush, device, steps):
+    """256 independent solves (N log-uniform in [1e3, 2e5], cube / Plummer / sphere surface
+    by i mod 3, spherical P = 8, theta = 0.4, FP32 + compensation) in one batched call
+    (a forest of independent trees) against the same solves one call each."""
+    rng = np.random.default_rng(44)
+    sizes = log_uniform_sizes(rng, BATCH["solves"], BATCH["n_min"], BATCH["n_max"])
+    dists = ("cube", "plummer", "sphere")
+    xs, qs = [], []
+    for i, n in enumerate(sizes):
+        x, q = datasets.make(dists[i % 3], int(n), seed=1000 + i, precision="f32")
+        xs.append(x)
+        qs.append(q)
+    counts = sizes.astype(np.int32)
+    total = int(counts.sum())
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    host = np.concatenate([np.concatenate([x, q[:, None]], axis=1) for x, q in zip(xs, qs)])
+    bodies = torch.tensor(host, dtype=torch.float32, device=dev)
+    out = torch.empty_like(bodies)
+    kw = dict(basis="spherical", P=BATCH["P"], theta=BATCH["theta"], ncrit=BATCH["ncrit"],
+              nspawn=BATCH["nspawn"], use_rmax=1, use_ropt=1)
+    s = fmm.Solver(precision="f32", device=device, **kw)
+    s.set_stream(stream.cuda_stream)
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    batch = lambda: s.solve_batch_device(counts, bodies.data_ptr(), out.data_ptr())
+    for _ in range(3):
+        timed(batch)
+    ms = [timed(batch) for _ in range(max(3, steps // 2))]
+    phases = s.timings()
+    nm2l, np2p, body_pairs = s.list_counts()
+    res = out.cpu().numpy().astype(np.float64)
+
+    def one_by_one():
+        for i in range(len(counts)):
+            s.solve_device(int(counts[i]), bodies.data_ptr() + 16 * int(offs[i]),
+                           out.data_ptr() + 16 * int(offs[i]))
+
+    timed(one_by_one)
+    seq_ms = [timed(one_by_one) for _ in range(2)]
+    errs = []
+    for i in range(6):  # two solves of each distribution
+        idx = datasets.sample_targets(int(counts[i]), 256)
+        d = fmm.direct(xs[i][idx], xs[i], qs[i], device=device)
+        errs.append(rel_err(res[offs[i]:offs[i + 1]][idx], d))
+    del bodies, out, s
+    return {
+        "workload": "batched: %d solves, N log-uniform [%d, %d] (seed 44), cube/plummer/sphere "
+                    "by i mod 3, spherical P=%d theta=%.2f ncrit=%d, fp32 + compensation" % (
+                        BATCH["solves"], BATCH["n_min"], BATCH["n_max"], BATCH["P"],
+                        BATCH["theta"], BATCH["ncrit"]),
+        "bodies": total, "value": total / (float(np.median(ms)) * 1e-3), "unit": "particles/s",
+        "ms_per_batch": {"p50": float(np.median(ms)), "p99": float(np.percentile(ms, 99))},
+        "one_call_per_solve": {"ms": float(np.median(seq_ms)),
+                               "value": total / (float(np.median(seq_ms)) * 1e-3)},
+        "speedup_vs_one_call_per_solve": float(np.median(seq_ms)) / float(np.median(ms)),
+        "phases_ms": phases,
+        "work": {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs},
+        "accuracy": {"max_rel_l2_pot": max(e[0] for e in errs),
+                     "max_rel_l2_acc": max(e[1] for e in errs),
+                     "sample": "256 targets of each of solves 0-5, FP64 direct sum on the GPU"},
+        "l2": "256 MB flush before each timed batch"}
+
+
+def bench_serving(fmm, datasets, device):
+    """Continuous batching: Poisson arrivals of solves with N log-uniform in [1e3, 1e6],
+    P uniform over {6, 8, 10}, cube or Plummer bodies (FP32 + compensation), submitted
+    through the host C ABI at three loads (fractions of the capacity measured by a burst)."""
+    import threading as th
+    rng = np.random.default_rng(45)
+    R = SERVE["requests"]
+    sizes = log_uniform_sizes(rng, R, SERVE["n_min"], SERVE["n_max"])
+    orders = rng.choice(SERVE["orders"], R)
+    reqs = []
+    for i in range(R):
+        x, q = datasets.make(("cube", "plummer")[i % 2], int(sizes[i]), seed=2000 + i,
+                             precision="f32")
+        reqs.append((x, q, int(orders[i])))
+    total = int(sizes.sum())
+    srv = fmm.Server(theta=SERVE["theta"], ncrit=SERVE["ncrit"], workers=SERVE["workers"],
+                     max_batch=SERVE["max_batch"], hbm_budget_gb=SERVE["hbm_budget_gb"],
+                     device=device)
+
+    def run(gaps):
+        ids, t0 = [None] * R, time.perf_counter()
+
+        def submitter():
+            t = t0
+            for i, (x, q, P) in enumerate(reqs):
+                t += gaps[i]
+                d = t - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(x, q, P)
+
+        st = th.Thread(target=submitter)
+        st.start()
+        st.join()
+        outs, lat, que = [None] * R, [], []
+        for i in range(R):
+            o, l, qd = srv.wait(ids[i])
+            outs[i] = o
+            lat.append(l)
+            que.append(qd)
+        wall = time.perf_counter() - t0
+        return outs, np.array(lat), np.array(que), wall
+
+    b0 = srv.stats()["batches"]
+    run(np.zeros(R))  # warm-up: handles per order, pinned staging
+    outs, lat, que, wall = run(np.zeros(R))  # burst: every request at t = 0
+    capacity = R / wall
+    sweep = [{"load": "burst", "lambda_rps": None, "p50_ms": 1e3 * float(np.median(lat)),
+              "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+              "queue_p50_ms": 1e3 * float(np.median(que)), "particles_per_s": total / wall}]
+    for f in SERVE["load"]:
+        lam = f * capacity
+        gaps = rng.exponential(1.0 / lam, R)
+        gaps[0] = 0.0
+        _, lat, que, wall = run(gaps)
+        sweep.append({"load": f, "lambda_rps": lam, "p50_ms": 1e3 * float(np.median(lat)),
+                      "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                      "queue_p50_ms": 1e3 * float(np.median(que)),
+                      "particles_per_s": total / wall})
+    st = srv.stats()
+    srv.close()
+    errs = {}
+    for i in range(R):
+        P = reqs[i][2]
+        if P in errs or sizes[i] < 20000:
+            continue
+        x, q = reqs[i][0], reqs[i][1]
+        idx = datasets.sample_targets(len(q), 256)
+        errs[P] = rel_err(outs[i][idx], fmm.direct(x[idx], x, q, device=device))
+    return {
+        "workload": "serving: %d requests, N log-uniform [%d, %d] (seed 45), P in %s, "
+                    "cube/plummer, theta=%.2f ncrit=%d, fp32 + compensation; %d workers, "
+                    "max batch %d, HBM budget %.0f GB; host double buffers through the C ABI" % (
+                        R, SERVE["n_min"], SERVE["n_max"], list(SERVE["orders"]),
+                        SERVE["theta"], SERVE["ncrit"], SERVE["workers"], SERVE["max_batch"],
+                        SERVE["hbm_budget_gb"]),
+        "bodies_per_pass": total, "capacity_rps": capacity, "sweep": sweep,
+        "batches": st["batches"] - b0,
+        "accuracy": {str(P): {"rel_l2_pot": e[0], "rel_l2_acc": e[1]} for P, e in errs.items()},
+        "latency": "submit to result ready, host clock; Poisson gaps at load x capacity"}
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -180,6 +353,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=REF_SAMPLE_N)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop line")
     ap.add_argument("--profile", action="store_true",
                     help="warm-ups, then one solve between cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off), then exit")
@@ -323,6 +498,10 @@ def main():
             pg.destroy_process_group()
         return
 
+    batched = None if args.no_batch else bench_batched(fmm, datasets, torch, dev, stream, flush,
+                                                       local, args.steps)
+    serving = None if args.no_serve else bench_serving(fmm, datasets, local)
+
     peak = fmm.fp32_peak_tflops(local)
     m2l_flops = nm2l * m2l_flops_per_pair(WORKLOAD["P"])
     m2l_tflops = m2l_flops / (phases["m2l"] * 1e-3) / 1e12
@@ -369,6 +548,8 @@ def main():
                      "frac": m2l_tflops / peak, "traffic": traffic,
                      "peak_source": "fmm_b200_fp32_peak: FMA probe measured on this GPU in this run"},
         "cpu_baseline": cpu,
+        "batched": batched,
+        "serving": serving,
         "clocks": clk,
         "gpu_launches": int(launches),
     }

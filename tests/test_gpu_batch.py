@@ -20,6 +20,9 @@ def mixed_solves(datasets, sizes, seed=0, precision="f32"):
     dists = ("cube", "plummer", "sphere")
     out = []
     for i, n in enumerate(sizes):
+        if n == 0:  # an empty solve in the batch
+            out.append((np.zeros((0, 3)), np.zeros(0)))
+            continue
         x, q = datasets.make(dists[i % 3], n, seed=seed + i, precision=precision)
         out.append((x, q))
     return out

@@ -6,9 +6,9 @@
 // take every G-th source; a leaf of 33..64 bodies gives each lane two targets that share
 // every staged source.  Source leaves stream through shared memory 32 bodies at a time
 // (one coalesced 16-byte load per lane, read back as a broadcast), the inner loop is
-// FP32 FMA + one rsqrt per pair, and each source leaf's plain FP32 partial sum is folded
-// into a compensated (TwoSum) accumulator, so the accumulation error does not grow with
-// the number of source leaves.  Pairs with r^2 == 0 are skipped, as the reference does
+// FP32 FMA + one rsqrt per pair (no r^2 == 0 test outside the target leaf itself), and
+// each source leaf's plain FP32 partial sum is folded into a compensated (TwoSum)
+// accumulator, so the accumulation error does not grow with the number of source leaves.  Pairs with r^2 == 0 are skipped, as the reference does
 // (:149); the result is per unit target charge (the reference multiplies by q_i in P2P
 // and divides again in L2P / normalize).
 #include <algorithm>
@@ -19,18 +19,53 @@ namespace fmmb200 {
 
 constexpr int kP2PWarps = 4;
 
-template <typename T>
+// 1/sqrt with subnormal inputs flushed to zero (PTX rsqrt.approx.ftz.f32): no handling of
+// subnormal inputs and no r^2 == 0 test, for the source leaves where neither can occur
+__device__ __forceinline__ float rsqrt_ftz(float a) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ double rsqrt_ftz(double a) { return rsqrt(a); }
+
+// one pair; EXACT: skip r^2 == 0 and take subnormal r^2 as it is (the reference's
+// arithmetic); otherwise an r^2 of zero or below the normal range makes `pot` non-finite
+template <typename T, bool EXACT = true>
 __device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, T eps2, T& pot,
                                           T& ax, T& ay, T& az) {
   const T dx = sj.x - xi.x, dy = sj.y - xi.y, dz = sj.z - xi.z;
   const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-  const T inv = r2 > T(0) ? rsqrt_(r2) : T(0);
+  const T inv = EXACT ? (r2 > T(0) ? rsqrt_(r2) : T(0)) : rsqrt_ftz(r2);
   const T qinv = sj.w * inv;
   const T inv3 = qinv * inv * inv;
   pot += qinv;
   ax = fma(dx, inv3, ax);
   ay = fma(dy, inv3, ay);
   az = fma(dz, inv3, az);
+}
+
+// all bodies of one source leaf (first body j0, nj bodies) on the lane's TPL targets, its
+// sums started from zero; sources are staged through the warp's shared row 32 at a time
+template <typename T, int TPL, bool EXACT>
+__device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32], int sub, int G,
+                                            int j0, int nj, const vec4<T>* __restrict__ bodies,
+                                            T eps2, const vec4<T>* xi, T* pot, T* ax, T* ay,
+                                            T* az) {
+#pragma unroll
+  for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
+  for (int jb = 0; jb < nj; jb += 32) {
+    const int cnt = min(32, nj - jb);
+    __syncwarp();
+    if (lane < cnt) sh[wl][lane] = bodies[j0 + jb + lane];
+    __syncwarp();
+#pragma unroll 4
+    for (int k = sub; k < cnt; k += G) {
+      const vec4<T> sj = sh[wl][k];
+#pragma unroll
+      for (int u = 0; u < TPL; u++)
+        p2p_accum<T, EXACT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u]);
+    }
+  }
 }
 
 // TPL targets per lane (1 or 2): a lane holds targets ti and ti + 32 / G and reuses every
@@ -68,19 +103,21 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
       njn = nbody[cn];
     }
     T pot[TPL], ax[TPL], ay[TPL], az[TPL];
+    // Bodies at one position share every octant and so one leaf: only the target leaf
+    // itself can hold a pair at r^2 == 0.  Other source leaves take the fast pair form;
+    // if a pair underflowed to r^2 == 0 or below the normal range there, its sum is not
+    // finite and the leaf is summed again in the exact form, so results are always those
+    // of the exact form.
+    const bool self = j0 == b0;
+    if (!self) {
+      source_leaf<T, TPL, false>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
+      bool bad = false;
 #pragma unroll
-    for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
-    for (int jb = 0; jb < nj; jb += 32) {
-      const int cnt = min(32, nj - jb);
-      __syncwarp();
-      if (lane < cnt) sh[wl][lane] = bodies[j0 + jb + lane];
-      __syncwarp();
-#pragma unroll 4
-      for (int k = sub; k < cnt; k += G) {
-        const vec4<T> sj = sh[wl][k];
-#pragma unroll
-        for (int u = 0; u < TPL; u++) p2p_accum(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u]);
-      }
+      for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(pot[u]);
+      if (__any_sync(0xffffffffu, bad))
+        source_leaf<T, TPL, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
+    } else {
+      source_leaf<T, TPL, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
     }
 #pragma unroll
     for (int u = 0; u < TPL; u++) {

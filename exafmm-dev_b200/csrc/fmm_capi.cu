@@ -260,8 +260,8 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
   s.ncoef = cfg->basis == FMM_SPHERICAL ? 2 * s.nterm : s.nterm;
   try {
     FMM_CUDA(cudaSetDevice(cfg->device));
-    s.scal.ensure(64);
-    FMM_CUDA(cudaMallocHost((void**)&s.scal_host, 64 * sizeof(int)));
+    s.scal.ensure(512);
+    FMM_CUDA(cudaMallocHost((void**)&s.scal_host, 512 * sizeof(int)));
     for (int i = 0; i < 2 * FMM_NUM_PHASES; i++) FMM_CUDA(cudaEventCreate(&s.ev[i]));
   } catch (const FmmError& e) {
     g_create_error = e.what();

@@ -81,6 +81,7 @@ struct SolverBase {
   DevArr<int> order;
   // interaction lists
   DevArr<int2> front, front2;
+  bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
   DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches

@@ -133,6 +133,83 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
   }
 }
 
+// One traversal step without a count pass, for a solver whose list and frontier buffers
+// were sized by an earlier solve.  The frontier size is read on the device (no host round
+// trip per step); output slots come from one warp-wide scan of a packed (M2L, P2P,
+// children) count and three atomics per warp.  Writes beyond a buffer's capacity are
+// skipped but still counted, so the host can tell an overflow from the final counts and
+// redo the traversal with the counted path.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
+                unsigned long long front_cap, const vec4<T>* __restrict__ X,
+                const int* __restrict__ nchild, const int* __restrict__ ichild,
+                const int* __restrict__ nbody, int nspawn, int ncells,
+                unsigned long long* __restrict__ ctr,  // [0] M2L, [1] P2P, [2] bad index
+                unsigned long long* __restrict__ next_count, unsigned long long* __restrict__ m2l,
+                unsigned long long m2l_cap, unsigned long long* __restrict__ p2p,
+                unsigned long long p2p_cap, int2* __restrict__ next,
+                unsigned long long next_cap) {
+  const long long nfront = (long long)min(*nfront_p, front_cap);
+  const int lane = lane_id();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane;
+  for (long long w = wbase; w < nfront; w += stride) {  // warp-uniform trip count
+    const long long t = w + lane;
+    int ty = -1, k = 0;
+    int2 p = make_int2(0, 0);
+    if (t < nfront) {
+      p = front[t];
+      if ((unsigned)p.x < (unsigned)ncells && (unsigned)p.y < (unsigned)ncells)
+        ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+      else
+        atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
+    }
+    // packed counts: M2L in bits 0-7, P2P in 8-15, children in 16-31 (warp totals fit)
+    const unsigned v = (ty == PAIR_M2L ? 1u : 0u) | (ty == PAIR_P2P ? 1u << 8 : 0u) |
+                       (ty >= PAIR_SPLIT_I ? (unsigned)k << 16 : 0u);
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long bm = 0, bp = 0, bn = 0;
+    if (lane == 31) {
+      if (tot & 0xffu) bm = atomicAdd(&ctr[0], (unsigned long long)(tot & 0xffu));
+      if ((tot >> 8) & 0xffu) bp = atomicAdd(&ctr[1], (unsigned long long)((tot >> 8) & 0xffu));
+      if (tot >> 16) bn = atomicAdd(next_count, (unsigned long long)(tot >> 16));
+    }
+    bm = __shfl_sync(0xffffffffu, bm, 31);
+    bp = __shfl_sync(0xffffffffu, bp, 31);
+    bn = __shfl_sync(0xffffffffu, bn, 31);
+    const unsigned ex = incl - v;
+    const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+    if (ty == PAIR_M2L) {
+      const unsigned long long o = bm + (ex & 0xffu);
+      if (o < m2l_cap) m2l[o] = packed;
+    } else if (ty == PAIR_P2P) {
+      const unsigned long long o = bp + ((ex >> 8) & 0xffu);
+      if (o < p2p_cap) p2p[o] = packed;
+    } else if (ty >= PAIR_SPLIT_I) {
+      // every slot below the capacity is written (the next step reads up to it)
+      const unsigned long long o = bn + (ex >> 16);
+      const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k, next_cap - o);
+      if (ty == PAIR_SPLIT_I) {
+        const int c0 = ichild[p.x];
+        for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p.y);
+      } else if (ty == PAIR_SPLIT_J) {
+        const int c0 = ichild[p.y];
+        for (int j = 0; j < kw; j++) next[o + j] = make_int2(p.x, c0 + j);
+      } else {
+        const int ci0 = ichild[p.x], cj0 = ichild[p.y], nj = nchild[p.y];
+        for (int i = 0; i < kw; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+      }
+    }
+  }
+}
+
 // CSR offsets of a sorted packed list: off[c] = first pair whose target >= c
 __global__ void k_csr(const unsigned long long* __restrict__ pairs, long long n, int ncells,
                       int* __restrict__ off) {
@@ -191,20 +268,26 @@ static int bits_for(int n) {
   return b;
 }
 
-template <typename T> void build_lists(Solver<T>& s) {
-  const int TB = 256;
-  s.nm2l = s.np2p = s.p2p_body_pairs = 0;
-  if (s.ncells == 0) return;
-  unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
-  unsigned long long* hc = (unsigned long long*)s.scal_host;
+template <typename T> static void upload_roots(Solver<T>& s) {
   // one (root, root) pair per solve of the batch: lists never cross solves
   std::vector<int2> roots(s.nroots);
   for (int r = 0; r < s.nroots; r++) roots[r] = make_int2(s.root_cell[r], s.root_cell[r]);
   s.front.ensure(std::max(s.nroots, 1));
   FMM_CUDA(cudaMemcpyAsync(s.front.p, roots.data(), sizeof(int2) * s.nroots,
                            cudaMemcpyHostToDevice, s.stream));
-  long long nfront = s.nroots;
-  long long nm2l = 0, np2p = 0;
+  FMM_CUDA(cudaStreamSynchronize(s.stream));  // roots[] lives on the host stack
+}
+
+// Traversal with the sizes known up front: per step a count pass, one host read of the
+// three totals, buffers grown to fit, then the write pass.  Returns the largest frontier.
+template <typename T>
+static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
+  const int TB = 256;
+  unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
+  unsigned long long* hc = (unsigned long long*)s.scal_host;
+  upload_roots(s);
+  long long nfront = s.nroots, maxfront = s.nroots;
+  nm2l = np2p = 0;
   s.m2l.ensure(1024);
   s.p2p.ensure(1024);
   while (nfront > 0) {
@@ -240,12 +323,68 @@ template <typename T> void build_lists(Solver<T>& s) {
                                                s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn, cnt,
                                                s.m2l.p, s.p2p.p, s.front2.p);
     FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
     nm2l += am;
     np2p += ap;
     nfront = an;
+    maxfront = std::max(maxfront, an);
     std::swap(s.front, s.front2);
   }
-  FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
+  return maxfront;
+}
+
+// Traversal on buffers sized by an earlier solve: a fixed number of steps (enough for the
+// deepest pair of cells), frontier sizes kept on the device, one host read at the end.
+// Returns false, with the lists incomplete, when a buffer was too small or the steps did
+// not reach the end.
+template <typename T>
+static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
+  const int TB = 256;
+  const int steps = 2 * (s.maxlevel + 1) + 2;
+  // [0] M2L total, [1] P2P total, [2] invalid-index flag, [3 + l] frontier size of step l
+  unsigned long long* ctr = (unsigned long long*)s.scal.p + 32;
+  unsigned long long* hctr = (unsigned long long*)s.scal_host + 32;
+  upload_roots(s);
+  FMM_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * (4 + steps), s.stream));
+  hctr[3] = (unsigned long long)s.nroots;
+  FMM_CUDA(cudaMemcpyAsync(ctr + 3, hctr + 3, sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice, s.stream));
+  const unsigned long long fcap = std::min(s.front.cap, s.front2.cap);
+  for (int l = 0; l < steps; l++) {
+    DevArr<int2>& in = (l & 1) ? s.front2 : s.front;
+    DevArr<int2>& out = (l & 1) ? s.front : s.front2;
+    k_trav_step<T><<<148 * 8, TB, 0, s.stream>>>(
+        in.p, ctr + 3 + l, fcap, s.cX.p, s.c_nchild.p, s.c_ichild.p, s.c_nbody.p,
+        s.cfg.nspawn, s.ncells, ctr, ctr + 4 + l, s.m2l.p, s.m2l.cap, s.p2p.p, s.p2p.cap,
+        out.p, fcap);
+    FMM_LAUNCH_CHECK();
+  }
+  FMM_CUDA(cudaMemcpyAsync(hctr, ctr, sizeof(unsigned long long) * (4 + steps),
+                           cudaMemcpyDeviceToHost, s.stream));
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  if (hctr[2]) throw FmmError(FMM_ERR_DEVICE, "traversal read a cell index out of range");
+  nm2l = (long long)hctr[0];
+  np2p = (long long)hctr[1];
+  if (hctr[0] > s.m2l.cap || hctr[1] > s.p2p.cap || hctr[3 + steps] != 0) return false;
+  for (int l = 0; l <= steps; l++)
+    if (hctr[3 + l] > fcap) return false;
+  return true;
+}
+
+template <typename T> void build_lists(Solver<T>& s) {
+  const int TB = 256;
+  s.nm2l = s.np2p = s.p2p_body_pairs = 0;
+  if (s.ncells == 0) return;
+  unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
+  unsigned long long* hc = (unsigned long long*)s.scal_host;
+  long long nm2l = 0, np2p = 0;
+  if (!s.trav_sized || !fast_traversal(s, nm2l, np2p)) {
+    const long long maxfront = counted_traversal(s, nm2l, np2p);
+    // size the buffers for the next solves of this handle (the 25% headroom of DevArr)
+    s.front.ensure(maxfront);
+    s.front2.ensure(maxfront);
+    s.trav_sized = true;
+  }
   s.nm2l = nm2l;
   s.np2p = np2p;
   // sort on (target << b | source) with b = bits(ncells): 2b key bits instead of 32 + b

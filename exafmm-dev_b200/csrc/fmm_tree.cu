@@ -147,29 +147,73 @@ __global__ void k_split(int lo, int hi, int level, int ncrit,
                         const unsigned long long* __restrict__ keys,
                         const int* __restrict__ nbegin, const int* __restrict__ ncount,
                         int* __restrict__ cnt, int* __restrict__ starts) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int m = hi - lo;
-  if (t == m) cnt[m] = 0;
-  if (t >= m) return;
-  int v = lo + t;
-  int b = nbegin[v], c = ncount[v];
+  // one warp per node: the 7 octant boundaries of its sorted key range are found together
+  // by 32-ary searches (32 samples per boundary and round, all loads of a round
+  // independent), so a node of c bodies needs log32(c) dependent rounds instead of the
+  // 7 log2(c) of a binary search per boundary
+  const int lane = lane_id();
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int m = hi - lo;
+  if (w == m && lane == 0) cnt[m] = 0;
+  if (w >= m) return;
+  const int v = lo + (int)w;
+  const int b = nbegin[v], c = ncount[v];
   int nch = 0;
-  int* st = starts + 9 * t;
   if (c > ncrit && level < kMaxLevel) {
-    st[0] = b;
-    st[8] = b + c;
+    int* st = starts + 9 * w;
+    int slo[8], shi[8];
+#pragma unroll
     for (int o = 1; o < 8; o++) {
-      int a = b, z = b + c;
-      while (a < z) {
-        int mid = (a + z) >> 1;
-        if (digit_at(keys[mid], level) < o) a = mid + 1;
-        else z = mid;
-      }
-      st[o] = a;
+      slo[o] = b;
+      shi[o] = b + c;
     }
-    for (int o = 0; o < 8; o++) nch += st[o + 1] > st[o];
+    // invariant: the first index whose octant digit is >= o lies in [slo[o], shi[o]]
+    for (;;) {
+      bool open = false;
+#pragma unroll
+      for (int o = 1; o < 8; o++) open |= slo[o] < shi[o];
+      if (!open) break;
+      unsigned ball[8];
+      int step[8];
+#pragma unroll
+      for (int o = 1; o < 8; o++) {
+        const int len = shi[o] - slo[o];
+        step[o] = len <= 32 ? 1 : (len + 31) / 32;
+        const long long idx = slo[o] + (long long)lane * step[o];
+        const bool pred = len > 0 && idx < shi[o] && digit_at(keys[idx], level) < o;
+        ball[o] = __ballot_sync(0xffffffffu, pred);
+      }
+#pragma unroll
+      for (int o = 1; o < 8; o++) {
+        if (slo[o] >= shi[o]) continue;
+        const int t = __popc(ball[o]);
+        if (step[o] == 1) {
+          slo[o] = shi[o] = slo[o] + t;
+        } else if (t == 0) {
+          shi[o] = slo[o];
+        } else {
+          const long long nlo = slo[o] + (long long)(t - 1) * step[o] + 1;
+          const long long nhi = slo[o] + (long long)t * step[o];
+          shi[o] = (int)(nhi < shi[o] ? nhi : shi[o]);
+          slo[o] = (int)nlo;
+        }
+      }
+    }
+    if (lane == 0) {
+      st[0] = b;
+      st[8] = b + c;
+#pragma unroll
+      for (int o = 1; o < 8; o++) st[o] = slo[o];
+    }
+    int prev = b;
+#pragma unroll
+    for (int o = 1; o < 8; o++) {
+      nch += slo[o] > prev;
+      prev = slo[o];
+    }
+    nch += b + c > prev;
   }
-  cnt[t] = nch;
+  if (lane == 0) cnt[w] = nch;
 }
 
 template <typename T>
@@ -453,7 +497,7 @@ template <typename T> void build_tree(Solver<T>& s) {
     s.coff.ensure(m + 1);
     s.idx.ensure(std::max((size_t)n, (size_t)m + 1));
     int* cnt = s.idx.p;  // the input-order index array is free until the second sort
-    k_split<<<ceil_div(m + 1, TB), TB, 0, s.stream>>>(lo, hi, level, s.cfg.ncrit, s.keys2.p,
+    k_split<<<ceil_div(32LL * (m + 1), TB), TB, 0, s.stream>>>(lo, hi, level, s.cfg.ncrit, s.keys2.p,
                                                        s.nbegin.p, s.ncount.p, cnt, s.nsplit.p);
     FMM_LAUNCH_CHECK();
     exclusive_sum_int(s, cnt, s.coff.p, m + 1);

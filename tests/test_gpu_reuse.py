@@ -1,0 +1,46 @@
+"""A solver handle reused across solves.
+
+The first traversal of a handle counts every step before writing it and sizes the list
+and frontier buffers; later traversals run without count passes on those buffers and fall
+back to the counted form when a buffer turns out too small.  Both forms must give the same
+lists (they are sorted by target and source) and therefore bitwise the same results.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+fmm = importlib.import_module("exafmm-dev_b200")
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_second_traversal_gives_the_same_lists(prec, datasets):
+    x, q = datasets.make("plummer", 40000, seed=5, precision=prec)
+    s = fmm.Solver(P=6, theta=0.4, ncrit=32, precision=prec)
+    s.set_bodies(x, q)
+    s.build_tree()
+    s.upward_pass()
+    s.traverse()                      # counted form (first traversal of the handle)
+    m2l1, p2p1 = s.lists()
+    s.traverse()                      # device-counted form on the sized buffers
+    m2l2, p2p2 = s.lists()
+    assert len(m2l1) > 0 and len(p2p1) > 0
+    assert np.array_equal(m2l1, m2l2)
+    assert np.array_equal(p2p1, p2p2)
+
+
+def test_growing_inputs_on_one_handle_match_fresh_handles(datasets):
+    # each input needs larger buffers than the one before: the device-counted traversal
+    # overflows, is detected, and the counted form redoes it
+    s = fmm.Solver(P=6, theta=0.4, ncrit=32)
+    for k, n in enumerate((2000, 30000, 120000, 5000)):
+        x, q = datasets.make(("cube", "plummer", "sphere", "plummer")[k], n, seed=20 + k,
+                             precision="f32")
+        got = s.solve(x, q)
+        fresh = fmm.Solver(P=6, theta=0.4, ncrit=32)
+        ref = fresh.solve(x, q)
+        ok = ~np.isnan(ref)
+        assert np.array_equal(np.isnan(got), np.isnan(ref))
+        assert np.array_equal(got[ok], ref[ok]), n
+        assert s.list_counts() == fresh.list_counts()

@@ -279,6 +279,7 @@ def bench_serving(fmm, datasets, device):
                       "queue_p50_ms": 1e3 * float(np.median(que)),
                       "particles_per_s": total / wall})
     st = srv.stats()
+    prof = srv.profile()
     srv.close()
     errs = {}
     for i in range(R):
@@ -297,6 +298,7 @@ def bench_serving(fmm, datasets, device):
                                    SERVE["workers"], SERVE["max_batch"], SERVE["hbm_budget_gb"]),
         "bodies_per_pass": total, "capacity_rps": capacity, "sweep": sweep,
         "batches": st["batches"] - b0,
+        "worker_seconds_all_passes": prof,
         "accuracy": {str(P): {"rel_l2_pot": e[0], "rel_l2_acc": e[1]} for P, e in errs.items()},
         "latency": "submit to result ready, host clock; Poisson gaps at load x capacity"}
 

@@ -80,6 +80,7 @@ SIGNATURES = {
     "fmm_b200_server_poll": (_i, [_vp, _ll, _vp]),
     "fmm_b200_server_wait": (_i, [_vp, _ll, _vp, _vp, _vp, _vp]),
     "fmm_b200_server_stats": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "fmm_b200_server_profile": (_i, [_vp, _vp, _vp, _vp]),
     "fmm_b200_server_destroy": (_i, [_vp]),
     "fmm_b200_direct": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_direct_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
@@ -415,6 +416,12 @@ class Server:
         a, b, c, d = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_int()
         self.lib.fmm_b200_server_stats(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
         return dict(completed=a.value, bodies=b.value, batches=c.value, pending=d.value)
+
+    def profile(self):
+        """Worker seconds: staging inputs, batched solves, copying results out."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self.lib.fmm_b200_server_profile(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return dict(stage_s=a.value, solve_s=b.value, unstage_s=c.value)
 
     def close(self):
         if getattr(self, "h", None):

@@ -68,6 +68,8 @@ struct fmm_b200_server {
   bool stop = false;
   long long next_id = 1;
   long long completed = 0, bodies_done = 0, batches = 0;
+  // worker seconds spent staging inputs, in the batched solve, and copying results out
+  double t_stage = 0, t_solve = 0, t_unstage = 0;
   std::string err;
 };
 
@@ -121,6 +123,7 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
       }
     }
     const auto t_start = Clock::now();
+    auto t_a = t_start, t_b = t_start;
     if (rc == FMM_OK) {
       double *x = W->pin, *q = x + 3 * n, *p = q + n, *f = p + n;
       size_t o = 0;
@@ -129,7 +132,9 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
         std::memcpy(q + o, r->q.data(), sizeof(double) * r->n);
         o += r->n;
       }
+      t_a = Clock::now();
       rc = fmm_b200_solve_batch_host(h, (int)counts.size(), counts.data(), x, q, p, f);
+      t_b = Clock::now();
       if (rc == FMM_OK) {
         o = 0;
         for (auto& r : batch) {
@@ -152,6 +157,9 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
         S->bodies_done += r->n;
       }
       S->batches++;
+      S->t_stage += std::chrono::duration<double>(t_a - t_start).count();
+      S->t_solve += std::chrono::duration<double>(t_b - t_a).count();
+      S->t_unstage += std::chrono::duration<double>(t_done - t_b).count();
       W->busy = false;
       if (rc != FMM_OK && h) S->err = fmm_b200_last_error(h);
     }
@@ -288,6 +296,16 @@ int fmm_b200_server_stats(fmm_b200_server* S, long long* completed, long long* b
   if (bodies) *bodies = S->bodies_done;
   if (batches) *batches = S->batches;
   if (pending) *pending = (int)S->pending.size();
+  return FMM_OK;
+}
+
+int fmm_b200_server_profile(fmm_b200_server* S, double* stage_s, double* solve_s,
+                            double* unstage_s) {
+  if (!S) return FMM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (stage_s) *stage_s = S->t_stage;
+  if (solve_s) *solve_s = S->t_solve;
+  if (unstage_s) *unstage_s = S->t_unstage;
   return FMM_OK;
 }
 

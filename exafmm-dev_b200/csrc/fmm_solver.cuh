@@ -80,6 +80,10 @@ struct SolverBase {
   DevArr<unsigned long long> c_icell;
   DevArr<int> order;
   // interaction lists
+  DevArr<unsigned> fs_root, fs_root2;  // forest sort: root of each key-sorted body
+  DevArr<int> fs_pos, fs_pos2;
+  DevArr<unsigned long long> fs_keys;
+  DevArr<int> fs_idx;
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
   DevArr<unsigned long long> m2l, p2p, list_tmp;
@@ -134,6 +138,8 @@ void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long 
                     const int* vin, int* vout, int n, int end_bit);
 void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
                    int n, int end_bit);
+void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,
+                    int* vout, int n, int end_bit);
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n);
 void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
                               unsigned long long* kout, const int* vin, int* vout, int n,

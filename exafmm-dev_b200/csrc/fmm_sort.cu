@@ -39,6 +39,17 @@ void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
                                                     nseg, begin, end, 0, end_bit, s.stream));
 }
 
+void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,
+                    int* vout, int n, int end_bit) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  FMM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit,
+                                           s.stream));
+  s.cub_tmp.ensure(bytes);
+  FMM_CUDA(cub::DeviceRadixSort::SortPairs(s.cub_tmp.p, bytes, kin, kout, vin, vout, n, 0,
+                                           end_bit, s.stream));
+}
+
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n) {
   if (n <= 0) return;
   size_t bytes = 0;

@@ -135,10 +135,13 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
 
 // One traversal step without a count pass, for a solver whose list and frontier buffers
 // were sized by an earlier solve.  The frontier size is read on the device (no host round
-// trip per step); output slots come from one warp-wide scan of a packed (M2L, P2P,
-// children) count and three atomics per warp.  Writes beyond a buffer's capacity are
-// skipped but still counted, so the host can tell an overflow from the final counts and
-// redo the traversal with the counted path.
+// trip per step).  Each lane takes kTravItems consecutive frontier pairs (their loads are
+// independent); output slots come from one warp-wide scan of the lanes' packed (M2L, P2P,
+// children) counts and three atomics per warp.  Writes beyond a buffer's capacity are
+// skipped but every slot below it is written and all are counted, so the host can tell an
+// overflow from the final counts and redo the traversal in the counted form.
+constexpr int kTravItems = 4;
+
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
@@ -152,27 +155,36 @@ __global__ void __launch_bounds__(256)
                 unsigned long long next_cap) {
   const long long nfront = (long long)min(*nfront_p, front_cap);
   const int lane = lane_id();
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane;
+  const long long stride = (long long)gridDim.x * blockDim.x * kTravItems;
+  const long long wbase =
+      ((long long)blockIdx.x * blockDim.x + threadIdx.x - lane) * kTravItems;
   for (long long w = wbase; w < nfront; w += stride) {  // warp-uniform trip count
-    const long long t = w + lane;
-    int ty = -1, k = 0;
-    int2 p = make_int2(0, 0);
-    if (t < nfront) {
-      p = front[t];
-      if ((unsigned)p.x < (unsigned)ncells && (unsigned)p.y < (unsigned)ncells)
-        ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
-      else
-        atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
+    const long long t0 = w + (long long)lane * kTravItems;
+    int ty[kTravItems], k[kTravItems];
+    int2 p[kTravItems];
+    unsigned v = 0;  // packed: M2L in bits 0-7, P2P in 8-15, children in 16-31
+#pragma unroll
+    for (int u = 0; u < kTravItems; u++) {
+      ty[u] = -1;
+      k[u] = 0;
+      p[u] = t0 + u < nfront ? front[t0 + u] : make_int2(0, 0);
     }
-    // packed counts: M2L in bits 0-7, P2P in 8-15, children in 16-31 (warp totals fit)
-    const unsigned v = (ty == PAIR_M2L ? 1u : 0u) | (ty == PAIR_P2P ? 1u << 8 : 0u) |
-                       (ty >= PAIR_SPLIT_I ? (unsigned)k << 16 : 0u);
+#pragma unroll
+    for (int u = 0; u < kTravItems; u++) {
+      if (t0 + u < nfront) {
+        if ((unsigned)p[u].x < (unsigned)ncells && (unsigned)p[u].y < (unsigned)ncells)
+          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, &k[u]);
+        else
+          atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
+      }
+      v += (ty[u] == PAIR_M2L ? 1u : 0u) | (ty[u] == PAIR_P2P ? 1u << 8 : 0u) |
+           (ty[u] >= PAIR_SPLIT_I ? (unsigned)k[u] << 16 : 0u);
+    }
     unsigned incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += u;
+      const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
     }
     const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
     unsigned long long bm = 0, bp = 0, bn = 0;
@@ -181,30 +193,34 @@ __global__ void __launch_bounds__(256)
       if ((tot >> 8) & 0xffu) bp = atomicAdd(&ctr[1], (unsigned long long)((tot >> 8) & 0xffu));
       if (tot >> 16) bn = atomicAdd(next_count, (unsigned long long)(tot >> 16));
     }
-    bm = __shfl_sync(0xffffffffu, bm, 31);
-    bp = __shfl_sync(0xffffffffu, bp, 31);
-    bn = __shfl_sync(0xffffffffu, bn, 31);
-    const unsigned ex = incl - v;
-    const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
-    if (ty == PAIR_M2L) {
-      const unsigned long long o = bm + (ex & 0xffu);
-      if (o < m2l_cap) m2l[o] = packed;
-    } else if (ty == PAIR_P2P) {
-      const unsigned long long o = bp + ((ex >> 8) & 0xffu);
-      if (o < p2p_cap) p2p[o] = packed;
-    } else if (ty >= PAIR_SPLIT_I) {
-      // every slot below the capacity is written (the next step reads up to it)
-      const unsigned long long o = bn + (ex >> 16);
-      const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k, next_cap - o);
-      if (ty == PAIR_SPLIT_I) {
-        const int c0 = ichild[p.x];
-        for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p.y);
-      } else if (ty == PAIR_SPLIT_J) {
-        const int c0 = ichild[p.y];
-        for (int j = 0; j < kw; j++) next[o + j] = make_int2(p.x, c0 + j);
-      } else {
-        const int ci0 = ichild[p.x], cj0 = ichild[p.y], nj = nchild[p.y];
-        for (int i = 0; i < kw; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+    bm = __shfl_sync(0xffffffffu, bm, 31) + ((incl - v) & 0xffu);
+    bp = __shfl_sync(0xffffffffu, bp, 31) + (((incl - v) >> 8) & 0xffu);
+    bn = __shfl_sync(0xffffffffu, bn, 31) + ((incl - v) >> 16);
+#pragma unroll
+    for (int u = 0; u < kTravItems; u++) {
+      const unsigned long long packed =
+          ((unsigned long long)(unsigned)p[u].x << 32) | (unsigned)p[u].y;
+      if (ty[u] == PAIR_M2L) {
+        if (bm < m2l_cap) m2l[bm] = packed;
+        bm++;
+      } else if (ty[u] == PAIR_P2P) {
+        if (bp < p2p_cap) p2p[bp] = packed;
+        bp++;
+      } else if (ty[u] >= PAIR_SPLIT_I) {
+        // every slot below the capacity is written (the next step reads up to it)
+        const unsigned long long o = bn;
+        const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k[u], next_cap - o);
+        if (ty[u] == PAIR_SPLIT_I) {
+          const int c0 = ichild[p[u].x];
+          for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p[u].y);
+        } else if (ty[u] == PAIR_SPLIT_J) {
+          const int c0 = ichild[p[u].y];
+          for (int j = 0; j < kw; j++) next[o + j] = make_int2(p[u].x, c0 + j);
+        } else {
+          const int ci0 = ichild[p[u].x], cj0 = ichild[p[u].y], nj = nchild[p[u].y];
+          for (int i = 0; i < kw; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+        }
+        bn += k[u];
       }
     }
   }
@@ -288,8 +304,9 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
   upload_roots(s);
   long long nfront = s.nroots, maxfront = s.nroots;
   nm2l = np2p = 0;
-  s.m2l.ensure(1024);
-  s.p2p.ensure(1024);
+  // first sizes from typical list lengths per cell; grown below when they fall short
+  s.m2l.ensure(std::max(1024LL, 64LL * s.ncells));
+  s.p2p.ensure(std::max(1024LL, 16LL * s.ncells));
   while (nfront > 0) {
     FMM_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s.stream));
     int grid = std::min(ceil_div(nfront, TB), 148 * 16);

@@ -122,6 +122,34 @@ __global__ void k_keys(const vec4<T>* __restrict__ b, int n, const T* __restrict
   idx[i] = i;
 }
 
+// forest sort helpers: root of each key-sorted body (binary search of its input index in
+// the roots' first bodies), then a gather through the root-sorted permutation
+__global__ void k_root_of(int n, const int* __restrict__ body, const int* __restrict__ root_first,
+                          int nroots, unsigned* __restrict__ root, int* __restrict__ pos) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = body[i];
+  int lo = 0, hi = nroots - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (root_first[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  root[i] = (unsigned)lo;
+  pos[i] = i;
+}
+
+__global__ void k_gather_kv(int n, const int* __restrict__ perm,
+                            const unsigned long long* __restrict__ kin,
+                            const int* __restrict__ vin, unsigned long long* __restrict__ kout,
+                            int* __restrict__ vout) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = perm[i];
+  kout[i] = kin[j];
+  vout[i] = vin[j];
+}
+
 __device__ __forceinline__ int digit_at(unsigned long long key, int level) {
   return (int)((key >> (3 * (kMaxLevel - 1 - level))) & 7ULL);
 }
@@ -413,6 +441,36 @@ template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
   b.cap = 0;
 }
 
+// Sort (key, body) pairs by (root, key), stable: one radix sort on the key over all roots,
+// then a stable radix sort on the root id (least significant digit first), so the result is
+// each root's range sorted on its own, as when the root is solved alone.  (CUB's segmented
+// sort gives each segment one thread block, which is slow for a few large segments.)
+template <typename T>
+static void forest_sort(Solver<T>& s, const unsigned long long* kin, unsigned long long* kout,
+                        const int* vin, int* vout, int n, int nroots, int end_bit) {
+  if (nroots == 1) {
+    sort_pairs_u64(s, kin, kout, vin, vout, n, end_bit);
+    return;
+  }
+  const int TB = 256;
+  s.fs_keys.ensure(n);
+  s.fs_idx.ensure(n);
+  s.fs_root.ensure(n);
+  s.fs_root2.ensure(n);
+  s.fs_pos.ensure(n);
+  s.fs_pos2.ensure(n);
+  sort_pairs_u64(s, kin, s.fs_keys.p, vin, s.fs_idx.p, n, end_bit);
+  k_root_of<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.fs_idx.p, s.d_root_first.p, nroots,
+                                                  s.fs_root.p, s.fs_pos.p);
+  FMM_LAUNCH_CHECK();
+  int bits = 1;
+  while ((1LL << bits) < (long long)nroots) bits++;
+  sort_pairs_u32(s, s.fs_root.p, s.fs_root2.p, s.fs_pos.p, s.fs_pos2.p, n, bits);
+  k_gather_kv<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.fs_pos2.p, s.fs_keys.p, s.fs_idx.p,
+                                                    kout, vout);
+  FMM_LAUNCH_CHECK();
+}
+
 template <typename T> void build_tree(Solver<T>& s) {
   const int n = s.n;
   const int TB = 256;
@@ -473,11 +531,7 @@ template <typename T> void build_tree(Solver<T>& s) {
   k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, s.d_root_first.p,
                                                   nroots, s.keys.p, s.idx.p);
   FMM_LAUNCH_CHECK();
-  if (nroots == 1)
-    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, 3 * kMaxLevel);
-  else
-    segmented_sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots,
-                             s.d_root_first.p, s.d_root_first.p + 1, 3 * kMaxLevel);
+  forest_sort(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots, 3 * kMaxLevel);
   // nodes, level by level
   size_t cap0 = (size_t)std::max(1024, 4 * (n / std::max(1, s.cfg.ncrit)) + 64 + nroots);
   DevArr<int>* narr[] = {&s.nbegin, &s.ncount, &s.nparent, &s.nchildn, &s.nfirst,
@@ -572,11 +626,7 @@ template <typename T> void build_tree(Solver<T>& s) {
     // s.order holds 0..n-1 (input positions); sort them by truncated key within each root
     FMM_CUDA(cudaMemcpyAsync(s.idx.p, s.order.p, n * sizeof(int), cudaMemcpyDeviceToDevice,
                              s.stream));
-    if (nroots == 1)
-      sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, 3 * kMaxLevel);
-    else
-      segmented_sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, nroots,
-                               s.d_root_first.p, s.d_root_first.p + 1, 3 * kMaxLevel);
+    forest_sort(s, s.keys.p, s.keys2.p, s.idx.p, s.order.p, n, nroots, 3 * kMaxLevel);
   }
   s.bodies.ensure(n);
   k_permute<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.bodies_in.p, s.order.p, s.bodies.p);

@@ -167,6 +167,10 @@ int fmm_b200_server_wait(fmm_b200_server* srv, long long request_id, double* p, 
                          double* latency_s, double* queue_s);
 int fmm_b200_server_stats(fmm_b200_server* srv, long long* completed, long long* bodies,
                           long long* batches, int* pending);
+/* Worker seconds summed over all batches so far: copying requests into the pinned staging
+ * buffer, inside the batched solve (host<->device copies included), copying results out. */
+int fmm_b200_server_profile(fmm_b200_server* srv, double* stage_s, double* solve_s,
+                            double* unstage_s);
 int fmm_b200_server_destroy(fmm_b200_server* srv);
 
 /* ---- utilities ----------------------------------------------------------------------- */

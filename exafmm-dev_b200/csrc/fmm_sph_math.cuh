@@ -127,6 +127,30 @@ __host__ __device__ __forceinline__ void local(const Angles<T>& a, T* yr, T* yi)
 // unnormalised multipoles), for the output degrees j in [J0, J1) only (the FP32 kernel
 // splits the outputs into passes).  Mj holds NT (re, im) pairs.  The loop bounds are
 // compile-time after unrolling, so the whole contraction resolves to register operands.
+// (re, im) of one coefficient; on the device one 8-byte (float) or 16-byte (double) load,
+// for a row that starts on a multiple of 2 reals (every expansion row does: its length is
+// even)
+__host__ __device__ __forceinline__ void load_pair(const float* p, float& a, float& b) {
+#ifdef __CUDA_ARCH__
+  const float2 v = *reinterpret_cast<const float2*>(p);
+  a = v.x;
+  b = v.y;
+#else
+  a = p[0];
+  b = p[1];
+#endif
+}
+__host__ __device__ __forceinline__ void load_pair(const double* p, double& a, double& b) {
+#ifdef __CUDA_ARCH__
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  a = v.x;
+  b = v.y;
+#else
+  a = p[0];
+  b = p[1];
+#endif
+}
+
 template <typename T, int P, int J0 = 0, int J1 = P>
 __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, const T* Mj, T* Lr,
                                                   T* Li) {
@@ -134,7 +158,8 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, cons
   for (int n = 0; n < P - J0; n++) {
 #pragma unroll
     for (int mu = 0; mu <= n; mu++) {
-      const T mr = Mj[2 * sidx(n, mu)], mi = Mj[2 * sidx(n, mu) + 1];
+      T mr, mi;
+      load_pair(Mj + 2 * sidx(n, mu), mr, mi);
 #pragma unroll
       for (int j = J0; j < J1; j++) {
         if (j + n >= P) break;

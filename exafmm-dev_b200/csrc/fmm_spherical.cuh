@@ -314,19 +314,26 @@ __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
   return j;
 }
 
+// warps per block of one FP32 M2L pass: as many as the pass's registers allow in one block
+// per SM without spilling (P = 10: about 130, 128 and 154 registers for the passes starting
+// at degrees 0, 3 and 6)
+__host__ __device__ constexpr int m2l_pass_warps(int P, int J0) {
+  return P == 10 ? (J0 == 0 ? 14 : (J0 == 3 ? 15 : 12)) : kM2LWarps;
+}
+
 // Warps of a block run in lockstep (a block barrier per batch of 32 sources) so that they
 // execute the same unrolled instructions together and share the fetched instruction lines;
 // targets arrive ordered by their number of batches, so the warps of a block have about
 // the same amount of work.
-template <typename T, int P, int J0, int J1>
-__global__ void __launch_bounds__(32 * kM2LWarps)
+template <typename T, int P, int J0, int J1, int W>
+__global__ void __launch_bounds__(32 * W)
     k_m2l_reg(int ntgt, const int* __restrict__ tgt, const int* __restrict__ off,
               const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
               const T* __restrict__ M, T* __restrict__ L, int ncoef) {
   constexpr int NT = sph::NT(P);
   __shared__ int smax;
   const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int w = blockIdx.x * kM2LWarps + wl;
+  const int w = blockIdx.x * W + wl;
   const int c = w < ntgt ? tgt[w] : 0;
   const int s0 = w < ntgt ? off[c] : 0, s1 = w < ntgt ? off[c + 1] : 0;
   const int nbat = (s1 - s0 + 31) >> 5;
@@ -367,7 +374,8 @@ template <typename T, int P, int J0>
 static void launch_m2l_passes(Solver<T>& s) {
   if constexpr (J0 < P) {
     constexpr int J1 = m2l_pass_end(P, J0);
-    k_m2l_reg<T, P, J0, J1><<<ceil_div(s.m2l_ntgt, kM2LWarps), 32 * kM2LWarps, 0, s.stream>>>(
+    constexpr int W = m2l_pass_warps(P, J0);
+    k_m2l_reg<T, P, J0, J1, W><<<ceil_div(s.m2l_ntgt, W), 32 * W, 0, s.stream>>>(
         s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
     FMM_LAUNCH_CHECK();
     launch_m2l_passes<T, P, J1>(s);

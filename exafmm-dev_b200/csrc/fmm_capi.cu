@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -203,6 +204,7 @@ int fmm_b200_default_config(fmm_b200_config* c) {
   c->eps2 = 0.0;
   c->images = 0;
   c->device = 0;
+  c->cycle = 2 * M_PI;
   return FMM_OK;
 }
 
@@ -219,13 +221,17 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
     return FMM_ERR_INVALID;
   }
   *out = nullptr;
-  if (cfg->images != 0) {
-    g_create_error = "periodic images are not supported";
-    return FMM_ERR_NOT_SUPPORTED;
-  }
   if (cfg->basis != FMM_SPHERICAL && cfg->basis != FMM_CARTESIAN) {
     g_create_error = "unknown basis";
     return FMM_ERR_INVALID;
+  }
+  if (cfg->images < 0 || (cfg->images > 0 && !(cfg->cycle > 0.0))) {
+    g_create_error = "images must be >= 0 and cycle > 0 when images > 0";
+    return FMM_ERR_INVALID;
+  }
+  if (cfg->images > 0 && cfg->basis != FMM_SPHERICAL) {
+    g_create_error = "periodic images are supported on the spherical basis only";
+    return FMM_ERR_NOT_SUPPORTED;
   }
   std::vector<int> ords = cfg->basis == FMM_CARTESIAN ? cartesian_orders() : spherical_orders();
   if (std::find(ords.begin(), ords.end(), cfg->P) == ords.end()) {
@@ -311,6 +317,15 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     delete h->base;
   }
   delete h;
+  return FMM_OK;
+}
+
+int fmm_b200_set_periodic(fmm_b200_solver* h, int images, double cycle) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  if (images < 0 || (images > 0 && !(cycle > 0.0))) return FMM_ERR_INVALID;
+  if (images > 0 && h->base->cfg.basis != FMM_SPHERICAL) return FMM_ERR_NOT_SUPPORTED;
+  h->base->cfg.images = images;
+  h->base->cfg.cycle = cycle;
   return FMM_OK;
 }
 

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int t = 0; t < NT; t++) acc[t] = 0;
   for (int s = s0 + lane; s < s1; s += 32) {
-    const int j = (int)(pairs[s] & 0xffffffffULL);
+    const int j = pair_cell((unsigned)pairs[s]);  // no periodic images on this basis
     const vec4<T> Xj = cX[j];
     const T dx = Xi.x - Xj.x, dy = Xi.y - Xj.y, dz = Xi.z - Xj.z;
     const T invR2 = T(1) / (dx * dx + dy * dy + dz * dz);
@@ -267,6 +267,7 @@ template <typename T, int P> static void l2p_(Solver<T>& s) {
 
 // fill the dispatch table for one (precision, order); one object file per instantiation
 template <typename T, int P> void cart_fill(ExpansionOps<T>* ops) {
+  ops->periodic = nullptr;  // periodic images are spherical-basis only
   ops->p2m = &p2m_<T, P>;
   ops->m2m_level = &m2m_<T, P>;
   ops->m2l = &m2l_<T, P>;

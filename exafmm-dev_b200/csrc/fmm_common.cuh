@@ -51,6 +51,25 @@ __device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ float rsqrt_(float a) { return rsqrtf(a); }
 __device__ __forceinline__ double rsqrt_(double a) { return rsqrt(a); }
 
+// Source field of a packed list pair (target << 32 | source): the source cell in bits 0-26
+// and the periodic image of the source tree in bits 27-31, coded 9 d(ix) + 3 d(iy) + d(iz)
+// for a shift of (ix, iy, iz) periods with d(0) = 0, d(1) = 1, d(-1) = 2 (0: no shift).
+constexpr int kImgShift = 27;
+constexpr unsigned kCellMask = (1u << kImgShift) - 1;
+__host__ __device__ __forceinline__ int pair_cell(unsigned src) { return (int)(src & kCellMask); }
+__host__ __device__ __forceinline__ int pair_img(unsigned src) { return (int)(src >> kImgShift); }
+__host__ __device__ __forceinline__ int img_code(int ix, int iy, int iz) {
+  return 9 * (ix < 0 ? 2 : ix) + 3 * (iy < 0 ? 2 : iy) + (iz < 0 ? 2 : iz);
+}
+// shift of image code c: (ix, iy, iz) times the period (exact: |i| <= 1)
+template <typename T>
+__host__ __device__ __forceinline__ void img_shift(int c, T cycle, T& sx, T& sy, T& sz) {
+  const int dx = c / 9, dy = (c / 3) % 3, dz = c % 3;
+  sx = (T)(dx == 2 ? -1 : dx) * cycle;
+  sy = (T)(dy == 2 ? -1 : dy) * cycle;
+  sz = (T)(dz == 2 ? -1 : dz) * cycle;
+}
+
 // |d|^2 as ((dx*dx + dy*dy) + dz*dz) with every step rounded (vec.h norm, no fusion)
 template <typename T> __device__ __forceinline__ T norm_rn(T dx, T dy, T dz) {
   return add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));

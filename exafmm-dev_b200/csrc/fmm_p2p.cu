@@ -30,10 +30,17 @@ __device__ __forceinline__ double rsqrt_ftz(double a) { return rsqrt(a); }
 
 // one pair; EXACT: skip r^2 == 0 and take subnormal r^2 as it is (the reference's
 // arithmetic); otherwise an r^2 of zero or below the normal range makes `pot` non-finite
-template <typename T, bool EXACT = true>
+// SHIFT: the source is a periodic image shifted by (px, py, pz); the offset is formed as
+// (xj - xi) + p, the negation of the reference's (xi - xj) - Xperiodic
+template <typename T, bool EXACT = true, bool SHIFT = false>
 __device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, T eps2, T& pot,
-                                          T& ax, T& ay, T& az) {
-  const T dx = sj.x - xi.x, dy = sj.y - xi.y, dz = sj.z - xi.z;
+                                          T& ax, T& ay, T& az, T px = 0, T py = 0, T pz = 0) {
+  T dx = sj.x - xi.x, dy = sj.y - xi.y, dz = sj.z - xi.z;
+  if (SHIFT) {
+    dx += px;
+    dy += py;
+    dz += pz;
+  }
   const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
   const T inv = EXACT ? (r2 > T(0) ? rsqrt_(r2) : T(0)) : rsqrt_ftz(r2);
   const T qinv = sj.w * inv;
@@ -46,11 +53,11 @@ __device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, 
 
 // all bodies of one source leaf (first body j0, nj bodies) on the lane's TPL targets, its
 // sums started from zero; sources are staged through the warp's shared row 32 at a time
-template <typename T, int TPL, bool EXACT>
+template <typename T, int TPL, bool EXACT, bool SHIFT = false>
 __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32], int sub, int G,
                                             int j0, int nj, const vec4<T>* __restrict__ bodies,
                                             T eps2, const vec4<T>* xi, T* pot, T* ax, T* ay,
-                                            T* az) {
+                                            T* az, T px = 0, T py = 0, T pz = 0) {
 #pragma unroll
   for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
   for (int jb = 0; jb < nj; jb += 32) {
@@ -63,7 +70,7 @@ __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32],
       const vec4<T> sj = sh[wl][k];
 #pragma unroll
       for (int u = 0; u < TPL; u++)
-        p2p_accum<T, EXACT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u]);
+        p2p_accum<T, EXACT, SHIFT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u], px, py, pz);
     }
   }
 }
@@ -76,7 +83,7 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
                                          const unsigned long long* __restrict__ pairs,
                                          const int* __restrict__ ibody,
                                          const int* __restrict__ nbody,
-                                         const vec4<T>* __restrict__ bodies, T eps2,
+                                         const vec4<T>* __restrict__ bodies, T eps2, T cycle,
                                          vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
   const int tpp = 32 / G;
   const int sub = lane % G;
@@ -92,15 +99,17 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
 #pragma unroll
     for (int d = 0; d < 4; d++) acc[u][d] = Comp<T>{0, 0};
   }
-  // source leaf s: (first body, count), the next one prefetched
-  int cj = s0 < s1 ? (int)(pairs[s0] & 0xffffffffULL) : 0;
-  int j0 = s0 < s1 ? ibody[cj] : 0, nj = s0 < s1 ? nbody[cj] : 0;
+  // source leaf s: (first body, count, periodic image), the next one prefetched
+  const unsigned src0 = s0 < s1 ? (unsigned)pairs[s0] : 0u;
+  int j0 = s0 < s1 ? ibody[pair_cell(src0)] : 0, nj = s0 < s1 ? nbody[pair_cell(src0)] : 0;
+  int img = pair_img(src0);
   for (int s = s0; s < s1; s++) {
-    int j0n = 0, njn = 0;
+    int j0n = 0, njn = 0, imgn = 0;
     if (s + 1 < s1) {
-      const int cn = (int)(pairs[s + 1] & 0xffffffffULL);
-      j0n = ibody[cn];
-      njn = nbody[cn];
+      const unsigned srcn = (unsigned)pairs[s + 1];
+      j0n = ibody[pair_cell(srcn)];
+      njn = nbody[pair_cell(srcn)];
+      imgn = pair_img(srcn);
     }
     T pot[TPL], ax[TPL], ay[TPL], az[TPL];
     // Bodies at one position share every octant and so one leaf: only the target leaf
@@ -108,8 +117,20 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
     // if a pair underflowed to r^2 == 0 or below the normal range there, its sum is not
     // finite and the leaf is summed again in the exact form, so results are always those
     // of the exact form.
-    const bool self = j0 == b0;
-    if (!self) {
+    if (img != 0) {
+      // a periodic image of a source leaf (r^2 == 0 would take bodies exactly one period
+      // apart): fast form, exact re-sum if not finite
+      T px, py, pz;
+      img_shift<T>(img, cycle, px, py, pz);
+      source_leaf<T, TPL, false, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax,
+                                       ay, az, px, py, pz);
+      bool bad = false;
+#pragma unroll
+      for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(pot[u]);
+      if (__any_sync(0xffffffffu, bad))
+        source_leaf<T, TPL, true, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax,
+                                        ay, az, px, py, pz);
+    } else if (j0 != b0) {
       source_leaf<T, TPL, false>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
       bool bad = false;
 #pragma unroll
@@ -135,6 +156,7 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
     }
     j0 = j0n;
     nj = njn;
+    img = imgn;
   }
   for (int o = 1; o < G; o <<= 1) {
 #pragma unroll
@@ -162,7 +184,7 @@ template <typename T, bool COMP>
 __global__ void __launch_bounds__(32 * kP2PWarps)
     k_p2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ off,
           const unsigned long long* __restrict__ pairs, const int* __restrict__ ibody,
-          const int* __restrict__ nbody, const vec4<T>* __restrict__ bodies, T eps2,
+          const int* __restrict__ nbody, const vec4<T>* __restrict__ bodies, T eps2, T cycle,
           vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
   __shared__ vec4<T> sh[kP2PWarps][32];
   const int wl = threadIdx.x >> 5;
@@ -175,11 +197,11 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
   const int s0 = off[c], s1 = off[c + 1];
   if (nb <= 32) {
     p2p_leaf<T, COMP, 1>(lane, wl, sh, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
-                         trg_s, trg_e);
+                         cycle, trg_s, trg_e);
   } else {
     for (int base = 0; base < nb; base += 64)
       p2p_leaf<T, COMP, 2>(lane, wl, sh, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
-                           eps2, trg_s, trg_e);
+                           eps2, cycle, trg_s, trg_e);
   }
 }
 
@@ -188,7 +210,7 @@ template <typename T> void run_p2p(Solver<T>& s) {
   constexpr bool comp = sizeof(T) == 4;
   k_p2p<T, comp><<<ceil_div(s.nleaves, kP2PWarps), 32 * kP2PWarps, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.p2p_off.p, s.p2p.p, s.c_ibody.p, s.c_nbody.p, s.bodies.p,
-      (T)s.cfg.eps2, s.trg_s.p, s.trg_e.p);
+      (T)s.cfg.eps2, (T)s.cfg.cycle, s.trg_s.p, s.trg_e.p);
   FMM_LAUNCH_CHECK();
 }
 

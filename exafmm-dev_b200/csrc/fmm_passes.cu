@@ -71,9 +71,13 @@ template <typename T> void upward_pass(Solver<T>& s) {
 }
 
 template <typename T> void run_m2l(Solver<T>& s) {
-  if (s.ncells == 0 || s.nm2l == 0) return;
+  if (s.ncells == 0) return;
   ExpansionOps<T> ops = ops_of(s);
-  ops.m2l(s);
+  if (s.nm2l > 0) ops.m2l(s);
+  if (s.cfg.images > 1) {
+    if (!ops.periodic) throw FmmError(FMM_ERR_NOT_SUPPORTED, "periodic images on this basis");
+    ops.periodic(s);
+  }
 }
 
 template <typename T> void downward_pass(Solver<T>& s) {

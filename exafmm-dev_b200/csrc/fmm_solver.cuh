@@ -86,6 +86,7 @@ struct SolverBase {
   DevArr<int> fs_idx;
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
+  int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
   DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches
@@ -102,6 +103,8 @@ template <typename T> struct Solver : SolverBase {
   DevArr<vec4<T>> bodies_in, bodies, trg_s, trg_e, trg_out, cX;
   DevArr<T> box;  // per root, 16 values: X0[3], R0, Xmin[3], Xmax[3]
   DevArr<T> M, L, nX;
+  DevArr<T> pM, pM2, pC;  // periodic cell multipoles and per-shift M2L terms
+  DevArr<int> c_root_cells;
   DevArr<T> minmax_part;
 };
 
@@ -121,6 +124,7 @@ template <typename T> struct ExpansionOps {
   void (*m2l)(Solver<T>& s);
   void (*l2l_level)(Solver<T>& s, int lo, int hi);
   void (*l2p)(Solver<T>& s);
+  void (*periodic)(Solver<T>& s);  // far field of the periodic images, or null
 };
 template <typename T> bool spherical_ops(int P, ExpansionOps<T>* ops);
 template <typename T> bool cartesian_ops(int P, ExpansionOps<T>* ops);

@@ -329,7 +329,7 @@ template <typename T, int P, int J0, int J1, int W>
 __global__ void __launch_bounds__(32 * W)
     k_m2l_reg(int ntgt, const int* __restrict__ tgt, const int* __restrict__ off,
               const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
-              const T* __restrict__ M, T* __restrict__ L, int ncoef) {
+              const T* __restrict__ M, T* __restrict__ L, int ncoef, T cycle) {
   constexpr int NT = sph::NT(P);
   __shared__ int smax;
   const int wl = threadIdx.x >> 5, lane = lane_id();
@@ -349,10 +349,13 @@ __global__ void __launch_bounds__(32 * W)
   for (int bt = 0; bt < maxbat; bt++) {
     const int s = s0 + bt * 32 + lane;
     if (s < s1) {
-      const int j = (int)(pairs[s] & 0xffffffffULL);
+      const unsigned src = (unsigned)pairs[s];
+      const int j = pair_cell(src);
+      T px, py, pz;  // periodic shift of the source (0 without images)
+      img_shift<T>(pair_img(src), cycle, px, py, pz);
       const vec4<T> Xj = cX[j];
       T yr[NT], yi[NT];
-      sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
+      sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
       sph::local<T, P>(a, yr, yi);
       sph::m2l_pair<T, P, J0, J1>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
     }
@@ -376,7 +379,8 @@ static void launch_m2l_passes(Solver<T>& s) {
     constexpr int J1 = m2l_pass_end(P, J0);
     constexpr int W = m2l_pass_warps(P, J0);
     k_m2l_reg<T, P, J0, J1, W><<<ceil_div(s.m2l_ntgt, W), 32 * W, 0, s.stream>>>(
-        s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+        s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef,
+        (T)s.cfg.cycle);
     FMM_LAUNCH_CHECK();
     launch_m2l_passes<T, P, J1>(s);
   }
@@ -431,7 +435,7 @@ template <typename T, int P>
 __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     k_m2l_lanes(int ncells, const int* __restrict__ off,
                 const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
-                const T* __restrict__ M, T* __restrict__ L, int ncoef) {
+                const T* __restrict__ M, T* __restrict__ L, int ncoef, T cycle) {
   constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
   constexpr int W = SphCfg<T>::W;
   __shared__ T sy[W][NC], sm[W][NC];
@@ -451,11 +455,14 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     jk_of(ot[i] < NT ? ot[i] : 0, oj[i], ok[i]);
   }
   for (int s = s0; s < s1; s++) {
-    const int j = (int)(pairs[s] & 0xffffffffULL);
+    const unsigned src = (unsigned)pairs[s];
+    const int j = pair_cell(src);
+    T px, py, pz;  // periodic shift of the source (0 without images)
+    img_shift<T>(pair_img(src), cycle, px, py, pz);
     const vec4<T> Xj = cX[j];
     {
       T yr[NT], yi[NT];
-      sph::Angles<T> a = sph::angles(Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z);
+      sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
       sph::local<T, P>(a, yr, yi);
       __syncwarp();
       spread_y<T, NT>(yr, yi, sy[wl], lane);
@@ -579,7 +586,7 @@ template <typename T, int P> static void m2l_(Solver<T>& s) {
   } else {
     constexpr int W = SphCfg<T>::W;
     k_m2l_lanes<T, P><<<ceil_div(s.ncells, W), 32 * W, 0, s.stream>>>(
-        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef);
+        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef, (T)s.cfg.cycle);
     FMM_LAUNCH_CHECK();
   }
 }
@@ -606,7 +613,157 @@ template <typename T, int P> static void l2p_(Solver<T>& s) {
 
 
 // fill the dispatch table for one (precision, order); one object file per instantiation
+// ---------------------------------------------------------------- periodic far field
+// Traversal::traversePeriodic (include/traversal.h:127-185), one root per solve of the
+// batch.  Per sub-level of images: the periodic cell (the root's multipole, at the root's
+// centre) sends M2L into the root from the 26 x 27 shifts (3 ix + cx, ...) cycle, |i|,
+// |c| <= 1, (ix, iy, iz) != 0 (k_per_m2l: one warp per shift, lanes over outputs; then
+// k_per_reduce adds the 702 terms to the root's local expansion in the reference's loop
+// order); then the periodic cell becomes the M2M of its 26 copies shifted by
+// (ix, iy, iz) cycle, (ix, iy, iz) != 0 (k_per_m2m; as in the reference, the unshifted copy
+// is not among them), and the period grows three times.
+constexpr int kPerShifts = 26 * 27;
+
+__device__ __forceinline__ void per_outer(int o, int& ix, int& iy, int& iz) {
+  const int q = o < 13 ? o : o + 1;  // the 26 of {-1,0,1}^3 other than (0,0,0), loop order
+  ix = q / 9 - 1;
+  iy = (q / 3) % 3 - 1;
+  iz = q % 3 - 1;
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(32)
+    k_per_m2l(const T* __restrict__ Mp, T cycle, int ncoef, T* __restrict__ contrib) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
+  __shared__ T sy[NC], sm[NC];
+  const int lane = lane_id();
+  const int sidx = blockIdx.x, r = blockIdx.y;
+  int ix, iy, iz;
+  per_outer(sidx / 27, ix, iy, iz);
+  const int c = sidx % 27, cx = c / 9 - 1, cy = (c / 3) % 3 - 1, cz = c % 3 - 1;
+  // dX = Ci0->X - Ci->X - Xperiodic with Ci at the root's own centre: -Xperiodic
+  const T px = (T)(ix * 3 + cx) * cycle, py = (T)(iy * 3 + cy) * cycle,
+          pz = (T)(iz * 3 + cz) * cycle;
+  {
+    T yr[NT], yi[NT];
+    sph::Angles<T> a = sph::angles(T(0) - px, T(0) - py, T(0) - pz);
+    sph::local<T, P>(a, yr, yi);
+    spread_y<T, NT>(yr, yi, sy, lane);
+    for (int t = lane; t < NC; t += 32) sm[t] = Mp[(size_t)r * ncoef + t];
+  }
+  __syncwarp();
+  T* out = contrib + ((size_t)r * kPerShifts + sidx) * NC;
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    const int t = lane + 32 * i;
+    if (t < NT) {
+      int j, kk;
+      jk_of(t, j, kk);
+      T re, im;
+      m2l_term<T>(P, j, kk, sy, sm, re, im);
+      out[2 * t] = re;
+      out[2 * t + 1] = im;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_per_reduce(int nroots, int nc, const int* __restrict__ root_cell,
+                             const T* __restrict__ contrib, T* __restrict__ L, int ncoef) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nroots * nc) return;
+  const int r = t / nc, e = t % nc;
+  T acc = L[(size_t)root_cell[r] * ncoef + e];
+  for (int q = 0; q < kPerShifts; q++) acc += contrib[((size_t)r * kPerShifts + q) * nc + e];
+  L[(size_t)root_cell[r] * ncoef + e] = acc;
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(32)
+    k_per_m2m(const T* __restrict__ Mp, const int* __restrict__ root_cell,
+              const vec4<T>* __restrict__ cX, T cycle, int ncoef, T* __restrict__ Mout) {
+  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
+  __shared__ T sy[NC], sm[NC];
+  const int lane = lane_id(), r = blockIdx.x;
+  const vec4<T> X = cX[root_cell[r]];
+  for (int t = lane; t < NC; t += 32) sm[t] = Mp[(size_t)r * ncoef + t];
+  T ar[KO], ai[KO];
+#pragma unroll
+  for (int i = 0; i < KO; i++) ar[i] = ai[i] = 0;
+  for (int o = 0; o < 26; o++) {
+    int ix, iy, iz;
+    per_outer(o, ix, iy, iz);
+    // child centre X + (ix, iy, iz) cycle, then dX = Xparent - Xchild as the reference rounds
+    const T xc = X.x + (T)ix * cycle, yc = X.y + (T)iy * cycle, zc = X.z + (T)iz * cycle;
+    __syncwarp();
+    {
+      T yr[NT], yi[NT];
+      sph::Angles<T> a = sph::angles(X.x - xc, X.y - yc, X.z - zc);
+      sph::multipole<T, P>(a, a.r, yr, yi);
+      spread_y<T, NT>(yr, yi, sy, lane);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KO; i++) {
+      const int t = lane + 32 * i;
+      if (t < NT) {
+        int j, kk;
+        jk_of(t, j, kk);
+        T re, im;
+        sph::m2m_term<T>(j, kk, sy, sy + NT, sm, re, im);
+        ar[i] += re;
+        ai[i] += im;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    const int t = lane + 32 * i;
+    if (t < NT) {
+      Mout[(size_t)r * ncoef + 2 * t] = ar[i];
+      Mout[(size_t)r * ncoef + 2 * t + 1] = ai[i];
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_per_init(int nroots, const int* __restrict__ root_cell, const T* __restrict__ M,
+                           int ncoef, T* __restrict__ Mp) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nroots * ncoef) return;
+  const int r = t / ncoef, e = t % ncoef;
+  Mp[t] = M[(size_t)root_cell[r] * ncoef + e];
+}
+
+template <typename T, int P> static void periodic_(Solver<T>& s) {
+  const int R = s.nroots, nc = 2 * sph::NT(P);
+  if (s.cfg.images < 2 || R == 0) return;
+  s.pM.ensure((size_t)R * s.ncoef);
+  s.pM2.ensure((size_t)R * s.ncoef);
+  s.pC.ensure((size_t)R * kPerShifts * nc);
+  s.c_root_cells.ensure(R);
+  FMM_CUDA(cudaMemcpyAsync(s.c_root_cells.p, s.root_cell.data(), sizeof(int) * R,
+                           cudaMemcpyHostToDevice, s.stream));
+  k_per_init<T><<<ceil_div((long long)R * s.ncoef, 256), 256, 0, s.stream>>>(
+      R, s.c_root_cells.p, s.M.p, s.ncoef, s.pM.p);
+  FMM_LAUNCH_CHECK();
+  T cycle = (T)s.cfg.cycle;
+  for (int level = 0; level < s.cfg.images - 1; level++) {
+    k_per_m2l<T, P><<<dim3(kPerShifts, R), 32, 0, s.stream>>>(s.pM.p, cycle, s.ncoef, s.pC.p);
+    FMM_LAUNCH_CHECK();
+    k_per_reduce<T><<<ceil_div((long long)R * nc, 128), 128, 0, s.stream>>>(
+        R, nc, s.c_root_cells.p, s.pC.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+    k_per_m2m<T, P><<<R, 32, 0, s.stream>>>(s.pM.p, s.c_root_cells.p, s.cX.p, cycle, s.ncoef,
+                                            s.pM2.p);
+    FMM_LAUNCH_CHECK();
+    std::swap(s.pM, s.pM2);
+    cycle = cycle * (T)3;
+  }
+}
+
 template <typename T, int P> void sph_fill(ExpansionOps<T>* ops) {
+  ops->periodic = &periodic_<T, P>;
   ops->p2m = &p2m_<T, P>;
   ops->m2m_level = &m2m_<T, P>;
   ops->m2l = &m2l_<T, P>;

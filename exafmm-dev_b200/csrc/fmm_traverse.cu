@@ -18,12 +18,19 @@ namespace fmmb200 {
 
 enum { PAIR_M2L = 0, PAIR_P2P = 1, PAIR_SPLIT_I = 2, PAIR_SPLIT_J = 3, PAIR_SPLIT_IJ = 4 };
 
+// cj: source cell with the periodic image of the source tree in its top bits (pair_cell,
+// pair_img); the distance is (Xi - Xj) - Xperiodic as the reference rounds it (:38)
 template <typename T>
-__device__ __forceinline__ int classify(int ci, int cj, const vec4<T>* __restrict__ X,
+__device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
                                         const int* __restrict__ nchild,
-                                        const int* __restrict__ nbody, int nspawn, int* nout) {
+                                        const int* __restrict__ nbody, int nspawn, T cycle,
+                                        int* nout) {
+  const int cj = pair_cell((unsigned)cjp);
+  T px, py, pz;
+  img_shift<T>(pair_img((unsigned)cjp), cycle, px, py, pz);
   vec4<T> a = X[ci], b = X[cj];
-  T R2 = norm_rn(sub_rn(a.x, b.x), sub_rn(a.y, b.y), sub_rn(a.z, b.z));
+  T R2 = norm_rn(sub_rn(sub_rn(a.x, b.x), px), sub_rn(sub_rn(a.y, b.y), py),
+                 sub_rn(sub_rn(a.z, b.z), pz));
   T Rs = add_rn(a.w, b.w);
   if (R2 > mul_rn(Rs, Rs)) {
     *nout = 1;
@@ -58,13 +65,13 @@ __device__ __forceinline__ int classify(int ci, int cj, const vec4<T>* __restric
 template <typename T>
 __global__ void k_trav_count(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
-                             const int* __restrict__ nbody, int nspawn,
+                             const int* __restrict__ nbody, int nspawn, T cycle,
                              unsigned long long* __restrict__ counters) {
   unsigned long long c[3] = {0, 0, 0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
     int2 p = front[t];
     int k;
-    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, &k);
     c[ty == PAIR_M2L ? 0 : ty == PAIR_P2P ? 1 : 2] += k;
   }
   for (int i = 0; i < 3; i++) {
@@ -96,7 +103,7 @@ template <typename T>
 __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
                              const int* __restrict__ ichild, const int* __restrict__ nbody,
-                             int nspawn, unsigned long long* __restrict__ counters,
+                             int nspawn, T cycle, unsigned long long* __restrict__ counters,
                              unsigned long long* __restrict__ m2l,
                              unsigned long long* __restrict__ p2p, int2* __restrict__ next) {
   const int stride = gridDim.x * blockDim.x;
@@ -109,9 +116,10 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
     int2 p = make_int2(0, 0);
     if (t < nfront) {
       p = front[t];
-      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, &k);
+      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, &k);
     }
     const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+    const int cj = pair_cell((unsigned)p.y), img = (int)((unsigned)p.y & ~kCellMask);
     const unsigned long long om = warp_alloc(&counters[0], ty == PAIR_M2L ? 1u : 0u);
     const unsigned long long op = warp_alloc(&counters[1], ty == PAIR_P2P ? 1u : 0u);
     const unsigned long long o = warp_alloc(&counters[2], ty >= PAIR_SPLIT_I ? (unsigned)k : 0u);
@@ -123,12 +131,12 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
       int c0 = ichild[p.x];
       for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
     } else if (ty == PAIR_SPLIT_J) {
-      int c0 = ichild[p.y];
-      for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, c0 + j);
+      int c0 = ichild[cj];
+      for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, (c0 + j) | img);
     } else if (ty == PAIR_SPLIT_IJ) {
-      int ci0 = ichild[p.x], cj0 = ichild[p.y];
-      int nj = nchild[p.y];
-      for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+      int ci0 = ichild[p.x], cj0 = ichild[cj];
+      int nj = nchild[cj];
+      for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, (cj0 + i % nj) | img);
     }
   }
 }
@@ -147,7 +155,7 @@ __global__ void __launch_bounds__(256)
     k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
                 unsigned long long front_cap, const vec4<T>* __restrict__ X,
                 const int* __restrict__ nchild, const int* __restrict__ ichild,
-                const int* __restrict__ nbody, int nspawn, int ncells,
+                const int* __restrict__ nbody, int nspawn, T cycle, int ncells,
                 unsigned long long* __restrict__ ctr,  // [0] M2L, [1] P2P, [2] bad index
                 unsigned long long* __restrict__ next_count, unsigned long long* __restrict__ m2l,
                 unsigned long long m2l_cap, unsigned long long* __restrict__ p2p,
@@ -172,8 +180,10 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int u = 0; u < kTravItems; u++) {
       if (t0 + u < nfront) {
-        if ((unsigned)p[u].x < (unsigned)ncells && (unsigned)p[u].y < (unsigned)ncells)
-          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, &k[u]);
+        if ((unsigned)p[u].x < (unsigned)ncells &&
+            (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
+            pair_img((unsigned)p[u].y) < 27)
+          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, cycle, &k[u]);
         else
           atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
       }
@@ -210,15 +220,17 @@ __global__ void __launch_bounds__(256)
         // every slot below the capacity is written (the next step reads up to it)
         const unsigned long long o = bn;
         const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k[u], next_cap - o);
+        const int cj = pair_cell((unsigned)p[u].y), img = (int)((unsigned)p[u].y & ~kCellMask);
         if (ty[u] == PAIR_SPLIT_I) {
           const int c0 = ichild[p[u].x];
           for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p[u].y);
         } else if (ty[u] == PAIR_SPLIT_J) {
-          const int c0 = ichild[p[u].y];
-          for (int j = 0; j < kw; j++) next[o + j] = make_int2(p[u].x, c0 + j);
+          const int c0 = ichild[cj];
+          for (int j = 0; j < kw; j++) next[o + j] = make_int2(p[u].x, (c0 + j) | img);
         } else {
-          const int ci0 = ichild[p[u].x], cj0 = ichild[p[u].y], nj = nchild[p[u].y];
-          for (int i = 0; i < kw; i++) next[o + i] = make_int2(ci0 + i / nj, cj0 + i % nj);
+          const int ci0 = ichild[p[u].x], cj0 = ichild[cj], nj = nchild[cj];
+          for (int i = 0; i < kw; i++)
+            next[o + i] = make_int2(ci0 + i / nj, (cj0 + i % nj) | img);
         }
         bn += k[u];
       }
@@ -262,19 +274,28 @@ __global__ void k_p2p_bodypairs(const unsigned long long* __restrict__ pairs, lo
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     unsigned long long p = pairs[t];
-    s += (unsigned long long)nbody[p >> 32] * (unsigned long long)nbody[p & 0xffffffffULL];
+    s += (unsigned long long)nbody[p >> 32] * (unsigned long long)nbody[pair_cell((unsigned)p)];
   }
   s = warp_sum(s);
   if (lane_id() == 0 && s) atomicAdd(out, s);
 }
 
-// (target << 32 | source) <-> (target << b | source)
-__global__ void k_pack_pairs(unsigned long long* __restrict__ a, long long n, int b, int pack) {
+// (target << 32 | image << 27 | cell) <-> (target << (b + ib) | image << b | cell): sort keys
+// of 2 b + ib bits (ib = 5 with periodic images, else 0)
+__global__ void k_pack_pairs(unsigned long long* __restrict__ a, long long n, int b, int ib,
+                             int pack) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const unsigned long long v = a[t];
-    if (pack) a[t] = ((v >> 32) << b) | (v & 0xffffffffULL);
-    else a[t] = ((v >> b) << 32) | (v & ((1ULL << b) - 1));
+    if (pack) {
+      const unsigned src = (unsigned)v;
+      a[t] = ((v >> 32) << (b + ib)) | ((unsigned long long)pair_img(src) << b) |
+             (unsigned long long)pair_cell(src);
+    } else {
+      const unsigned long long src = ((v >> b) & ((1ULL << ib) - 1)) << kImgShift |
+                                     (v & ((1ULL << b) - 1));
+      a[t] = ((v >> (b + ib)) << 32) | src;
+    }
   }
 }
 
@@ -285,11 +306,23 @@ static int bits_for(int n) {
 }
 
 template <typename T> static void upload_roots(Solver<T>& s) {
-  // one (root, root) pair per solve of the batch: lists never cross solves
-  std::vector<int2> roots(s.nroots);
-  for (int r = 0; r < s.nroots; r++) roots[r] = make_int2(s.root_cell[r], s.root_cell[r]);
-  s.front.ensure(std::max(s.nroots, 1));
-  FMM_CUDA(cudaMemcpyAsync(s.front.p, roots.data(), sizeof(int2) * s.nroots,
+  // one (root, root) pair per solve of the batch (lists never cross solves); with periodic
+  // images one per shift of the source tree, in the reference's image order (:250-260)
+  std::vector<int2> roots;
+  for (int r = 0; r < s.nroots; r++) {
+    if (s.cfg.images == 0) {
+      roots.push_back(make_int2(s.root_cell[r], s.root_cell[r]));
+      continue;
+    }
+    for (int ix = -1; ix <= 1; ix++)
+      for (int iy = -1; iy <= 1; iy++)
+        for (int iz = -1; iz <= 1; iz++)
+          roots.push_back(make_int2(s.root_cell[r],
+                                    s.root_cell[r] | (img_code(ix, iy, iz) << kImgShift)));
+  }
+  s.nfront0 = (int)roots.size();
+  s.front.ensure(std::max(s.nfront0, 1));
+  FMM_CUDA(cudaMemcpyAsync(s.front.p, roots.data(), sizeof(int2) * roots.size(),
                            cudaMemcpyHostToDevice, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));  // roots[] lives on the host stack
 }
@@ -302,7 +335,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
   unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
   unsigned long long* hc = (unsigned long long*)s.scal_host;
   upload_roots(s);
-  long long nfront = s.nroots, maxfront = s.nroots;
+  long long nfront = s.nfront0, maxfront = s.nfront0;
   nm2l = np2p = 0;
   // first sizes from typical list lengths per cell; grown below when they fall short
   s.m2l.ensure(std::max(1024LL, 64LL * s.ncells));
@@ -311,7 +344,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     FMM_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s.stream));
     int grid = std::min(ceil_div(nfront, TB), 148 * 16);
     k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
-                                               s.c_nbody.p, s.cfg.nspawn, cnt);
+                                               s.c_nbody.p, s.cfg.nspawn, (T)s.cfg.cycle, cnt);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaMemcpyAsync(hc, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s.stream));
@@ -337,7 +370,8 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     unsigned long long base[3] = {(unsigned long long)nm2l, (unsigned long long)np2p, 0};
     FMM_CUDA(cudaMemcpyAsync(cnt, base, sizeof(base), cudaMemcpyHostToDevice, s.stream));
     k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
-                                               s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn, cnt,
+                                               s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn,
+                                               (T)s.cfg.cycle, cnt,
                                                s.m2l.p, s.p2p.p, s.front2.p);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
@@ -363,7 +397,7 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
   unsigned long long* hctr = (unsigned long long*)s.scal_host + 32;
   upload_roots(s);
   FMM_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * (4 + steps), s.stream));
-  hctr[3] = (unsigned long long)s.nroots;
+  hctr[3] = (unsigned long long)s.nfront0;
   FMM_CUDA(cudaMemcpyAsync(ctr + 3, hctr + 3, sizeof(unsigned long long),
                            cudaMemcpyHostToDevice, s.stream));
   const unsigned long long fcap = std::min(s.front.cap, s.front2.cap);
@@ -372,7 +406,8 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
     DevArr<int2>& out = (l & 1) ? s.front : s.front2;
     k_trav_step<T><<<148 * 8, TB, 0, s.stream>>>(
         in.p, ctr + 3 + l, fcap, s.cX.p, s.c_nchild.p, s.c_ichild.p, s.c_nbody.p,
-        s.cfg.nspawn, s.ncells, ctr, ctr + 4 + l, s.m2l.p, s.m2l.cap, s.p2p.p, s.p2p.cap,
+        s.cfg.nspawn, (T)s.cfg.cycle, s.ncells, ctr, ctr + 4 + l, s.m2l.p, s.m2l.cap, s.p2p.p,
+        s.p2p.cap,
         out.p, fcap);
     FMM_LAUNCH_CHECK();
   }
@@ -392,6 +427,8 @@ template <typename T> void build_lists(Solver<T>& s) {
   const int TB = 256;
   s.nm2l = s.np2p = s.p2p_body_pairs = 0;
   if (s.ncells == 0) return;
+  if (s.ncells > (int)kCellMask)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED, "more than 2^27 - 1 cells (list pairs hold 27-bit cells)");
   unsigned long long* cnt = (unsigned long long*)s.scal.p;  // [0..2] counts, [3] body pairs
   unsigned long long* hc = (unsigned long long*)s.scal_host;
   long long nm2l = 0, np2p = 0;
@@ -404,19 +441,20 @@ template <typename T> void build_lists(Solver<T>& s) {
   }
   s.nm2l = nm2l;
   s.np2p = np2p;
-  // sort on (target << b | source) with b = bits(ncells): 2b key bits instead of 32 + b
-  const int b = bits_for(s.ncells);
+  // sort on (target << (b + ib) | image << b | source) with b = bits(ncells): 2 b + ib key
+  // bits instead of 64
+  const int b = bits_for(s.ncells), ib = s.cfg.images > 0 ? 5 : 0;
   s.list_tmp.ensure(std::max<long long>(std::max(nm2l, np2p), 1));
   for (int which = 0; which < 2; which++) {
     DevArr<unsigned long long>& lst = which ? s.p2p : s.m2l;
     const long long cnt = which ? np2p : nm2l;
     if (cnt == 0) continue;
     const int grid = std::min(ceil_div(cnt, TB), 148 * 16);
-    k_pack_pairs<<<grid, TB, 0, s.stream>>>(lst.p, cnt, b, 1);
+    k_pack_pairs<<<grid, TB, 0, s.stream>>>(lst.p, cnt, b, ib, 1);
     FMM_LAUNCH_CHECK();
     s.list_tmp.ensure(cnt);
-    sort_keys_u64(s, lst.p, s.list_tmp.p, (int)cnt, 2 * b);
-    k_pack_pairs<<<grid, TB, 0, s.stream>>>(s.list_tmp.p, cnt, b, 0);
+    sort_keys_u64(s, lst.p, s.list_tmp.p, (int)cnt, 2 * b + ib);
+    k_pack_pairs<<<grid, TB, 0, s.stream>>>(s.list_tmp.p, cnt, b, ib, 0);
     FMM_LAUNCH_CHECK();
     std::swap(lst, s.list_tmp);
   }

@@ -11,7 +11,9 @@
 // around the solve: positions wrapped into [-cycle/2, cycle/2] (vec.h wrap, :193-204),
 // incoming p and f taken as initial TRG values (which kernel::L2P then divides by the
 // charge), the dipole correction of UpDownPass::dipoleCorrection (up_down_pass.h:160-168)
-// applied with the given cycle, and p / f overwritten per original index.
+// applied with the given cycle, and p / f overwritten per original index.  Periodic
+// images (FMM_Init's images > 0) are the solver's own: the 27 nearest copies through the
+// tree and images - 1 levels of super-cells through the root multipole.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,6 +25,7 @@ namespace {
 
 fmm_b200_solver* g_solver = nullptr;
 bool g_verbose = false;
+int g_images = 0;  // periodic image levels given to FMM_Init / fmm_init_
 
 int env_order() {
   const char* e = std::getenv("EXAFMM_B200_P");
@@ -35,10 +38,7 @@ void init_solver(int images, double theta, int ncrit, bool verbose) {
     g_solver = nullptr;
   }
   g_verbose = verbose;
-  if (images != 0) {
-    std::fprintf(stderr, "exafmm_b200: periodic images (%d) are not supported\n", images);
-    return;
-  }
+  g_images = images;
   fmm_b200_config cfg;
   fmm_b200_default_config(&cfg);
   cfg.P = env_order();
@@ -48,6 +48,7 @@ void init_solver(int images, double theta, int ncrit, bool verbose) {
   cfg.use_rmax = 1;
   cfg.use_ropt = 1;
   cfg.eps2 = 0.0;
+  cfg.images = images;
   int rc = fmm_b200_create(&cfg, &g_solver);
   if (rc != FMM_OK) {
     std::fprintf(stderr, "exafmm_b200: create failed (%d): %s\n", rc, fmm_b200_last_error(nullptr));
@@ -61,13 +62,15 @@ double wrap1(double v, double w) {
   return v;
 }
 
-// solve bodies (x: 3n wrapped positions, q: n) -> phi, grad phi per body (trg: 4n)
-bool solve(int n, const std::vector<double>& x, const std::vector<double>& q,
+// solve bodies (x: 3n wrapped positions, q: n) -> phi, grad phi per body (trg: 4n), with
+// the periodic images of the box of side cycle when images > 0
+bool solve(int n, const std::vector<double>& x, const std::vector<double>& q, double cycle,
            std::vector<double>& trg) {
   if (!g_solver) return false;
   trg.assign(4 * (size_t)n, 0.0);
   std::vector<double> p(n), f(3 * (size_t)n);
-  int rc = fmm_b200_solve_host(g_solver, n, x.data(), q.data(), p.data(), f.data());
+  int rc = fmm_b200_set_periodic(g_solver, g_images, cycle);
+  if (rc == FMM_OK) rc = fmm_b200_solve_host(g_solver, n, x.data(), q.data(), p.data(), f.data());
   if (rc != FMM_OK) {
     std::fprintf(stderr, "exafmm_b200: solve failed (%d): %s\n", rc, fmm_b200_last_error(g_solver));
     return false;
@@ -102,7 +105,7 @@ void FMM_Coulomb(int n, double* x, double* q, double* p, double* f, double cycle
   if (!g_solver || n <= 0) return;
   std::vector<double> xw(3 * (size_t)n), qv(q, q + n), trg;
   for (int i = 0; i < 3 * n; i++) xw[i] = wrap1(x[i], cycle);
-  if (!solve(n, xw, qv, trg)) return;
+  if (!solve(n, xw, qv, cycle, trg)) return;
   double dip[3] = {0, 0, 0};
   for (int i = 0; i < n; i++)
     for (int d = 0; d < 3; d++) dip[d] += xw[3 * i + d] * q[i];
@@ -145,7 +148,7 @@ void fmm_coulomb_(int* nglobal, int* icpumap, double* x, double* q, double* p, d
     for (int d = 0; d < 3; d++) xw[3 * k + d] = wrap1(x[3 * i + d], *cycle);
     qv[k] = q[i];
   }
-  if (!solve(n, xw, qv, trg)) return;
+  if (!solve(n, xw, qv, *cycle, trg)) return;
   double dip[3] = {0, 0, 0};
   for (int k = 0; k < n; k++)
     for (int d = 0; d < 3; d++) dip[d] += xw[3 * k + d] * qv[k];

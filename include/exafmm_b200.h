@@ -56,8 +56,12 @@ typedef struct fmm_b200_config {
   int use_ropt;    /* include/args.h:99 (-o) */
   int precision;   /* FMM_FP32 or FMM_FP64 */
   double eps2;     /* softening squared (Traversal::eps2; see fmm_b200_config note) */
-  int images;      /* periodic image levels; only 0 is supported */
+  int images;      /* periodic image levels (Traversal::images, include/traversal.h:21):
+                    * 0 open boundary; k > 0: the 27 nearest copies of the box through the
+                    * tree and k - 1 levels of 3x3x3 super-cells of copies through the root
+                    * multipole (traversePeriodic); spherical basis only */
   int device;      /* CUDA device ordinal */
+  double cycle;    /* period of the box when images > 0 (dualTreeTraversal's cycle) */
 } fmm_b200_config;
 
 typedef struct fmm_b200_solver fmm_b200_solver;
@@ -82,6 +86,9 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out);
 int fmm_b200_destroy(fmm_b200_solver* s);
 /* Work is issued on this stream (a cudaStream_t; NULL = the legacy default stream). */
 int fmm_b200_set_stream(fmm_b200_solver* s, void* stream);
+/* Periodic boundary of the next traversals: image levels and period (the arguments the
+ * reference passes to Traversal() and dualTreeTraversal(); include/traversal.h:216-264). */
+int fmm_b200_set_periodic(fmm_b200_solver* s, int images, double cycle);
 /* Message of the last failure on this handle (or of the last failed create if s is NULL). */
 const char* fmm_b200_last_error(const fmm_b200_solver* s);
 /* Which P values were compiled for a basis: writes up to cap values, returns the count. */
@@ -139,8 +146,10 @@ int fmm_b200_get_box(fmm_b200_solver* s, double* x0r0);
 /* which = 0: multipoles M, 1: locals L.  Spherical: NTERM (re, im) pairs per cell;
  * Cartesian: NTERM reals per cell. */
 int fmm_b200_get_expansion(fmm_b200_solver* s, int which, double* out);
-/* Interaction lists of the last traversal: cell pairs packed (target << 32) | source,
- * sorted; body-pair counts are the sum of target x source body counts. */
+/* Interaction lists of the last traversal: cell pairs packed (target << 32) | source |
+ * image << 27, sorted; image is 0 without periodic images, else the source tree's shift
+ * (ix, iy, iz) cycle, |i| <= 1, coded 9 d(ix) + 3 d(iy) + d(iz) with d(0) = 0, d(1) = 1,
+ * d(-1) = 2.  Body-pair counts are the sum of target x source body counts. */
 int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2p,
                        long long* p2p_body_pairs);
 int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
@@ -211,8 +220,8 @@ long long fmm_b200_kernel_launches(void);
 /* ---- reference wrapper ABI (single GPU, single rank) ----------------------------------
  * FMM_Init: the gromacs wrapper's fixed parameters (ncrit 32, nspawn 1000, theta 0.4,
  * use_rmax, use_ropt, eps2 0, wrappers/gromacs.cxx:28-56) on the spherical basis at
- * EXAFMM_B200_P (default 10) in FP32; images must be 0 (periodic boundaries are not
- * supported: the call leaves the library uninitialised and FMM_Coulomb does nothing). */
+ * EXAFMM_B200_P (default 10) in FP32, with `images` periodic image levels of the box of
+ * side `cycle` that each FMM_Coulomb call passes. */
 void FMM_Init(int images);
 void FMM_Finalize(void);
 #ifdef __cplusplus

@@ -15,8 +15,8 @@
 //     (phi, grad phi per unit charge, include/types.h:71 and kernels/*CPU.cxx L2P).
 // Run-time parameters replace the reference's compile-time ones (EXPANSION, Spherical /
 // Cartesian, FP64, include/types.h:12-45): set them in a Context before building.
-// Only the non-periodic, non-mutual path exists (images = 0); Traversal::direct runs the
-// FP64 direct sum on the GPU.
+// Periodic images (spherical basis) are supported, mutual interactions are not;
+// Traversal::direct runs the FP64 direct sum on the GPU (one call per periodic shift).
 #pragma once
 #include <complex>
 #include <cstdint>
@@ -245,7 +245,7 @@ class UpDownPass {
   Context& ctx_;
 };
 
-// Traversal (include/traversal.h:214-337); images = 0, mutual = false only.
+// Traversal (include/traversal.h:214-337); mutual = false only.
 class Traversal {
  public:
   Traversal(int nspawn, int images, real_t eps2, Context& ctx = Context::global()) : ctx_(ctx) {
@@ -256,29 +256,41 @@ class Traversal {
   void dualTreeTraversal(Cells& icells, Cells& jcells, real_t cycle, bool mutual,
                          real_t remote = 1) {
     (void)jcells;
-    (void)cycle;
     (void)remote;
     if (mutual) throw Error(FMM_ERR_NOT_SUPPORTED, "mutual traversal is not supported");
     if (icells.empty()) return;
+    ctx_.check(fmm_b200_set_periodic(ctx_.get(), ctx_.cfg.images, (double)cycle));
     ctx_.check(fmm_b200_traverse(ctx_.get()));
   }
   // direct sum on the GPU in FP64: TRG of ibodies += contributions of jbodies
   // (times the target's own charge, as kernel::P2P leaves it before normalize)
+  // with periodic images: the shifts (ix, iy, iz) cycle, |i| <= sum_{l < images} 3^l, of
+  // the reference's DirectRecursion (:266-301)
   void direct(Bodies& ibodies, Bodies& jbodies, real_t cycle) {
-    (void)cycle;
     const int nt = (int)ibodies.size(), ns = (int)jbodies.size();
-    std::vector<double> xt(3 * (size_t)nt), xs(3 * (size_t)ns), qs(ns), out(4 * (size_t)nt);
+    std::vector<double> x0(3 * (size_t)nt), xt(3 * (size_t)nt), xs(3 * (size_t)ns), qs(ns),
+        out(4 * (size_t)nt), acc(4 * (size_t)nt, 0.0);
     for (int i = 0; i < nt; i++)
-      for (int d = 0; d < 3; d++) xt[3 * i + d] = ibodies[i].X[d];
+      for (int d = 0; d < 3; d++) x0[3 * i + d] = ibodies[i].X[d];
     for (int j = 0; j < ns; j++) {
       for (int d = 0; d < 3; d++) xs[3 * j + d] = jbodies[j].X[d];
       qs[j] = jbodies[j].SRC;
     }
-    int rc = fmm_b200_direct(ctx_.cfg.device, nt, xt.data(), ns, xs.data(), qs.data(),
-                             (double)(int)ctx_.cfg.eps2, out.data());
-    if (rc != FMM_OK) throw Error(rc, "direct sum failed");
+    int prange = 0;
+    for (int l = 0, p3 = 1; l < ctx_.cfg.images; l++, p3 *= 3) prange += p3;
+    for (int ix = -prange; ix <= prange; ix++)
+      for (int iy = -prange; iy <= prange; iy++)
+        for (int iz = -prange; iz <= prange; iz++) {
+          const double sh[3] = {ix * (double)cycle, iy * (double)cycle, iz * (double)cycle};
+          for (int i = 0; i < nt; i++)
+            for (int d = 0; d < 3; d++) xt[3 * i + d] = x0[3 * i + d] - sh[d];
+          int rc = fmm_b200_direct(ctx_.cfg.device, nt, xt.data(), ns, xs.data(), qs.data(),
+                                   (double)(int)ctx_.cfg.eps2, out.data());
+          if (rc != FMM_OK) throw Error(rc, "direct sum failed");
+          for (size_t k = 0; k < acc.size(); k++) acc[k] += out[k];
+        }
     for (int i = 0; i < nt; i++)
-      for (int d = 0; d < 4; d++) ibodies[i].TRG[d] += ibodies[i].SRC * out[4 * (size_t)i + d];
+      for (int d = 0; d < 4; d++) ibodies[i].TRG[d] += ibodies[i].SRC * acc[4 * (size_t)i + d];
   }
   void normalize(Bodies& bodies) {  // include/traversal.h:333-337
     for (Body& B : bodies)

@@ -72,8 +72,11 @@ typedef struct {
   unsigned long long* icell;
   real *cX, *R, *Rbuilt;
   real *M, *L;
-  /* lists (target << 32 | source) in visiting order */
+  /* lists (target << 32 | source | image << 27) in visiting order */
   long long *m2l, *p2p;
+  /* periodic shift of the source tree in the traversal under way, and its image code */
+  real xp[3];
+  int img;
   long long nm2l, np2p, capm2l, capp2p;
   /* cartesian index helpers */
   int* cidx;   /* [nx][ny][nz] -> term, size P^3 */
@@ -298,18 +301,20 @@ int oracle_build_tree(void* h) {
   free(xb); free(qb); free(ib);
   int nc = o->nodes[o->root].nnode;
   o->nc = nc;
-  o->iparent = (int*)calloc(nc, sizeof(int));
-  o->ichild = (int*)calloc(nc, sizeof(int));
-  o->nchild = (int*)calloc(nc, sizeof(int));
-  o->cibody = (int*)calloc(nc, sizeof(int));
-  o->cnbody = (int*)calloc(nc, sizeof(int));
-  o->clevel = (int*)calloc(nc, sizeof(int));
-  o->icell = (unsigned long long*)calloc(nc, sizeof(unsigned long long));
-  o->cX = (real*)calloc(3 * nc, sizeof(real));
-  o->R = (real*)calloc(nc, sizeof(real));
-  o->Rbuilt = (real*)calloc(nc, sizeof(real));
-  o->M = (real*)calloc((size_t)nc * o->ncoef, sizeof(real));
-  o->L = (real*)calloc((size_t)nc * o->ncoef, sizeof(real));
+  /* cell arrays hold 27 more cells past the tree: the periodic cells of traversePeriodic */
+  int na = nc + 27;
+  o->iparent = (int*)calloc(na, sizeof(int));
+  o->ichild = (int*)calloc(na, sizeof(int));
+  o->nchild = (int*)calloc(na, sizeof(int));
+  o->cibody = (int*)calloc(na, sizeof(int));
+  o->cnbody = (int*)calloc(na, sizeof(int));
+  o->clevel = (int*)calloc(na, sizeof(int));
+  o->icell = (unsigned long long*)calloc(na, sizeof(unsigned long long));
+  o->cX = (real*)calloc(3 * na, sizeof(real));
+  o->R = (real*)calloc(na, sizeof(real));
+  o->Rbuilt = (real*)calloc(na, sizeof(real));
+  o->M = (real*)calloc((size_t)na * o->ncoef, sizeof(real));
+  o->L = (real*)calloc((size_t)na * o->ncoef, sizeof(real));
   nodes2cells(o, o->root, 0, 1, 0, 0);
   memcpy(o->Rbuilt, o->R, sizeof(real) * nc);
   return 0;
@@ -452,7 +457,7 @@ static void sph_m2l(Oracle* o, int ci, int cj) {
   cplx Ynmi[P * P];
   cplx *Mi = CM(o, ci), *Mj = CM(o, cj), *Li = CL(o, ci);
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
   real rho, alpha, beta;
   cart2sph(&rho, &alpha, &beta, dX);
   eval_local(P, rho, alpha, beta, Ynmi);
@@ -668,7 +673,7 @@ static void cart_m2l(Oracle* o, int ci, int cj) {
   real *Mi = &o->M[(size_t)ci * o->ncoef], *Mj = &o->M[(size_t)cj * o->ncoef];
   real* Li = &o->L[(size_t)ci * o->ncoef];
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
   real invR2 = 1 / (dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2]);
   real invR = o->p.mass ? Mi[0] * Mj[0] * sqrt(invR2) : sqrt(invR2);
   cart_coef(o, C, dX, invR2, invR);
@@ -761,7 +766,7 @@ static void p2p_pair(Oracle* o, int ci, int cj) {
     real ppot = 0, pax = 0, pay = 0, paz = 0;
     for (int j = o->cibody[cj]; j < o->cibody[cj] + o->cnbody[cj]; j++) {
       real dX[3];
-      for (int d = 0; d < 3; d++) dX[d] = o->x[3 * i + d] - o->x[3 * j + d];
+      for (int d = 0; d < 3; d++) dX[d] = o->x[3 * i + d] - o->x[3 * j + d] - o->xp[d];
       real R2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2] + o->eps2;
       if (R2 != 0) {
         real invR2 = 1.0 / R2;
@@ -880,12 +885,12 @@ int oracle_upward(void* h) {
 }
 
 /* ------------------------------------------------------------------ traversal */
-static void push_pair(long long** a, long long* n, long long* cap, int i, int j) {
+static void push_pair(long long** a, long long* n, long long* cap, int i, int j, int img) {
   if (*n == *cap) {
     *cap = *cap ? 2 * *cap : 4096;
     *a = (long long*)realloc(*a, sizeof(long long) * *cap);
   }
-  (*a)[(*n)++] = ((long long)i << 32) | (long long)j;
+  (*a)[(*n)++] = ((long long)i << 32) | (long long)j | ((long long)img << 27);
 }
 
 static void traverse(Oracle* o, int ci, int cj);
@@ -927,26 +932,96 @@ static void split_cell(Oracle* o, int ci, int cj) {
 /* Traversal::traverse (include/traversal.h:37-62), kernels applied as pairs are visited */
 static void traverse(Oracle* o, int ci, int cj) {
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
   real R2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2];
   real Rs = o->R[ci] + o->R[cj];
   if (R2 > Rs * Rs) {
-    push_pair(&o->m2l, &o->nm2l, &o->capm2l, ci, cj);
+    push_pair(&o->m2l, &o->nm2l, &o->capm2l, ci, cj, o->img);
     if (o->p.basis == ORACLE_SPHERICAL) sph_m2l(o, ci, cj); else cart_m2l(o, ci, cj);
   } else if (o->nchild[ci] == 0 && o->nchild[cj] == 0) {
-    push_pair(&o->p2p, &o->np2p, &o->capp2p, ci, cj);
+    push_pair(&o->p2p, &o->np2p, &o->capp2p, ci, cj, o->img);
     if (R2 == 0 && ci == cj) p2p_self(o, ci); else p2p_pair(o, ci, cj);
   } else {
     split_cell(o, ci, cj);
   }
 }
 
-/* Traversal::dualTreeTraversal, images = 0 (include/traversal.h:240-248) */
+static int img_digit(int i) { return i < 0 ? 2 : i; }
+
+/* Traversal::traversePeriodic (include/traversal.h:127-185) for a non-MASS build: the
+ * periodic parent cell (scratch cell nc + 26, the source root's copy with the 26 scratch
+ * cells nc .. nc + 25 as children) sends M2L to the target root from the 26 x 27 images
+ * around the 3 x 3 x 3 block of each sub-level, then becomes the M2M of its 26 shifted
+ * copies (the centre copy is not among the children, as in the reference), and the
+ * period grows three times. */
+static void traverse_periodic(Oracle* o) {
+  const int base = o->nc, pc = o->nc + 26;
+  const int nco = o->ncoef;
+  for (int d = 0; d < 3; d++) o->cX[3 * pc + d] = o->cX[d];
+  o->R[pc] = o->R[0];
+  memcpy(&o->M[(size_t)pc * nco], &o->M[0], sizeof(real) * nco);
+  o->ichild[pc] = base;
+  o->nchild[pc] = 26;
+  real cycle = (real)o->p.cycle;
+  for (int level = 0; level < o->p.images - 1; level++) {
+    for (int ix = -1; ix <= 1; ix++)
+      for (int iy = -1; iy <= 1; iy++)
+        for (int iz = -1; iz <= 1; iz++) {
+          if (ix == 0 && iy == 0 && iz == 0) continue;
+          for (int cx = -1; cx <= 1; cx++)
+            for (int cy = -1; cy <= 1; cy++)
+              for (int cz = -1; cz <= 1; cz++) {
+                o->xp[0] = (real)(ix * 3 + cx) * cycle;
+                o->xp[1] = (real)(iy * 3 + cy) * cycle;
+                o->xp[2] = (real)(iz * 3 + cz) * cycle;
+                if (o->p.basis == ORACLE_SPHERICAL) sph_m2l(o, 0, pc); else cart_m2l(o, 0, pc);
+              }
+        }
+    int k = base;
+    for (int ix = -1; ix <= 1; ix++)
+      for (int iy = -1; iy <= 1; iy++)
+        for (int iz = -1; iz <= 1; iz++) {
+          if (ix == 0 && iy == 0 && iz == 0) continue;
+          o->cX[3 * k] = o->cX[3 * pc] + (real)ix * cycle;
+          o->cX[3 * k + 1] = o->cX[3 * pc + 1] + (real)iy * cycle;
+          o->cX[3 * k + 2] = o->cX[3 * pc + 2] + (real)iz * cycle;
+          memcpy(&o->M[(size_t)k * nco], &o->M[(size_t)pc * nco], sizeof(real) * nco);
+          k++;
+        }
+    memset(&o->M[(size_t)pc * nco], 0, sizeof(real) * nco);
+    if (o->p.basis == ORACLE_SPHERICAL) sph_m2m(o, pc); else cart_m2m(o, pc);
+    cycle *= 3;
+  }
+  o->xp[0] = o->xp[1] = o->xp[2] = 0;
+}
+
+/* Traversal::dualTreeTraversal (include/traversal.h:240-264), mutual = false: from
+ * (root, root) once, or for images > 0 once per shift of the source tree by
+ * (ix, iy, iz) cycle, |i| <= 1, then traversePeriodic. */
 int oracle_traverse(void* h) {
   Oracle* o = (Oracle*)h;
   o->nm2l = o->np2p = 0;
+  o->xp[0] = o->xp[1] = o->xp[2] = 0;
+  o->img = 0;
   if (o->nc == 0) return 0;
-  traverse(o, 0, 0);
+  if (o->p.images == 0) {
+    traverse(o, 0, 0);
+    return 0;
+  }
+  if (o->p.mass) return -1; /* the MASS normalisations of traversePeriodic are not restated */
+  const real cycle = (real)o->p.cycle;
+  for (int ix = -1; ix <= 1; ix++)
+    for (int iy = -1; iy <= 1; iy++)
+      for (int iz = -1; iz <= 1; iz++) {
+        o->xp[0] = (real)ix * cycle;
+        o->xp[1] = (real)iy * cycle;
+        o->xp[2] = (real)iz * cycle;
+        o->img = 9 * img_digit(ix) + 3 * img_digit(iy) + img_digit(iz);
+        traverse(o, 0, 0);
+      }
+  o->xp[0] = o->xp[1] = o->xp[2] = 0;
+  o->img = 0;
+  traverse_periodic(o);
   return 0;
 }
 
@@ -1044,6 +1119,38 @@ void oracle_direct(int nt, const double* xt, int ns, const double* xs, const dou
         az -= dz * invR3;
       }
     }
+    out[4 * i] = pot;
+    out[4 * i + 1] = ax;
+    out[4 * i + 2] = ay;
+    out[4 * i + 3] = az;
+  }
+}
+
+void oracle_direct_periodic(int nt, const double* xt, int ns, const double* xs,
+                            const double* qs, double eps2, int images, double cycle,
+                            double* out) {
+  int prange = 0;
+  for (int i = 0, p3 = 1; i < images; i++, p3 *= 3) prange += p3;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int i = 0; i < nt; i++) {
+    double pot = 0, ax = 0, ay = 0, az = 0;
+    for (int ix = -prange; ix <= prange; ix++)
+      for (int iy = -prange; iy <= prange; iy++)
+        for (int iz = -prange; iz <= prange; iz++)
+          for (int j = 0; j < ns; j++) {
+            double dx = xt[3 * i] - xs[3 * j] - ix * cycle;
+            double dy = xt[3 * i + 1] - xs[3 * j + 1] - iy * cycle;
+            double dz = xt[3 * i + 2] - xs[3 * j + 2] - iz * cycle;
+            double R2 = dx * dx + dy * dy + dz * dz + eps2;
+            if (R2 != 0) {
+              double invR = 1.0 / sqrt(R2);
+              double invR3 = qs[j] * invR * invR * invR;
+              pot += qs[j] * invR;
+              ax -= dx * invR3;
+              ay -= dy * invR3;
+              az -= dz * invR3;
+            }
+          }
     out[4 * i] = pot;
     out[4 * i + 1] = ax;
     out[4 * i + 2] = ay;

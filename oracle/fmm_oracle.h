@@ -30,7 +30,13 @@ typedef struct oracle_params {
   int mass;       /* MASS semantics: normalised multipoles (up_down_pass.h:29-31) */
   int kahan;      /* compensated TRG accumulation (include/types.h:27-35) */
   double eps2;    /* softening; the reference truncates it to int (traversal.h:17) */
+  int images;     /* periodic image levels (include/traversal.h:21; 0 = open boundary) */
+  double cycle;   /* period of the box (Traversal::dualTreeTraversal's cycle) */
 } oracle_params;
+
+/* Pairs in the lists are packed (target << 32) | source | image << 27, image 0 for the
+ * unshifted source and, for periodic runs, the shift (ix, iy, iz) in {-1, 0, 1}^3 coded
+ * as 9 d(ix) + 3 d(iy) + d(iz) with d(0) = 0, d(1) = 1, d(-1) = 2. */
 
 void* oracle_new(int n, const double* x, const double* q, const oracle_params* prm);
 void oracle_free(void* h);
@@ -59,6 +65,11 @@ void oracle_get_p2p(void* h, long long* out);
  * sources (3*ns positions, ns charges); out 4*nt = (phi, dphi/dx, dphi/dy, dphi/dz). */
 void oracle_direct(int nt, const double* xt, int ns, const double* xs, const double* qs,
                    double eps2, double* out);
+/* the same over the periodic images Traversal::direct sums (include/traversal.h:304-320):
+ * shifts (ix, iy, iz) cycle with |i| <= prange = sum_{l < images} 3^l */
+void oracle_direct_periodic(int nt, const double* xt, int ns, const double* xs,
+                            const double* qs, double eps2, int images, double cycle,
+                            double* out);
 /* rel-L2 (include/verify.h:18-83): returns sqrt(sum dif^2 / sum ref^2) for pot and grad */
 void oracle_rel_l2(int n, const double* trg, const double* ref, double* pot_acc);
 /* examples/kernel.cxx:5-93 chain in this precision; seed < 0 = glibc unseeded drand48 */

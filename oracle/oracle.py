@@ -22,7 +22,7 @@ class _Params(C.Structure):
     _fields_ = [("basis", C.c_int), ("P", C.c_int), ("theta", C.c_double),
                 ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
                 ("use_ropt", C.c_int), ("mass", C.c_int), ("kahan", C.c_int),
-                ("eps2", C.c_double)]
+                ("eps2", C.c_double), ("images", C.c_int), ("cycle", C.c_double)]
 
 
 def _ptr(a):
@@ -119,6 +119,10 @@ class Oracle:
         L.oracle_direct.restype = None
         L.oracle_direct.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_void_p]
+        L.oracle_direct_periodic.restype = None
+        L.oracle_direct_periodic.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_double, C.c_int, C.c_double,
+                                             C.c_void_p]
         L.oracle_rel_l2.restype = None
         L.oracle_rel_l2.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_kernel_chain.restype = C.c_double
@@ -127,11 +131,12 @@ class Oracle:
         self.precision = precision
 
     def run(self, x, q, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
-            use_ropt=0, mass=0, kahan=0, eps2=0.0, stages=15):
+            use_ropt=0, mass=0, kahan=0, eps2=0.0, stages=15, images=0, cycle=2 * np.pi):
         x = np.ascontiguousarray(x, np.float64)
         q = np.ascontiguousarray(q, np.float64)
         n = len(q)
-        prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2)
+        prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2,
+                      images, cycle)
         h = self.lib.oracle_new(n, _ptr(x), _ptr(q), C.byref(prm))
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
         run = OracleRun(self.lib, "oracle_", h, n, nterm, basis == SPHERICAL)
@@ -148,6 +153,16 @@ class Oracle:
         qs = np.ascontiguousarray(qs, np.float64)
         out = np.zeros((len(xt), 4))
         self.lib.oracle_direct(len(xt), _ptr(xt), len(xs), _ptr(xs), _ptr(qs), eps2, _ptr(out))
+        return out
+
+    def direct_periodic(self, xt, xs, qs, images, cycle, eps2=0.0):
+        """FP64 direct sum over the periodic images Traversal::direct visits."""
+        xt = np.ascontiguousarray(xt, np.float64)
+        xs = np.ascontiguousarray(xs, np.float64)
+        qs = np.ascontiguousarray(qs, np.float64)
+        out = np.zeros((len(xt), 4))
+        self.lib.oracle_direct_periodic(len(xt), _ptr(xt), len(xs), _ptr(xs), _ptr(qs), eps2,
+                                        images, cycle, _ptr(out))
         return out
 
     def kernel_chain(self, basis, P, mass=0, seed=-1):
@@ -204,7 +219,7 @@ class Reference:
             lib.ref_run.restype = C.c_void_p
             lib.ref_run.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
-                                    C.c_int, C.c_int, C.c_int]
+                                    C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
             for f in ("P", "nterm", "fp64", "spherical", "mass", "kahan"):
                 getattr(lib, "ref_" + f).restype = C.c_int
                 getattr(lib, "ref_" + f).argtypes = []
@@ -223,11 +238,12 @@ class Reference:
         self.mass, self.kahan = bool(L.ref_mass()), bool(L.ref_kahan())
 
     def run(self, x, q, ncrit=64, nspawn=1000, theta=0.4, use_rmax=1, use_ropt=0, eps2=0.0,
-            stages=15, record=True, threads=0):
+            stages=15, record=True, threads=0, images=0, cycle=2 * np.pi):
         x = np.ascontiguousarray(x, np.float64)
         q = np.ascontiguousarray(q, np.float64)
         h = self.lib.ref_run(len(q), _ptr(x), _ptr(q), ncrit, nspawn, theta, use_rmax,
-                             use_ropt, eps2, 0, stages, 1 if record else 0, threads)
+                             use_ropt, eps2, 0, stages, 1 if record else 0, threads, images,
+                             cycle)
         run = RefRun(self.lib, "ref_", h, len(q), self.nterm, self.spherical)
         if record:
             run._m2l = np.zeros(self.lib.ref_num_m2l(), np.int64)

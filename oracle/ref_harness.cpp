@@ -23,6 +23,8 @@
 namespace refrec {
 extern bool enabled;
 extern C_iter Ci0, Cj0;
+extern long long ncells;
+extern double cycle;
 extern std::vector<long long> m2l, p2p;
 }
 
@@ -65,9 +67,10 @@ int ref_kahan() {
 // stages: 1 = tree, 2 = +upward, 4 = +traversal, 8 = +downward.
 // record: record M2L/P2P lists (forces a serial traversal).
 // threads: 0 = serial (no omp parallel region), else omp parallel region with that many threads.
+// images, cycle: Traversal's periodic image levels and dualTreeTraversal's cycle.
 void* ref_run(int n, const double* x, const double* q, int ncrit, int nspawn, double theta,
               int useRmax, int useRopt, double eps2, int mutual, int stages, int record,
-              int threads) {
+              int threads, int images, double cycle) {
   RefRun* run = new RefRun();
   run->bodies.resize(n);
   for (int i = 0; i < n; i++) {
@@ -87,7 +90,8 @@ void* ref_run(int n, const double* x, const double* q, int ncrit, int nspawn, do
   BoundBox boundBox(nspawn);
   BuildTree buildTree(ncrit, nspawn);
   UpDownPass upDownPass(theta, useRmax, useRopt);
-  Traversal traversal(nspawn, 0, eps2);
+  Traversal traversal(nspawn, images, eps2);
+  refrec::cycle = cycle;
   refrec::enabled = record != 0;
   refrec::m2l.clear();
   refrec::p2p.clear();
@@ -109,7 +113,8 @@ void* ref_run(int n, const double* x, const double* q, int ncrit, int nspawn, do
     if (stages & 4) {
       refrec::Ci0 = run->cells.begin();
       refrec::Cj0 = run->cells.begin();
-      traversal.dualTreeTraversal(run->cells, run->cells, 2 * M_PI, mutual != 0);
+      refrec::ncells = run->cells.size();
+      traversal.dualTreeTraversal(run->cells, run->cells, cycle, mutual != 0);
       t4 = omp_get_wtime();
     }
     if (stages & 8) {
@@ -205,7 +210,9 @@ void ref_get_trg(void* h, double* trg) {
 
 long long ref_num_m2l() { return refrec::m2l.size(); }
 long long ref_num_p2p() { return refrec::p2p.size(); }
-// pairs packed as (target << 32) | source, in the order the reference visited them
+// pairs packed as (target << 32) | source | image << 27 (image code of the shift, 0 for
+// none), in the order the reference visited them; the M2L of traversePeriodic from cells
+// outside the tree are not recorded
 void ref_get_m2l(long long* out) { std::memcpy(out, refrec::m2l.data(), refrec::m2l.size() * 8); }
 void ref_get_p2p(long long* out) { std::memcpy(out, refrec::p2p.data(), refrec::p2p.size() * 8); }
 

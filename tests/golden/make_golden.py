@@ -8,7 +8,8 @@ Runs the reference compiled from its own sources (oracle/_ref/parity/*.so, built
 * ``<case>.npz``: bodies, tree cells, body order, M2L / P2P pair lists (sorted) and the
   potential + gradient per body, for each case in CASES.
 
-Usage (needs the reference build): python tests/golden/make_golden.py
+Usage (needs the reference build): python tests/golden/make_golden.py [case ...]
+(no case names: the kernel chain and every case)
 """
 import importlib
 import json
@@ -33,6 +34,9 @@ CASES = {
                              dict(ncrit=64, theta=0.35, use_ropt=1)),
     "cart_p5_f32_sphere": ("cart_p5_f32", "f32", "sphere", 8192,
                            dict(ncrit=32, theta=0.5, use_ropt=0)),
+    # periodic: the cube [-1, 1]^3 as the unit cell of period 2, three image levels
+    "sph_p6_f64_periodic": ("sph_p6_f64", "f64", "cube", 4096,
+                            dict(ncrit=32, theta=0.4, use_ropt=0, images=3, cycle=2.0)),
 }
 
 CHAIN = [("sph_p4_f64", "spherical", 4), ("sph_p6_f64", "spherical", 6),
@@ -41,13 +45,16 @@ CHAIN = [("sph_p4_f64", "spherical", 4), ("sph_p6_f64", "spherical", 6),
          ("cart_p6_f64", "cartesian", 6)]
 
 
-def main():
-    chain = {}
-    for cfg, basis, P in CHAIN:
-        chain["%s_p%d" % (basis, P)] = Reference(cfg).kernel_chain(-1)
-    with open(os.path.join(HERE, "kernel_chain.json"), "w") as f:
-        json.dump(chain, f, indent=1, sort_keys=True)
+def main(names):
+    if not names:
+        chain = {}
+        for cfg, basis, P in CHAIN:
+            chain["%s_p%d" % (basis, P)] = Reference(cfg).kernel_chain(-1)
+        with open(os.path.join(HERE, "kernel_chain.json"), "w") as f:
+            json.dump(chain, f, indent=1, sort_keys=True)
     for name, (cfg, prec, dist, n, kw) in CASES.items():
+        if names and name not in names:
+            continue
         x, q = datasets.make(dist, n, precision=prec)
         run = Reference(cfg).run(x, q, **kw)
         cells = run.cells()
@@ -60,4 +67,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -5,6 +5,7 @@ import importlib
 import os
 import re
 
+import numpy as np
 import pytest
 
 fmm = importlib.import_module("exafmm-dev_b200")
@@ -37,7 +38,7 @@ def test_defaults_and_orders():
     cfg = fmm.Config()
     assert lib.fmm_b200_default_config(C.byref(cfg)) == fmm.FMM_OK
     assert (cfg.basis, cfg.P, cfg.ncrit, cfg.nspawn, cfg.use_rmax, cfg.use_ropt) == (0, 10, 64, 1000, 1, 1)
-    assert abs(cfg.theta - 0.4) < 1e-15 and cfg.images == 0
+    assert abs(cfg.theta - 0.4) < 1e-15 and cfg.images == 0 and abs(cfg.cycle - 2 * np.pi) < 1e-15
     assert {4, 6, 8, 10} <= set(fmm.supported_orders(fmm.SPHERICAL))
     assert 5 in fmm.supported_orders(fmm.CARTESIAN)
     assert lib.fmm_b200_default_config(None) == fmm.FMM_ERR_INVALID
@@ -49,8 +50,17 @@ def test_create_validates_before_touching_a_device():
     lib.fmm_b200_default_config(C.byref(cfg))
     h = C.c_void_p()
     cfg.images = 1
+    cfg.basis = fmm.CARTESIAN
+    cfg.P = 5
     assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_NOT_SUPPORTED
     assert b"periodic" in lib.fmm_b200_last_error(None)
+    cfg.basis = fmm.SPHERICAL
+    cfg.P = 10
+    cfg.cycle = 0.0
+    assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_INVALID
+    cfg.images = -1
+    cfg.cycle = 1.0
+    assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_INVALID
     cfg.images = 0
     cfg.P = 99
     assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_INVALID

@@ -25,14 +25,15 @@ def _params(p):
 
 
 @pytest.mark.parametrize("case", ["sph_p6_f64_cube", "sph_p10_f32k_plummer",
-                                  "cart_p5_f32_sphere"])
+                                  "cart_p5_f32_sphere", "sph_p6_f64_periodic"])
 def test_oracle_matches_golden(case, golden_dir):
     g = np.load(os.path.join(golden_dir, case + ".npz"))
     p = json.loads(str(g["params"]))
     basis, P, mass, kahan = _params(p)
     o = Oracle(p["precision"]).run(g["x"], g["q"], basis=basis, P=P, theta=p["theta"],
                                    ncrit=p["ncrit"], use_ropt=p["use_ropt"], mass=mass,
-                                   kahan=kahan)
+                                   kahan=kahan, images=p.get("images", 0),
+                                   cycle=p.get("cycle", 2 * np.pi))
     cells = o.cells()
     for k in CELL_KEYS:
         assert np.array_equal(cells[k], g["cell_" + k]), k
@@ -118,3 +119,41 @@ def test_oracle_matches_reference(cfg, prec, dist, n, kw, datasets):
     pot, acc = rel_l2(o.trg(), r.trg())
     tol = 2e-6 if prec == "f32" else 5e-7  # the reference P2P uses AVX rsqrt + one Newton step
     assert pot < tol and acc < tol, (pot, acc)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) absent")
+@pytest.mark.parametrize("cfg,prec,images", [("sph_p6_f64", "f64", 1), ("sph_p6_f64", "f64", 2),
+                                             ("sph_p6_f64", "f64", 4), ("sph_p6_f32k", "f32", 3)])
+def test_oracle_matches_reference_periodic(cfg, prec, images, datasets):
+    """Traversal with the 27 shifted source trees and traversePeriodic's super-cells
+    (include/traversal.h:127-185, 250-260): the same pairs, with their image codes, in the
+    same visiting order, and the same potentials."""
+    R = Reference(cfg)
+    x, q = datasets.make("cube", 3000, seed=11, precision=prec)
+    kw = dict(ncrit=32, theta=0.4, use_ropt=0, images=images, cycle=2.0)
+    r = R.run(x, q, **kw)
+    o = Oracle(prec).run(x, q, P=R.P, kahan=int(R.kahan), **kw)
+    assert np.array_equal(r.m2l(), o.m2l())
+    assert np.array_equal(r.p2p(), o.p2p())
+    assert len(np.unique(o.m2l() >> 27 & 31)) == 27  # every image contributes
+    pot, acc = rel_l2(o.trg(), r.trg())
+    tol = 2e-6 if prec == "f32" else 5e-7
+    assert pot < tol and acc < tol, (pot, acc)
+
+
+def test_periodic_direct_sum():
+    """oracle_direct_periodic: the shifts |i| <= sum_{l < images} 3^l; one image level is
+    the 27 nearest copies."""
+    rng = np.random.default_rng(3)
+    xs = rng.uniform(-1, 1, (40, 3))
+    qs = rng.uniform(-1, 1, 40)
+    xt = xs[:5]
+    o = Oracle("f64")
+    got = o.direct_periodic(xt, xs, qs, 1, 2.0)
+    ref = np.zeros((5, 4))
+    for ix in (-1, 0, 1):
+        for iy in (-1, 0, 1):
+            for iz in (-1, 0, 1):
+                ref += o.direct(xt - 2.0 * np.array([ix, iy, iz]), xs, qs)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12)
+    assert np.allclose(o.direct_periodic(xt, xs, qs, 0, 2.0), o.direct(xt, xs, qs), rtol=1e-14)

@@ -154,6 +154,9 @@ __host__ __device__ __forceinline__ void load_pair(const double* p, double& a, d
 template <typename T, int P, int J0 = 0, int J1 = P>
 __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, const T* Mj, T* Lr,
                                                   T* Li) {
+  // Every product goes straight into its accumulator as one fused multiply-add; the signs
+  // ((-1)^j of :189, (-1)^min(k, mu) of the m > 0 half, the conjugations) are compile-time
+  // after unrolling and become operand negations.
 #pragma unroll
   for (int n = 0; n < P - J0; n++) {
 #pragma unroll
@@ -164,46 +167,40 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, cons
       for (int j = J0; j < J1; j++) {
         if (j + n >= P) break;
         const int a = j + n;
+        const T sr = (j & 1) ? -mr : mr, si = (j & 1) ? -mi : mi;  // (-1)^j M[n, mu]
 #pragma unroll
         for (int k = 0; k <= j; k++) {
           const int t = sidx(j, k);
-          T re, im;
           if (mu == 0) {
             // M[n,0] conj(Y[a,k])
             const T ur = yr[sidx(a, k)], ui = yi[sidx(a, k)];
-            re = mr * ur + mi * ui;
-            im = mi * ur - mr * ui;
+            Lr[t] = fma(sr, ur, Lr[t]);
+            Lr[t] = fma(si, ui, Lr[t]);
+            Li[t] = fma(si, ur, Li[t]);
+            Li[t] = fma(-sr, ui, Li[t]);
           } else {
             // m = -mu: conj(M[n,mu] Y[a, k+mu])
             const T ur = yr[sidx(a, k + mu)], ui = yi[sidx(a, k + mu)];
-            re = mr * ur - mi * ui;
-            im = -(mr * ui + mi * ur);
-            // m = +mu: (-1)^(k < mu ? k : mu) M[n,mu] Y[a, mu-k]
+            Lr[t] = fma(sr, ur, Lr[t]);
+            Lr[t] = fma(-si, ui, Lr[t]);
+            Li[t] = fma(-sr, ui, Li[t]);
+            Li[t] = fma(-si, ur, Li[t]);
+            // m = +mu: (-1)^(k < mu ? k : mu) M[n,mu] Y[a, mu-k] (conj Y[a, k-mu] if k > mu)
             const bool neg = ((k < mu ? k : mu) & 1) != 0;
-            T vr, vi;
+            const T br = neg ? -sr : sr, bi = neg ? -si : si;
             if (mu >= k) {
               const T wr = yr[sidx(a, mu - k)], wi = yi[sidx(a, mu - k)];
-              vr = mr * wr - mi * wi;
-              vi = mr * wi + mi * wr;
+              Lr[t] = fma(br, wr, Lr[t]);
+              Lr[t] = fma(-bi, wi, Lr[t]);
+              Li[t] = fma(br, wi, Li[t]);
+              Li[t] = fma(bi, wr, Li[t]);
             } else {
               const T wr = yr[sidx(a, k - mu)], wi = yi[sidx(a, k - mu)];
-              vr = mr * wr + mi * wi;
-              vi = mi * wr - mr * wi;
+              Lr[t] = fma(br, wr, Lr[t]);
+              Lr[t] = fma(bi, wi, Lr[t]);
+              Li[t] = fma(bi, wr, Li[t]);
+              Li[t] = fma(-br, wi, Li[t]);
             }
-            if (neg) {
-              re -= vr;
-              im -= vi;
-            } else {
-              re += vr;
-              im += vi;
-            }
-          }
-          if (j & 1) {
-            Lr[t] -= re;
-            Li[t] -= im;
-          } else {
-            Lr[t] += re;
-            Li[t] += im;
           }
         }
       }

@@ -90,36 +90,43 @@ __host__ __device__ __forceinline__ void multipole(const Angles<T>& a, T rho, T*
   }
 }
 
-// evalLocal (:68-101): singular harmonics rho^(-n-1) P_n^m e^(i m beta) (n - m)!-scaled
+// evalLocal (:68-101): singular harmonics y[n, m] = (-1)^n r^-(n+1) (n - m)! P_n^m e^(i m beta)
+// with the reference's P_n^m.  Q[n] = (n - m)! P_n^m follows
+//   Q[m] = P_m^m,   Q[n + 1] = (2n + 1) x Q[n] - (n + m)(n - m) Q[n - 1]
+// (the reference's recurrence times (n + 1 - m)!), so each term costs one multiply and one
+// fused multiply-add, and the radial factor is a table of P powers of -1/r.
 template <typename T, int P>
 __host__ __device__ __forceinline__ void local(const Angles<T>& a, T* yr, T* yi) {
+  const T ninvr = -T(1) / a.r;
   T fact = 1, pn = 1;
-  T invR = -T(1) / a.r;
-  T rhom = -invR;
+  T rpm = -ninvr;  // (-1)^m / r^(m+1)
   T er = 1, ei = 0;
 #pragma unroll
   for (int m = 0; m < P; m++) {
-    T p = pn;
-    yr[sidx(m, m)] = rhom * p * er;
-    yi[sidx(m, m)] = rhom * p * ei;
-    T p1 = p;
-    p = a.x * (2 * m + 1) * p1;
-    rhom *= invR;
-    T rhon = rhom;
+    T q = pn, qm1 = 0;  // Q[m] = P_m^m
+    {
+      const T t = q * rpm;
+      yr[sidx(m, m)] = t * er;
+      yi[sidx(m, m)] = t * ei;
+    }
+    T rpn = rpm;
 #pragma unroll
     for (int n = m + 1; n < P; n++) {
-      yr[sidx(n, m)] = rhon * p * er;
-      yi[sidx(n, m)] = rhon * p * ei;
-      T p2 = p1;
-      p1 = p;
-      p = (a.x * (2 * n + 1) * p1 - (n + m) * p2) * (T(1) / T(n - m + 1));
-      rhon *= invR * (n - m + 1);
+      // Q[n] = (2n - 1) x Q[n-1] - (n - 1 + m)(n - 1 - m) Q[n-2]
+      const T qn = fma(T(2 * n - 1) * a.x, q, T(-(n - 1 + m) * (n - 1 - m)) * qm1);
+      qm1 = q;
+      q = qn;
+      rpn *= ninvr;
+      const T t = q * rpn;
+      yr[sidx(n, m)] = t * er;
+      yi[sidx(n, m)] = t * ei;
     }
+    rpm *= ninvr;
     pn = -pn * fact * a.y;
     fact += 2;
-    T t = er * a.cb - ei * a.sb;
+    const T tt = er * a.cb - ei * a.sb;
     ei = er * a.sb + ei * a.cb;
-    er = t;
+    er = tt;
   }
 }
 

@@ -315,10 +315,10 @@ __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
 }
 
 // warps per block of one FP32 M2L pass: as many as the pass's registers allow in one block
-// per SM without spilling (P = 10: about 130, 128 and 154 registers for the passes starting
-// at degrees 0, 3 and 6)
+// per SM without spilling (P = 10: 128, 140 and 165 registers for the passes starting at
+// degrees 0, 3 and 6; ptxas keeps 13-15-warp blocks at 128 registers)
 __host__ __device__ constexpr int m2l_pass_warps(int P, int J0) {
-  return P == 10 ? (J0 == 0 ? 14 : (J0 == 3 ? 15 : 12)) : kM2LWarps;
+  return P == 10 ? (J0 == 0 ? 14 : 12) : kM2LWarps;
 }
 
 // Warps of a block run in lockstep (a block barrier per batch of 32 sources) so that they

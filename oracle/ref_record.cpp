@@ -8,6 +8,7 @@
 #undef kernel_h
 #include "kernel.h"
 #include <cmath>
+#include <cstdint>
 #include <vector>
 
 namespace refrec {
@@ -26,7 +27,13 @@ static inline long long image(const vec3& Xp) {
   }
   return c;
 }
-static inline bool in_tree(C_iter C) { return C - Cj0 >= 0 && C - Cj0 < ncells; }
+// by address: iterator subtraction across unrelated arrays is undefined (compilers divide
+// the byte distance by sizeof(Cell) assuming it is a multiple of it)
+static inline bool in_tree(C_iter C) {
+  const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(&*C);
+  const std::uintptr_t b = reinterpret_cast<std::uintptr_t>(&*Cj0);
+  return a >= b && a < b + (std::uintptr_t)ncells * sizeof(Cell);
+}
 static inline long long pack(C_iter Ci, C_iter Cj, const vec3& Xp) {
   return ((long long)(Ci - Ci0) << 32) | (long long)(Cj - Cj0) | (image(Xp) << 27);
 }

@@ -505,6 +505,13 @@ def main():
             pg.destroy_process_group()
         return
 
+    # what the ncrit autotuner would pick for this workload (the headline keeps ncrit = 64)
+    tuner = fmm.Solver(precision="f32", device=local, **kw)
+    tuner.set_stream(stream.cuda_stream)
+    best, tms = tuner.autotune_ncrit(x, q, candidates=(32, 48, 64, 96, 128), repeats=3)
+    autotune = {"best_ncrit": best, "median_ms": {str(k): v for k, v in tms.items()}}
+    del tuner
+
     batched = None if args.no_batch else bench_batched(fmm, datasets, torch, dev, stream, flush,
                                                        local, args.steps)
     serving = None if args.no_serve else bench_serving(fmm, datasets, local)
@@ -555,6 +562,7 @@ def main():
                      "frac": m2l_tflops / peak, "traffic": traffic,
                      "peak_source": "fmm_b200_fp32_peak: FMA probe measured on this GPU in this run"},
         "cpu_baseline": cpu,
+        "autotune_ncrit": autotune,
         "batched": batched,
         "serving": serving,
         "clocks": clk,

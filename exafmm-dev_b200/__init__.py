@@ -52,6 +52,7 @@ SIGNATURES = {
     "fmm_b200_destroy": (_i, [_vp]),
     "fmm_b200_set_stream": (_i, [_vp, _vp]),
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
+    "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "fmm_b200_last_error": (C.c_char_p, [_vp]),
     "fmm_b200_supported_orders": (_i, [_i, _vp, _i]),
     "fmm_b200_solve_device": (_i, [_vp, _i, _vp, _vp]),
@@ -222,6 +223,18 @@ class Solver:
             raise FmmError(rc, self.lib.fmm_b200_last_error(self.h).decode())
 
     # ---- configuration
+    def autotune_ncrit(self, x, q, candidates=(16, 32, 48, 64, 96, 128), repeats=3):
+        """Time solves of these bodies at each ncrit; the fastest becomes the solver's ncrit.
+        Returns (best ncrit, {ncrit: median ms})."""
+        self.set_bodies(x, q)
+        cand = np.ascontiguousarray(candidates, np.int32)
+        times = np.zeros(len(cand))
+        best = C.c_int()
+        self._check(self.lib.fmm_b200_autotune_ncrit(self.h, _p(cand), len(cand), repeats,
+                                                      C.byref(best), _p(times)))
+        self.cfg.ncrit = best.value
+        return best.value, dict(zip(cand.tolist(), times.tolist()))
+
     def set_periodic(self, images, cycle):
         self._check(self.lib.fmm_b200_set_periodic(self.h, images, cycle))
 

@@ -189,6 +189,56 @@ template <typename T> void solve_all(Solver<T>& s) {
 
 }  // namespace
 
+// ncrit autotuner: each candidate solves the handle's current bodies `repeats` times after
+// one untimed solve (which sizes the buffers); the median device time decides.
+template <typename T>
+static int autotune_ncrit_t(Solver<T>& s, const int* cand, int ncand, int repeats,
+                            int* best, double* times_ms) {
+  if (s.stage < ST_BODIES) throw FmmError(FMM_ERR_STATE, "bodies not set");
+  const int keep = s.cfg.ncrit;
+  cudaEvent_t e0, e1;
+  FMM_CUDA(cudaEventCreate(&e0));
+  FMM_CUDA(cudaEventCreate(&e1));
+  double best_ms = 1e300;
+  int best_nc = keep;
+  try {
+    for (int i = 0; i < ncand; i++) {
+      s.cfg.ncrit = cand[i];
+      s.trav_sized = false;  // list sizes change with the tree
+      solve_all(s);
+      std::vector<float> ms;
+      for (int r = 0; r < repeats; r++) {
+        FMM_CUDA(cudaEventRecord(e0, s.stream));
+        solve_all(s);
+        FMM_CUDA(cudaEventRecord(e1, s.stream));
+        FMM_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        FMM_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        ms.push_back(t);
+      }
+      std::sort(ms.begin(), ms.end());
+      const double med = ms[ms.size() / 2];
+      if (times_ms) times_ms[i] = med;
+      if (med < best_ms) {
+        best_ms = med;
+        best_nc = cand[i];
+      }
+    }
+  } catch (...) {
+    s.cfg.ncrit = keep;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s.cfg.ncrit = best_nc;
+  s.trav_sized = false;
+  s.stage = ST_BODIES;
+  if (best) *best = best_nc;
+  return FMM_OK;
+}
+
 extern "C" {
 
 int fmm_b200_default_config(fmm_b200_config* c) {
@@ -376,6 +426,14 @@ int fmm_b200_build_tree(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_tree(
 int fmm_b200_upward_pass(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_up(s)); }
 int fmm_b200_traverse(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_trav(s)); }
 int fmm_b200_downward_pass(fmm_b200_solver* h) { return FMM_DISPATCH(h, stage_down(s)); }
+
+int fmm_b200_autotune_ncrit(fmm_b200_solver* h, const int* candidates, int ncand, int repeats,
+                            int* best_ncrit, double* times_ms) {
+  if (!h || !h->base || !candidates || ncand < 1 || repeats < 1) return FMM_ERR_INVALID;
+  for (int i = 0; i < ncand; i++)
+    if (candidates[i] < 1) return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, autotune_ncrit_t(s, candidates, ncand, repeats, best_ncrit, times_ms));
+}
 
 int fmm_b200_solve_device(fmm_b200_solver* h, int n, const void* d_bodies, void* d_trg) {
   if (n < 0 || (n > 0 && (!d_bodies || !d_trg))) return FMM_ERR_INVALID;

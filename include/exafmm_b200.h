@@ -155,6 +155,16 @@ int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2
 int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
 int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
 
+/* ---- autotuning ------------------------------------------------------------------------
+ * Picks ncrit (bodies per leaf, which sets the split between P2P and M2L work) for the
+ * bodies last given to the handle (fmm_b200_set_bodies_* or a solve): every candidate
+ * solves them `repeats` times after one untimed solve; the median device time of each goes
+ * to times_ms[i] (may be NULL) and the fastest becomes the handle's ncrit (*best_ncrit).
+ * Results depend on ncrit only through the tree (same method error).  No reference
+ * counterpart (the reference takes ncrit from the command line, include/args.h:98). */
+int fmm_b200_autotune_ncrit(fmm_b200_solver* s, const int* candidates, int ncand, int repeats,
+                            int* best_ncrit, double* times_ms);
+
 /* ---- serving: continuous batching of independent solves ------------------------------ *
  * A server owns nworkers worker threads (one CUDA stream and one solver handle per order
  * each) and a scheduler that batches pending requests of equal order P, in arrival order,

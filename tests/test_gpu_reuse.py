@@ -44,3 +44,14 @@ def test_growing_inputs_on_one_handle_match_fresh_handles(datasets):
         assert np.array_equal(np.isnan(got), np.isnan(ref))
         assert np.array_equal(got[ok], ref[ok]), n
         assert s.list_counts() == fresh.list_counts()
+
+
+def test_autotune_ncrit_picks_the_fastest_candidate(datasets):
+    x, q = datasets.make("plummer", 60000, seed=8, precision="f32")
+    s = fmm.Solver(P=8, theta=0.4, ncrit=64)
+    best, times = s.autotune_ncrit(x, q, candidates=(8, 64, 256), repeats=2)
+    assert best in (8, 64, 256) and all(t > 0 for t in times.values())
+    assert times[best] == min(times.values())
+    # the handle now solves with the tuned ncrit: bitwise a fresh handle at that ncrit
+    got = s.solve(x, q)
+    assert np.array_equal(got, fmm.Solver(P=8, theta=0.4, ncrit=best).solve(x, q))

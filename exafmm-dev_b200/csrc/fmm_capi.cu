@@ -239,6 +239,25 @@ static int autotune_ncrit_t(Solver<T>& s, const int* cand, int ncand, int repeat
   return FMM_OK;
 }
 
+// targets (segment 0) and sources (segment 1) as two trees on a common box
+template <typename T>
+static void solve_ij_t(fmm_b200_solver* h, Solver<T>& s, int nt, int ns) {
+  if (s.cfg.images != 0)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED, "separate target and source sets with periodic images");
+  const int counts[2] = {nt, ns};
+  int n = 0;
+  if (!set_segments(*h->base, 2, counts, &n)) throw FmmError(FMM_ERR_INVALID, "sizes");
+  s.ij = true;
+  s.trav_sized = false;  // the frontier holds one pair, not one per root
+  try {
+    solve_all(s);
+  } catch (...) {
+    s.ij = false;
+    throw;
+  }
+  s.ij = false;
+}
+
 extern "C" {
 
 int fmm_b200_default_config(fmm_b200_config* c) {
@@ -515,6 +534,52 @@ int fmm_b200_solve_batch_host(fmm_b200_solver* h, int nsolves, const int* counts
                                s.stream));
     }
     FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_solve_ij_host(fmm_b200_solver* h, int nt, const double* xt, const double* qt,
+                           int ns, const double* xs, const double* qs, double* p, double* f) {
+  if (!h || !h->base || nt < 0 || ns < 0) return FMM_ERR_INVALID;
+  if ((nt > 0 && (!xt || !qt || !p || !f)) || (ns > 0 && (!xs || !qs))) return FMM_ERR_INVALID;
+  if (nt == 0) return FMM_OK;
+  std::vector<double> x(3 * ((size_t)nt + ns)), q((size_t)nt + ns);
+  std::memcpy(x.data(), xt, sizeof(double) * 3 * nt);
+  std::memcpy(q.data(), qt, sizeof(double) * nt);
+  if (ns) {
+    std::memcpy(x.data() + 3 * (size_t)nt, xs, sizeof(double) * 3 * ns);
+    std::memcpy(q.data() + nt, qs, sizeof(double) * ns);
+  }
+  return FMM_DISPATCH(h, {
+    DevArr<double>& tmp = h->base->dtmp;
+    set_bodies_host_t(s, nt + ns, x.data(), q.data(), tmp);
+    solve_ij_t(h, s, nt, ns);
+    tmp.ensure(4 * (size_t)nt);
+    k_unpack_pf<T><<<ceil_div(nt, 256), 256, 0, s.stream>>>(nt, s.trg_out.p, tmp.p, tmp.p + nt);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaMemcpyAsync(p, tmp.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, s.stream));
+    FMM_CUDA(cudaMemcpyAsync(f, tmp.p + nt, 3 * sizeof(double) * nt, cudaMemcpyDeviceToHost,
+                             s.stream));
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int fmm_b200_solve_ij_device(fmm_b200_solver* h, int nt, const void* d_targets, int ns,
+                             const void* d_sources, void* d_trg) {
+  if (!h || !h->base || nt < 0 || ns < 0) return FMM_ERR_INVALID;
+  if ((nt > 0 && (!d_targets || !d_trg)) || (ns > 0 && !d_sources)) return FMM_ERR_INVALID;
+  if (nt == 0) return FMM_OK;
+  return FMM_DISPATCH(h, {
+    s.n = nt + ns;
+    s.bodies_in.ensure(std::max(s.n, 1));
+    FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p, d_targets, sizeof(s.bodies_in.p[0]) * nt,
+                             cudaMemcpyDeviceToDevice, s.stream));
+    if (ns)
+      FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p + nt, d_sources, sizeof(s.bodies_in.p[0]) * ns,
+                               cudaMemcpyDeviceToDevice, s.stream));
+    s.stage = ST_BODIES;
+    solve_ij_t(h, s, nt, ns);
+    FMM_CUDA(cudaMemcpyAsync(d_trg, s.trg_out.p, sizeof(s.trg_out.p[0]) * nt,
+                             cudaMemcpyDeviceToDevice, s.stream));
   });
 }
 

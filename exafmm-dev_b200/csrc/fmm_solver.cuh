@@ -86,6 +86,9 @@ struct SolverBase {
   DevArr<int> fs_idx;
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
+  // targets and sources in two trees (segments 0 and 1) on a common box, traversed from
+  // (target root, source root) only (fmm_b200_solve_ij_*)
+  bool ij = false;
   int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;

@@ -309,7 +309,11 @@ template <typename T> static void upload_roots(Solver<T>& s) {
   // one (root, root) pair per solve of the batch (lists never cross solves); with periodic
   // images one per shift of the source tree, in the reference's image order (:250-260)
   std::vector<int2> roots;
-  for (int r = 0; r < s.nroots; r++) {
+  if (s.ij) {
+    // dualTreeTraversal(cells, jcells): the target root against the source root
+    if (s.nroots == 2) roots.push_back(make_int2(s.root_cell[0], s.root_cell[1]));
+  }
+  for (int r = 0; r < s.nroots && !s.ij; r++) {
     if (s.cfg.images == 0) {
       roots.push_back(make_int2(s.root_cell[r], s.root_cell[r]));
       continue;

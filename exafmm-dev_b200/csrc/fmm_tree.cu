@@ -66,10 +66,12 @@ __global__ void k_minmax_chunks(const vec4<T>* __restrict__ b, const int* __rest
 // box[16 r ..] = X0[3], R0, Xmin[3], Xmax[3]
 template <typename T>
 __global__ void k_box(int nroots, const int* __restrict__ chunk_lo, const T* __restrict__ part,
-                      T* __restrict__ box) {
+                      int shared, T* __restrict__ box) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nroots) return;
-  const int c0 = chunk_lo[r], c1 = chunk_lo[r + 1];
+  // shared: every root takes the box of the bounds of all bodies (BoundBox::getBounds of
+  // the targets, then of the sources with those bounds, include/bound_box.h:91-97)
+  const int c0 = shared ? chunk_lo[0] : chunk_lo[r], c1 = shared ? chunk_lo[nroots] : chunk_lo[r + 1];
   T mn[3], mx[3];
   for (int d = 0; d < 3; d++) mn[d] = part[6 * c0 + d], mx[d] = part[6 * c0 + 3 + d];
   for (int k = c0 + 1; k < c1; k++)
@@ -519,7 +521,8 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.minmax_part.ensure(6 * (size_t)nch);
   k_minmax_chunks<T><<<nch, TB, 0, s.stream>>>(s.bodies_in.p, dcb, dce, s.minmax_part.p);
   FMM_LAUNCH_CHECK();
-  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, dlo, s.minmax_part.p, s.box.p);
+  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, dlo, s.minmax_part.p, s.ij ? 1 : 0,
+                                                      s.box.p);
   FMM_LAUNCH_CHECK();
   phase_end(s, FMM_PHASE_BOUNDS);
   phase_begin(s, FMM_PHASE_TREE);

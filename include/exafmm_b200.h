@@ -155,6 +155,19 @@ int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2
 int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
 int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
 
+/* ---- separate target and source sets ----------------------------------------------------
+ * examples/serial.cxx with IneJ (:30-55): targets (nt, with charges qt that shape their own
+ * tree's radii) and sources (ns) in two trees on the box of their common bounds, both
+ * upward passes, dualTreeTraversal(cells, jcells) from the target root against the source
+ * root, the targets' downward pass.  p, f (host) or d_trg (device 4-vectors) receive the
+ * targets' potential and gradient per unit target charge, in input order.  Open boundary
+ * only (images > 0: FMM_ERR_NOT_SUPPORTED).  Lists and cells of the last call are the two
+ * trees' (source cells after the target tree's, from the second root of fmm_b200_get_roots). */
+int fmm_b200_solve_ij_host(fmm_b200_solver* s, int nt, const double* xt, const double* qt,
+                           int ns, const double* xs, const double* qs, double* p, double* f);
+int fmm_b200_solve_ij_device(fmm_b200_solver* s, int nt, const void* d_targets, int ns,
+                             const void* d_sources, void* d_trg);
+
 /* ---- autotuning ------------------------------------------------------------------------
  * Picks ncrit (bodies per leaf, which sets the split between P2P and M2L work) for the
  * bodies last given to the handle (fmm_b200_set_bodies_* or a solve): every candidate

@@ -77,6 +77,7 @@ typedef struct {
   /* periodic shift of the source tree in the traversal under way, and its image code */
   real xp[3];
   int img;
+  int box_fixed; /* the box was set from the bounds of two body sets (oracle_solve_ij) */
   long long nm2l, np2p, capm2l, capp2p;
   /* cartesian index helpers */
   int* cidx;   /* [nx][ny][nz] -> term, size P^3 */
@@ -153,19 +154,26 @@ int oracle_real_bytes(void) { return (int)sizeof(real); }
 /* ------------------------------------------------------------------ bounds and box */
 /* BoundBox::getBounds (include/bound_box.h:76-88, BodiesRecursion :20-39) and
  * BuildTree::bounds2box (include/build_tree_tbb.h:298-310). */
+static void update_bounds(const Oracle* o, real* Xmin, real* Xmax) {
+  for (int i = 0; i < o->n; i++)
+    for (int d = 0; d < 3; d++) {
+      real v = o->x[3 * i + d];
+      Xmin[d] = v < Xmin[d] ? v : Xmin[d];
+      Xmax[d] = v > Xmax[d] ? v : Xmax[d];
+    }
+}
+static void bounds2box(Oracle* o, const real* Xmin, const real* Xmax);
 static void make_box(Oracle* o) {
   real Xmin[3], Xmax[3];
   if (o->n == 0) {
     for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = 0;
   } else {
     for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = o->x[d];
-    for (int i = 0; i < o->n; i++)
-      for (int d = 0; d < 3; d++) {
-        real v = o->x[3 * i + d];
-        Xmin[d] = v < Xmin[d] ? v : Xmin[d];
-        Xmax[d] = v > Xmax[d] ? v : Xmax[d];
-      }
+    update_bounds(o, Xmin, Xmax);
   }
+  bounds2box(o, Xmin, Xmax);
+}
+static void bounds2box(Oracle* o, const real* Xmin, const real* Xmax) {
   real R = 0;
   for (int d = 0; d < 3; d++) o->X0[d] = (Xmax[d] + Xmin[d]) / 2;
   for (int d = 0; d < 3; d++) {
@@ -285,7 +293,7 @@ static void nodes2cells(Oracle* o, int v, int c, int CN, int level, int iparent)
 /* BuildTree::buildTree (include/build_tree_tbb.h:365-374) = growTree (:313) + linkTree (:347) */
 int oracle_build_tree(void* h) {
   Oracle* o = (Oracle*)h;
-  make_box(o);
+  if (!o->box_fixed) make_box(o);
   o->nnodes = 0;
   o->maxlevel = 0;
   free_cells(o);
@@ -452,12 +460,12 @@ static void sph_m2m(Oracle* o, int ci) {
 }
 
 /* M2L spherical, non-mutual (kernels/LaplaceSphericalCPU.cxx:149-191) */
-static void sph_m2l(Oracle* o, int ci, int cj) {
+static void sph_m2l2(Oracle* o, int ci, Oracle* oj, int cj) {
   int P = o->p.P;
   cplx Ynmi[P * P];
-  cplx *Mi = CM(o, ci), *Mj = CM(o, cj), *Li = CL(o, ci);
+  cplx *Mi = CM(o, ci), *Mj = CM(oj, cj), *Li = CL(o, ci);
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - oj->cX[3 * cj + d] - o->xp[d];
   real rho, alpha, beta;
   cart2sph(&rho, &alpha, &beta, dX);
   eval_local(P, rho, alpha, beta, Ynmi);
@@ -489,6 +497,8 @@ static void sph_m2l(Oracle* o, int ci, int cj) {
     }
   }
 }
+
+static void sph_m2l(Oracle* o, int ci, int cj) { sph_m2l2(o, ci, o, cj); }
 
 /* L2L spherical (kernels/LaplaceSphericalCPU.cxx:193-224) */
 static void sph_l2l(Oracle* o, int ci) {
@@ -667,13 +677,13 @@ static void cart_m2m(Oracle* o, int ci) {
 
 /* M2L Cartesian, non-mutual (kernels/LaplaceCartesianCPU.cxx:658-673; sumM2L :442-451,
  * LocalSum :139-166): L_n += sum_{|n|+|k|<=P-1} M_k C_{n+k}. */
-static void cart_m2l(Oracle* o, int ci, int cj) {
+static void cart_m2l2(Oracle* o, int ci, Oracle* oj, int cj) {
   int P = o->p.P;
   real C[o->nterm];
-  real *Mi = &o->M[(size_t)ci * o->ncoef], *Mj = &o->M[(size_t)cj * o->ncoef];
+  real *Mi = &o->M[(size_t)ci * o->ncoef], *Mj = &oj->M[(size_t)cj * o->ncoef];
   real* Li = &o->L[(size_t)ci * o->ncoef];
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - oj->cX[3 * cj + d] - o->xp[d];
   real invR2 = 1 / (dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2]);
   real invR = o->p.mass ? Mi[0] * Mj[0] * sqrt(invR2) : sqrt(invR2);
   cart_coef(o, C, dX, invR2, invR);
@@ -698,6 +708,8 @@ static void cart_m2l(Oracle* o, int ci, int cj) {
     Li[t] += s;
   }
 }
+
+static void cart_m2l(Oracle* o, int ci, int cj) { cart_m2l2(o, ci, o, cj); }
 
 /* L2L Cartesian (kernels/LaplaceCartesianCPU.cxx:675-687) */
 static void cart_l2l(Oracle* o, int ci) {
@@ -760,17 +772,17 @@ static void cart_l2p(Oracle* o, int ci) {
 /* ------------------------------------------------------------------ P2P */
 /* P2P between cells, non-mutual (kernels/LaplaceP2PCPU.cxx:141-169, the scalar form of the
  * SIMD loop :10-139): TRG_i += q_i q_j / r, grad -= q_i q_j (x_i - x_j) / r^3. */
-static void p2p_pair(Oracle* o, int ci, int cj) {
+static void p2p_pair2(Oracle* o, int ci, Oracle* oj, int cj) {
   for (int i = o->cibody[ci]; i < o->cibody[ci] + o->cnbody[ci]; i++) {
     kreal pot = {0, 0}, ax = {0, 0}, ay = {0, 0}, az = {0, 0};
     real ppot = 0, pax = 0, pay = 0, paz = 0;
-    for (int j = o->cibody[cj]; j < o->cibody[cj] + o->cnbody[cj]; j++) {
+    for (int j = oj->cibody[cj]; j < oj->cibody[cj] + oj->cnbody[cj]; j++) {
       real dX[3];
-      for (int d = 0; d < 3; d++) dX[d] = o->x[3 * i + d] - o->x[3 * j + d] - o->xp[d];
+      for (int d = 0; d < 3; d++) dX[d] = o->x[3 * i + d] - oj->x[3 * j + d] - o->xp[d];
       real R2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2] + o->eps2;
       if (R2 != 0) {
         real invR2 = 1.0 / R2;
-        real invR = o->q[i] * o->q[j] * sqrt(invR2);
+        real invR = o->q[i] * oj->q[j] * sqrt(invR2);
         for (int d = 0; d < 3; d++) dX[d] *= invR2 * invR;
         if (o->p.kahan) {
           kadd(&pot, invR); kadd(&ax, dX[0]); kadd(&ay, dX[1]); kadd(&az, dX[2]);
@@ -788,6 +800,8 @@ static void p2p_pair(Oracle* o, int ci, int cj) {
     trg_add(o, i, 3, -paz);
   }
 }
+
+static void p2p_pair(Oracle* o, int ci, int cj) { p2p_pair2(o, ci, o, cj); }
 
 /* P2P within one cell (kernels/LaplaceP2PCPU.cxx:304-330): each unordered pair once,
  * updating both bodies. */
@@ -893,56 +907,57 @@ static void push_pair(long long** a, long long* n, long long* cap, int i, int j,
   (*a)[(*n)++] = ((long long)i << 32) | (long long)j | ((long long)img << 27);
 }
 
-static void traverse(Oracle* o, int ci, int cj);
+/* target tree o, source tree oj (the same tree except for oracle_solve_ij) */
+static void traverse(Oracle* o, int ci, Oracle* oj, int cj);
 
 /* TraverseRange::operator() for mutual = false (include/traversal.h:81-123) */
-static void traverse_range(Oracle* o, int ib, int ie, int jb, int je) {
+static void traverse_range(Oracle* o, int ib, int ie, Oracle* oj, int jb, int je) {
   if (ie - ib == 1 || je - jb == 1) {
-    if (ib == jb) {
-      traverse(o, ib, jb);
+    if (ib == jb && o == oj) {
+      traverse(o, ib, oj, jb);
     } else {
       for (int i = ib; i < ie; i++)
-        for (int j = jb; j < je; j++) traverse(o, i, j);
+        for (int j = jb; j < je; j++) traverse(o, i, oj, j);
     }
   } else {
     int im = ib + (ie - ib) / 2, jm = jb + (je - jb) / 2;
-    traverse_range(o, ib, im, jb, jm);
-    traverse_range(o, im, ie, jm, je);
-    traverse_range(o, ib, im, jm, je);
-    traverse_range(o, im, ie, jb, jm);
+    traverse_range(o, ib, im, oj, jb, jm);
+    traverse_range(o, im, ie, oj, jm, je);
+    traverse_range(o, ib, im, oj, jm, je);
+    traverse_range(o, im, ie, oj, jb, jm);
   }
 }
 
 /* splitCell (include/traversal.h:188-212) */
-static void split_cell(Oracle* o, int ci, int cj) {
-  if (o->nchild[cj] == 0) {
-    for (int c = o->ichild[ci]; c < o->ichild[ci] + o->nchild[ci]; c++) traverse(o, c, cj);
+static void split_cell(Oracle* o, int ci, Oracle* oj, int cj) {
+  if (oj->nchild[cj] == 0) {
+    for (int c = o->ichild[ci]; c < o->ichild[ci] + o->nchild[ci]; c++) traverse(o, c, oj, cj);
   } else if (o->nchild[ci] == 0) {
-    for (int c = o->ichild[cj]; c < o->ichild[cj] + o->nchild[cj]; c++) traverse(o, ci, c);
-  } else if (o->cnbody[ci] + o->cnbody[cj] >= o->p.nspawn) {
-    traverse_range(o, o->ichild[ci], o->ichild[ci] + o->nchild[ci], o->ichild[cj],
-                   o->ichild[cj] + o->nchild[cj]);
-  } else if (o->R[ci] >= o->R[cj]) {
-    for (int c = o->ichild[ci]; c < o->ichild[ci] + o->nchild[ci]; c++) traverse(o, c, cj);
+    for (int c = oj->ichild[cj]; c < oj->ichild[cj] + oj->nchild[cj]; c++) traverse(o, ci, oj, c);
+  } else if (o->cnbody[ci] + oj->cnbody[cj] >= o->p.nspawn) {
+    traverse_range(o, o->ichild[ci], o->ichild[ci] + o->nchild[ci], oj, oj->ichild[cj],
+                   oj->ichild[cj] + oj->nchild[cj]);
+  } else if (o->R[ci] >= oj->R[cj]) {
+    for (int c = o->ichild[ci]; c < o->ichild[ci] + o->nchild[ci]; c++) traverse(o, c, oj, cj);
   } else {
-    for (int c = o->ichild[cj]; c < o->ichild[cj] + o->nchild[cj]; c++) traverse(o, ci, c);
+    for (int c = oj->ichild[cj]; c < oj->ichild[cj] + oj->nchild[cj]; c++) traverse(o, ci, oj, c);
   }
 }
 
 /* Traversal::traverse (include/traversal.h:37-62), kernels applied as pairs are visited */
-static void traverse(Oracle* o, int ci, int cj) {
+static void traverse(Oracle* o, int ci, Oracle* oj, int cj) {
   real dX[3];
-  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - o->cX[3 * cj + d] - o->xp[d];
+  for (int d = 0; d < 3; d++) dX[d] = o->cX[3 * ci + d] - oj->cX[3 * cj + d] - o->xp[d];
   real R2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2];
-  real Rs = o->R[ci] + o->R[cj];
+  real Rs = o->R[ci] + oj->R[cj];
   if (R2 > Rs * Rs) {
     push_pair(&o->m2l, &o->nm2l, &o->capm2l, ci, cj, o->img);
-    if (o->p.basis == ORACLE_SPHERICAL) sph_m2l(o, ci, cj); else cart_m2l(o, ci, cj);
-  } else if (o->nchild[ci] == 0 && o->nchild[cj] == 0) {
+    if (o->p.basis == ORACLE_SPHERICAL) sph_m2l2(o, ci, oj, cj); else cart_m2l2(o, ci, oj, cj);
+  } else if (o->nchild[ci] == 0 && oj->nchild[cj] == 0) {
     push_pair(&o->p2p, &o->np2p, &o->capp2p, ci, cj, o->img);
-    if (R2 == 0 && ci == cj) p2p_self(o, ci); else p2p_pair(o, ci, cj);
+    if (R2 == 0 && ci == cj && o == oj) p2p_self(o, ci); else p2p_pair2(o, ci, oj, cj);
   } else {
-    split_cell(o, ci, cj);
+    split_cell(o, ci, oj, cj);
   }
 }
 
@@ -1005,7 +1020,7 @@ int oracle_traverse(void* h) {
   o->img = 0;
   if (o->nc == 0) return 0;
   if (o->p.images == 0) {
-    traverse(o, 0, 0);
+    traverse(o, 0, o, 0);
     return 0;
   }
   if (o->p.mass) return -1; /* the MASS normalisations of traversePeriodic are not restated */
@@ -1017,7 +1032,7 @@ int oracle_traverse(void* h) {
         o->xp[1] = (real)iy * cycle;
         o->xp[2] = (real)iz * cycle;
         o->img = 9 * img_digit(ix) + 3 * img_digit(iy) + img_digit(iz);
-        traverse(o, 0, 0);
+        traverse(o, 0, o, 0);
       }
   o->xp[0] = o->xp[1] = o->xp[2] = 0;
   o->img = 0;
@@ -1040,6 +1055,36 @@ int oracle_downward(void* h) {
     }
   }
   return 0;
+}
+
+/* examples/serial.cxx with IneJ (:30-55): targets hi and sources hj in two trees on the box of
+ * their common bounds (BoundBox::getBounds(jbodies, bounds), include/bound_box.h:91-97),
+ * both upward passes, dualTreeTraversal(cells, jcells) with mutual = false and no periodic
+ * images, and the targets' downward pass.  Returns 0 on success. */
+int oracle_solve_ij(void* hi, void* hj) {
+  Oracle *o = (Oracle*)hi, *oj = (Oracle*)hj;
+  if (o->p.images != 0) return -1;
+  real Xmin[3], Xmax[3];
+  if (o->n == 0) {
+    for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = 0;
+  } else {
+    for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = o->x[d];
+    update_bounds(o, Xmin, Xmax);
+  }
+  update_bounds(oj, Xmin, Xmax);
+  bounds2box(o, Xmin, Xmax);
+  bounds2box(oj, Xmin, Xmax);
+  o->box_fixed = oj->box_fixed = 1;
+  int r = oracle_build_tree(o);
+  if (!r) r = oracle_upward(o);
+  if (!r) r = oracle_build_tree(oj);
+  if (!r) r = oracle_upward(oj);
+  if (r) return r;
+  o->nm2l = o->np2p = 0;
+  o->xp[0] = o->xp[1] = o->xp[2] = 0;
+  o->img = 0;
+  if (o->nc > 0 && oj->nc > 0) traverse(o, 0, oj, 0);
+  return oracle_downward(o);
 }
 
 int oracle_solve(void* h) {

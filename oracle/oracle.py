@@ -119,6 +119,8 @@ class Oracle:
         L.oracle_direct.restype = None
         L.oracle_direct.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_void_p]
+        L.oracle_solve_ij.restype = C.c_int
+        L.oracle_solve_ij.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_direct_periodic.restype = None
         L.oracle_direct_periodic.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                              C.c_void_p, C.c_double, C.c_int, C.c_double,
@@ -154,6 +156,24 @@ class Oracle:
         out = np.zeros((len(xt), 4))
         self.lib.oracle_direct(len(xt), _ptr(xt), len(xs), _ptr(xs), _ptr(qs), eps2, _ptr(out))
         return out
+
+    def run_ij(self, xt, qt, xs, qs, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000,
+               use_rmax=1, use_ropt=0, mass=0, kahan=0, eps2=0.0):
+        """Targets and sources in two trees (oracle_solve_ij); the returned run holds the
+        targets' tree, lists (source cells of the source tree) and results."""
+        xt = np.ascontiguousarray(xt, np.float64)
+        qt = np.ascontiguousarray(qt, np.float64)
+        xs = np.ascontiguousarray(xs, np.float64)
+        qs = np.ascontiguousarray(qs, np.float64)
+        prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2, 0,
+                      2 * np.pi)
+        hi = self.lib.oracle_new(len(qt), _ptr(xt), _ptr(qt), C.byref(prm))
+        hj = self.lib.oracle_new(len(qs), _ptr(xs), _ptr(qs), C.byref(prm))
+        nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
+        run = OracleRun(self.lib, "oracle_", hi, len(qt), nterm, basis == SPHERICAL)
+        run._jsrc = OracleRun(self.lib, "oracle_", hj, len(qs), nterm, basis == SPHERICAL)
+        assert self.lib.oracle_solve_ij(hi, hj) == 0
+        return run
 
     def direct_periodic(self, xt, xs, qs, images, cycle, eps2=0.0):
         """FP64 direct sum over the periodic images Traversal::direct visits."""
@@ -223,6 +243,10 @@ class Reference:
             for f in ("P", "nterm", "fp64", "spherical", "mass", "kahan"):
                 getattr(lib, "ref_" + f).restype = C.c_int
                 getattr(lib, "ref_" + f).argtypes = []
+            lib.ref_run_ij.restype = C.c_void_p
+            lib.ref_run_ij.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                       C.c_int, C.c_double]
             lib.ref_num_m2l.restype = C.c_longlong
             lib.ref_num_p2p.restype = C.c_longlong
             lib.ref_get_m2l.argtypes = [C.c_void_p]
@@ -250,6 +274,23 @@ class Reference:
             run._p2p = np.zeros(self.lib.ref_num_p2p(), np.int64)
             self.lib.ref_get_m2l(_ptr(run._m2l))
             self.lib.ref_get_p2p(_ptr(run._p2p))
+        return run
+
+    def run_ij(self, xt, qt, xs, qs, ncrit=64, nspawn=1000, theta=0.4, use_rmax=1, use_ropt=0,
+               eps2=0.0):
+        """Targets and sources in two trees (examples/serial.cxx IneJ); the run's getters
+        read the targets."""
+        xt = np.ascontiguousarray(xt, np.float64)
+        qt = np.ascontiguousarray(qt, np.float64)
+        xs = np.ascontiguousarray(xs, np.float64)
+        qs = np.ascontiguousarray(qs, np.float64)
+        h = self.lib.ref_run_ij(len(qt), _ptr(xt), _ptr(qt), len(qs), _ptr(xs), _ptr(qs), ncrit,
+                                nspawn, theta, use_rmax, use_ropt, eps2)
+        run = RefRun(self.lib, "ref_", h, len(qt), self.nterm, self.spherical)
+        run._m2l = np.zeros(self.lib.ref_num_m2l(), np.int64)
+        run._p2p = np.zeros(self.lib.ref_num_p2p(), np.int64)
+        self.lib.ref_get_m2l(_ptr(run._m2l))
+        self.lib.ref_get_p2p(_ptr(run._p2p))
         return run
 
     def kernel_chain(self, seed=-1):

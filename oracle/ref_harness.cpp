@@ -29,8 +29,8 @@ extern std::vector<long long> m2l, p2p;
 }
 
 struct RefRun {
-  Bodies bodies, buffer;
-  Cells cells;
+  Bodies bodies, buffer, jbodies;
+  Cells cells, jcells;
   std::vector<int> level;
   std::vector<double> R_built;  // cell radius straight out of buildTree
   double t[8];                  // bounds, tree, upward, traverse, downward, total
@@ -137,6 +137,67 @@ void* ref_run(int n, const double* x, const double* q, int ncrit, int nspawn, do
   }
   refrec::enabled = false;
   // cell levels from the parent links (root is cell 0)
+  int nc = run->cells.size();
+  run->level.assign(nc, 0);
+  run->maxlevel = 0;
+  for (int c = 0; c < nc; c++) {
+    const Cell& C = run->cells[c];
+    for (int k = 0; k < C.NCHILD; k++) {
+      run->level[C.ICHILD + k] = run->level[c] + 1;
+      if (run->level[c] + 1 > run->maxlevel) run->maxlevel = run->level[c] + 1;
+    }
+  }
+  return run;
+}
+
+// examples/serial.cxx with IneJ (:30-55): targets and sources in two trees on the box of
+// their common bounds, both upward passes, dualTreeTraversal(cells, jcells, cycle, false),
+// the targets' downward pass (serial; lists recorded).  The getters read the targets.
+void* ref_run_ij(int nt, const double* xt, const double* qt, int ns, const double* xs,
+                 const double* qs, int ncrit, int nspawn, double theta, int useRmax,
+                 int useRopt, double eps2) {
+  RefRun* run = new RefRun();
+  auto fill = [](Bodies& b, int n, const double* x, const double* q) {
+    b.resize(n);
+    for (int i = 0; i < n; i++) {
+      Body& B = b[i];
+      B.X[0] = x[3 * i + 0];
+      B.X[1] = x[3 * i + 1];
+      B.X[2] = x[3 * i + 2];
+      B.SRC = q[i];
+      B.TRG = 0;
+      B.IBODY = i;
+      B.IRANK = 0;
+      B.ICELL = 0;
+      B.WEIGHT = 1;
+    }
+  };
+  fill(run->bodies, nt, xt, qt);
+  fill(run->jbodies, ns, xs, qs);
+  run->buffer.reserve(nt > ns ? nt : ns);
+  logger::verbose = false;
+  BoundBox boundBox(nspawn);
+  BuildTree buildTree(ncrit, nspawn);
+  UpDownPass upDownPass(theta, useRmax, useRopt);
+  Traversal traversal(nspawn, 0, eps2);
+  for (int k = 0; k < 8; k++) run->t[k] = 0;
+  refrec::m2l.clear();
+  refrec::p2p.clear();
+  Bounds bounds = boundBox.getBounds(run->bodies);
+  bounds = boundBox.getBounds(run->jbodies, bounds);
+  run->cells = buildTree.buildTree(run->bodies, run->buffer, bounds);
+  run->R_built.resize(run->cells.size());
+  for (size_t c = 0; c < run->cells.size(); c++) run->R_built[c] = run->cells[c].R;
+  upDownPass.upwardPass(run->cells);
+  run->jcells = buildTree.buildTree(run->jbodies, run->buffer, bounds);
+  upDownPass.upwardPass(run->jcells);
+  refrec::enabled = true;
+  refrec::Ci0 = run->cells.begin();
+  refrec::Cj0 = run->jcells.begin();
+  refrec::ncells = run->jcells.size();
+  traversal.dualTreeTraversal(run->cells, run->jcells, 2 * M_PI, false);
+  refrec::enabled = false;
+  upDownPass.downwardPass(run->cells);
   int nc = run->cells.size();
   run->level.assign(nc, 0);
   run->maxlevel = 0;

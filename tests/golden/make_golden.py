@@ -9,7 +9,8 @@ Runs the reference compiled from its own sources (oracle/_ref/parity/*.so, built
   potential + gradient per body, for each case in CASES.
 
 Usage (needs the reference build): python tests/golden/make_golden.py [case ...]
-(no case names: the kernel chain and every case)
+(no case names: the kernel chain and every case; ``<case>.npz`` of an IneJ case holds the
+targets xt, qt, the sources xs, qs, the sorted lists and the targets' potential + gradient)
 """
 import importlib
 import json
@@ -39,6 +40,13 @@ CASES = {
                             dict(ncrit=32, theta=0.4, use_ropt=0, images=3, cycle=2.0)),
 }
 
+# separate target and source sets (examples/serial.cxx IneJ): targets from a cube moved to
+# x in [0, 1], sources from a Plummer sphere moved to x in [-1, 0]
+IJ_CASES = {
+    "sph_p8_f32k_ij": ("sph_p8_f32k_mass", "f32", 3000, 5000,
+                       dict(ncrit=32, theta=0.4, use_ropt=1)),
+}
+
 CHAIN = [("sph_p4_f64", "spherical", 4), ("sph_p6_f64", "spherical", 6),
          ("sph_p8_f64", "spherical", 8), ("sph_p10_f64", "spherical", 10),
          ("cart_p4_f64", "cartesian", 4), ("cart_p5_f64", "cartesian", 5),
@@ -66,5 +74,39 @@ def main(names):
         print(name, run.num_cells, "cells", len(run.m2l()), "M2L", len(run.p2p()), "P2P")
 
 
+def ij_bodies(nt, ns, precision):
+    xt, qt = datasets.make("cube", nt, seed=1, precision=precision)
+    xs, qs = datasets.make("plummer", ns, seed=2, precision=precision)
+    xt = xt.copy()
+    xs = xs.copy()
+    xt[:, 0] = (xt[:, 0] + 1) * 0.5
+    xs[:, 0] = (xs[:, 0] - 1) * 0.5
+    if precision == "f32":
+        xt = xt.astype(np.float32).astype(np.float64)
+        xs = xs.astype(np.float32).astype(np.float64)
+    return xt, qt, xs, qs
+
+
+def main_ij(names):
+    for name, (cfg, prec, nt, ns, kw) in IJ_CASES.items():
+        if names and name not in names:
+            continue
+        xt, qt, xs, qs = ij_bodies(nt, ns, prec)
+        run = Reference(cfg).run_ij(xt, qt, xs, qs, **kw)
+        np.savez_compressed(
+            os.path.join(HERE, name + ".npz"), xt=xt, qt=qt, xs=xs, qs=qs,
+            m2l=np.sort(run.m2l()), p2p=np.sort(run.p2p()), trg=run.trg(),
+            params=json.dumps(dict(config=cfg, precision=prec, nt=nt, ns=ns, **kw)))
+        print(name, len(run.m2l()), "M2L", len(run.p2p()), "P2P")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1:])
+    names = sys.argv[1:]
+    if not names:
+        main([])
+        main_ij([])
+    else:
+        if any(a in CASES for a in names):
+            main([a for a in names if a in CASES])
+        if any(a in IJ_CASES for a in names):
+            main_ij([a for a in names if a in IJ_CASES])

@@ -157,3 +157,41 @@ def test_periodic_direct_sum():
                 ref += o.direct(xt - 2.0 * np.array([ix, iy, iz]), xs, qs)
     assert np.allclose(got, ref, rtol=1e-12, atol=1e-12)
     assert np.allclose(o.direct_periodic(xt, xs, qs, 0, 2.0), o.direct(xt, xs, qs), rtol=1e-14)
+
+
+def _ij_run(prec, g, kw, P, mass, kahan, basis=SPHERICAL):
+    return Oracle(prec).run_ij(g["xt"], g["qt"], g["xs"], g["qs"], basis=basis, P=P, mass=mass,
+                               kahan=kahan, **kw)
+
+
+def test_oracle_ij_matches_golden(golden_dir):
+    """Separate target and source trees (examples/serial.cxx IneJ) against the reference's
+    recorded lists and potentials."""
+    g = np.load(os.path.join(golden_dir, "sph_p8_f32k_ij.npz"))
+    p = json.loads(str(g["params"]))
+    basis, P, mass, kahan = _params(p)
+    kw = dict(ncrit=p["ncrit"], theta=p["theta"], use_ropt=p["use_ropt"])
+    o = _ij_run(p["precision"], g, kw, P, mass, kahan, basis)
+    assert np.array_equal(np.sort(o.m2l()), g["m2l"])
+    assert np.array_equal(np.sort(o.p2p()), g["p2p"])
+    pot, acc = rel_l2(o.trg(), g["trg"])
+    assert pot < 2e-6 and acc < 2e-6, (pot, acc)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) absent")
+@pytest.mark.parametrize("cfg,prec", [("sph_p6_f64", "f64"), ("cart_p5_f32", "f32"),
+                                      ("sph_p10_f32k_mass", "f32")])
+def test_oracle_ij_matches_reference(cfg, prec, datasets):
+    R = Reference(cfg)
+    xt, qt = datasets.make("cube", 2500, seed=3, precision=prec)
+    xs, qs = datasets.make("sphere", 3500, seed=4, precision=prec)
+    xt = xt * 0.5 + 0.25
+    kw = dict(ncrit=32, theta=0.4, use_ropt=0)
+    r = R.run_ij(xt, qt, xs, qs, **kw)
+    o = Oracle(prec).run_ij(xt, qt, xs, qs, basis=SPHERICAL if R.spherical else CARTESIAN,
+                            P=R.P, mass=int(R.mass), kahan=int(R.kahan), **kw)
+    assert np.array_equal(r.m2l(), o.m2l())  # visiting order too
+    assert np.array_equal(r.p2p(), o.p2p())
+    pot, acc = rel_l2(o.trg(), r.trg())
+    tol = 2e-6 if prec == "f32" else 5e-7
+    assert pot < tol and acc < tol, (pot, acc)

@@ -53,8 +53,8 @@ SIGNATURES = {
     "fmm_b200_set_stream": (_i, [_vp, _vp]),
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
     "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
-    "fmm_b200_solve_ij_host": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
-    "fmm_b200_solve_ij_device": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
+    "fmm_b200_solve_ij_host": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "fmm_b200_solve_ij_device": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp]),
     "fmm_b200_last_error": (C.c_char_p, [_vp]),
     "fmm_b200_supported_orders": (_i, [_i, _vp, _i]),
     "fmm_b200_solve_device": (_i, [_vp, _i, _vp, _vp]),
@@ -285,9 +285,10 @@ class Solver:
         self.n = n
         return np.concatenate([p[:, None], f], axis=1)
 
-    def solve_ij(self, xt, qt, xs, qs):
-        """Targets (xt, qt) against sources (xs, qs) in two trees (examples/serial.cxx IneJ):
-        (nt, 4) potential and gradient per unit target charge."""
+    def solve_ij(self, xt, qt, xs, qs, common_box=True):
+        """Targets (xt, qt) against sources (xs, qs) in two trees (examples/serial.cxx IneJ
+        with common_box, the petiga wrapper's trees without): (nt, 4) potential and
+        gradient per unit target charge."""
         xt = np.ascontiguousarray(xt, np.float64).reshape(-1, 3)
         qt = np.ascontiguousarray(qt, np.float64).reshape(-1)
         xs = np.ascontiguousarray(xs, np.float64).reshape(-1, 3)
@@ -295,7 +296,8 @@ class Solver:
         p = np.zeros(len(qt))
         f = np.zeros((len(qt), 3))
         self._check(self.lib.fmm_b200_solve_ij_host(self.h, len(qt), _p(xt), _p(qt), len(qs),
-                                                     _p(xs), _p(qs), _p(p), _p(f)))
+                                                     _p(xs), _p(qs), int(common_box), _p(p),
+                                                     _p(f)))
         self.n = len(qt) + len(qs)
         return np.concatenate([p[:, None], f], axis=1)
 

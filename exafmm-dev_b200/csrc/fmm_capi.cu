@@ -241,13 +241,14 @@ static int autotune_ncrit_t(Solver<T>& s, const int* cand, int ncand, int repeat
 
 // targets (segment 0) and sources (segment 1) as two trees on a common box
 template <typename T>
-static void solve_ij_t(fmm_b200_solver* h, Solver<T>& s, int nt, int ns) {
+static void solve_ij_t(fmm_b200_solver* h, Solver<T>& s, int nt, int ns, int common_box) {
   if (s.cfg.images != 0)
     throw FmmError(FMM_ERR_NOT_SUPPORTED, "separate target and source sets with periodic images");
   const int counts[2] = {nt, ns};
   int n = 0;
   if (!set_segments(*h->base, 2, counts, &n)) throw FmmError(FMM_ERR_INVALID, "sizes");
   s.ij = true;
+  s.ij_common_box = common_box != 0;
   s.trav_sized = false;  // the frontier holds one pair, not one per root
   try {
     solve_all(s);
@@ -538,7 +539,8 @@ int fmm_b200_solve_batch_host(fmm_b200_solver* h, int nsolves, const int* counts
 }
 
 int fmm_b200_solve_ij_host(fmm_b200_solver* h, int nt, const double* xt, const double* qt,
-                           int ns, const double* xs, const double* qs, double* p, double* f) {
+                           int ns, const double* xs, const double* qs, int common_box, double* p,
+                           double* f) {
   if (!h || !h->base || nt < 0 || ns < 0) return FMM_ERR_INVALID;
   if ((nt > 0 && (!xt || !qt || !p || !f)) || (ns > 0 && (!xs || !qs))) return FMM_ERR_INVALID;
   if (nt == 0) return FMM_OK;
@@ -552,7 +554,7 @@ int fmm_b200_solve_ij_host(fmm_b200_solver* h, int nt, const double* xt, const d
   return FMM_DISPATCH(h, {
     DevArr<double>& tmp = h->base->dtmp;
     set_bodies_host_t(s, nt + ns, x.data(), q.data(), tmp);
-    solve_ij_t(h, s, nt, ns);
+    solve_ij_t(h, s, nt, ns, common_box);
     tmp.ensure(4 * (size_t)nt);
     k_unpack_pf<T><<<ceil_div(nt, 256), 256, 0, s.stream>>>(nt, s.trg_out.p, tmp.p, tmp.p + nt);
     FMM_LAUNCH_CHECK();
@@ -564,7 +566,7 @@ int fmm_b200_solve_ij_host(fmm_b200_solver* h, int nt, const double* xt, const d
 }
 
 int fmm_b200_solve_ij_device(fmm_b200_solver* h, int nt, const void* d_targets, int ns,
-                             const void* d_sources, void* d_trg) {
+                             const void* d_sources, int common_box, void* d_trg) {
   if (!h || !h->base || nt < 0 || ns < 0) return FMM_ERR_INVALID;
   if ((nt > 0 && (!d_targets || !d_trg)) || (ns > 0 && !d_sources)) return FMM_ERR_INVALID;
   if (nt == 0) return FMM_OK;
@@ -577,7 +579,7 @@ int fmm_b200_solve_ij_device(fmm_b200_solver* h, int nt, const void* d_targets, 
       FMM_CUDA(cudaMemcpyAsync(s.bodies_in.p + nt, d_sources, sizeof(s.bodies_in.p[0]) * ns,
                                cudaMemcpyDeviceToDevice, s.stream));
     s.stage = ST_BODIES;
-    solve_ij_t(h, s, nt, ns);
+    solve_ij_t(h, s, nt, ns, common_box);
     FMM_CUDA(cudaMemcpyAsync(d_trg, s.trg_out.p, sizeof(s.trg_out.p[0]) * nt,
                              cudaMemcpyDeviceToDevice, s.stream));
   });

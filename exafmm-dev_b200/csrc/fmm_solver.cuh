@@ -89,6 +89,7 @@ struct SolverBase {
   // targets and sources in two trees (segments 0 and 1) on a common box, traversed from
   // (target root, source root) only (fmm_b200_solve_ij_*)
   bool ij = false;
+  bool ij_common_box = true;  // else each tree on its own bodies' box (the petiga wrapper)
   int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;

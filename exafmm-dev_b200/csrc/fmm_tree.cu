@@ -521,8 +521,8 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.minmax_part.ensure(6 * (size_t)nch);
   k_minmax_chunks<T><<<nch, TB, 0, s.stream>>>(s.bodies_in.p, dcb, dce, s.minmax_part.p);
   FMM_LAUNCH_CHECK();
-  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, dlo, s.minmax_part.p, s.ij ? 1 : 0,
-                                                      s.box.p);
+  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(
+      nroots, dlo, s.minmax_part.p, s.ij && s.ij_common_box ? 1 : 0, s.box.p);
   FMM_LAUNCH_CHECK();
   phase_end(s, FMM_PHASE_BOUNDS);
   phase_begin(s, FMM_PHASE_TREE);

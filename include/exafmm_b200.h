@@ -156,17 +156,20 @@ int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
 int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
 
 /* ---- separate target and source sets ----------------------------------------------------
- * examples/serial.cxx with IneJ (:30-55): targets (nt, with charges qt that shape their own
- * tree's radii) and sources (ns) in two trees on the box of their common bounds, both
- * upward passes, dualTreeTraversal(cells, jcells) from the target root against the source
- * root, the targets' downward pass.  p, f (host) or d_trg (device 4-vectors) receive the
- * targets' potential and gradient per unit target charge, in input order.  Open boundary
- * only (images > 0: FMM_ERR_NOT_SUPPORTED).  Lists and cells of the last call are the two
- * trees' (source cells after the target tree's, from the second root of fmm_b200_get_roots). */
+ * Targets (nt, with charges qt that shape their own tree's radii) and sources (ns) in two
+ * trees, both upward passes, dualTreeTraversal(cells, jcells) from the target root against
+ * the source root, the targets' downward pass.  common_box = 1: both trees on the box of
+ * the two sets' common bounds (examples/serial.cxx with IneJ, :30-55); 0: each tree on its
+ * own bodies' box (wrappers/petiga.cxx:134-139).  p, f (host) or d_trg (device 4-vectors)
+ * receive the targets' potential and gradient per unit target charge, in input order.
+ * Open boundary only (images > 0: FMM_ERR_NOT_SUPPORTED).  Lists and cells of the last call
+ * are the two trees' (source cells after the target tree's, from the second root of
+ * fmm_b200_get_roots). */
 int fmm_b200_solve_ij_host(fmm_b200_solver* s, int nt, const double* xt, const double* qt,
-                           int ns, const double* xs, const double* qs, double* p, double* f);
+                           int ns, const double* xs, const double* qs, int common_box, double* p,
+                           double* f);
 int fmm_b200_solve_ij_device(fmm_b200_solver* s, int nt, const void* d_targets, int ns,
-                             const void* d_sources, void* d_trg);
+                             const void* d_sources, int common_box, void* d_trg);
 
 /* ---- autotuning ------------------------------------------------------------------------
  * Picks ncrit (bodies per leaf, which sets the split between P2P and M2L work) for the
@@ -241,10 +244,13 @@ int fmm_b200_fp32_peak(int device, double* tflops);
 long long fmm_b200_kernel_launches(void);
 
 /* ---- reference wrapper ABI (single GPU, single rank) ----------------------------------
+ * (Left out when EXAFMM_B200_NO_GROMACS_ABI is defined: the PetIGA wrapper library,
+ * include/exafmm_b200_petiga.h, reuses the names FMM_Init / FMM_Partition / FMM_Finalize.)
  * FMM_Init: the gromacs wrapper's fixed parameters (ncrit 32, nspawn 1000, theta 0.4,
  * use_rmax, use_ropt, eps2 0, wrappers/gromacs.cxx:28-56) on the spherical basis at
  * EXAFMM_B200_P (default 10) in FP32, with `images` periodic image levels of the box of
  * side `cycle` that each FMM_Coulomb call passes. */
+#ifndef EXAFMM_B200_NO_GROMACS_ABI
 void FMM_Init(int images);
 void FMM_Finalize(void);
 #ifdef __cplusplus
@@ -253,6 +259,7 @@ void FMM_Partition(int& n, int* index, double* x, double* q, double cycle);
 void FMM_Partition(int* n, int* index, double* x, double* q, double cycle);
 #endif
 void FMM_Coulomb(int n, double* x, double* q, double* p, double* f, double cycle);
+#endif
 
 /* Fortran ABI of the CHARMM wrapper (wrappers/charmm.cxx:31-202), single rank: bodies
  * with icpumap[i] == 1 are solved and p, f accumulate TRG * q * 332.0716. */

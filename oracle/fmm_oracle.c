@@ -1057,24 +1057,27 @@ int oracle_downward(void* h) {
   return 0;
 }
 
-/* examples/serial.cxx with IneJ (:30-55): targets hi and sources hj in two trees on the box of
- * their common bounds (BoundBox::getBounds(jbodies, bounds), include/bound_box.h:91-97),
+/* examples/serial.cxx with IneJ (:30-55): targets hi and sources hj in two trees, on the box
+ * of their common bounds (common_box; BoundBox::getBounds(jbodies, bounds),
+ * include/bound_box.h:91-97) or each on its own bodies' box (wrappers/petiga.cxx:134-139),
  * both upward passes, dualTreeTraversal(cells, jcells) with mutual = false and no periodic
  * images, and the targets' downward pass.  Returns 0 on success. */
-int oracle_solve_ij(void* hi, void* hj) {
+int oracle_solve_ij(void* hi, void* hj, int common_box) {
   Oracle *o = (Oracle*)hi, *oj = (Oracle*)hj;
   if (o->p.images != 0) return -1;
-  real Xmin[3], Xmax[3];
-  if (o->n == 0) {
-    for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = 0;
-  } else {
-    for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = o->x[d];
-    update_bounds(o, Xmin, Xmax);
+  if (common_box) {
+    real Xmin[3], Xmax[3];
+    if (o->n == 0) {
+      for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = 0;
+    } else {
+      for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = o->x[d];
+      update_bounds(o, Xmin, Xmax);
+    }
+    update_bounds(oj, Xmin, Xmax);
+    bounds2box(o, Xmin, Xmax);
+    bounds2box(oj, Xmin, Xmax);
   }
-  update_bounds(oj, Xmin, Xmax);
-  bounds2box(o, Xmin, Xmax);
-  bounds2box(oj, Xmin, Xmax);
-  o->box_fixed = oj->box_fixed = 1;
+  o->box_fixed = oj->box_fixed = common_box != 0;
   int r = oracle_build_tree(o);
   if (!r) r = oracle_upward(o);
   if (!r) r = oracle_build_tree(oj);

@@ -46,9 +46,10 @@ int oracle_upward(void* h);
 int oracle_traverse(void* h); /* also applies M2L/P2P as the traversal visits pairs */
 int oracle_downward(void* h);
 int oracle_solve(void* h);    /* all of the above */
-/* targets (hi) and sources (hj) in two trees (examples/serial.cxx IneJ): common box,
- * both upward passes, dualTreeTraversal(cells, jcells), the targets' downward pass */
-int oracle_solve_ij(void* hi, void* hj);
+/* targets (hi) and sources (hj) in two trees (examples/serial.cxx IneJ with common_box = 1;
+ * the petiga wrapper's trees on their own boxes with 0): both upward passes,
+ * dualTreeTraversal(cells, jcells), the targets' downward pass */
+int oracle_solve_ij(void* hi, void* hj, int common_box);
 
 int oracle_num_cells(void* h);
 int oracle_maxlevel(void* h);

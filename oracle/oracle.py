@@ -120,7 +120,7 @@ class Oracle:
         L.oracle_direct.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_void_p]
         L.oracle_solve_ij.restype = C.c_int
-        L.oracle_solve_ij.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_solve_ij.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.oracle_direct_periodic.restype = None
         L.oracle_direct_periodic.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                              C.c_void_p, C.c_double, C.c_int, C.c_double,
@@ -158,7 +158,7 @@ class Oracle:
         return out
 
     def run_ij(self, xt, qt, xs, qs, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000,
-               use_rmax=1, use_ropt=0, mass=0, kahan=0, eps2=0.0):
+               use_rmax=1, use_ropt=0, mass=0, kahan=0, eps2=0.0, common_box=1):
         """Targets and sources in two trees (oracle_solve_ij); the returned run holds the
         targets' tree, lists (source cells of the source tree) and results."""
         xt = np.ascontiguousarray(xt, np.float64)
@@ -172,7 +172,7 @@ class Oracle:
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
         run = OracleRun(self.lib, "oracle_", hi, len(qt), nterm, basis == SPHERICAL)
         run._jsrc = OracleRun(self.lib, "oracle_", hj, len(qs), nterm, basis == SPHERICAL)
-        assert self.lib.oracle_solve_ij(hi, hj) == 0
+        assert self.lib.oracle_solve_ij(hi, hj, common_box) == 0
         return run
 
     def direct_periodic(self, xt, xs, qs, images, cycle, eps2=0.0):
@@ -246,7 +246,7 @@ class Reference:
             lib.ref_run_ij.restype = C.c_void_p
             lib.ref_run_ij.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                        C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
-                                       C.c_int, C.c_double]
+                                       C.c_int, C.c_double, C.c_int]
             lib.ref_num_m2l.restype = C.c_longlong
             lib.ref_num_p2p.restype = C.c_longlong
             lib.ref_get_m2l.argtypes = [C.c_void_p]
@@ -277,7 +277,7 @@ class Reference:
         return run
 
     def run_ij(self, xt, qt, xs, qs, ncrit=64, nspawn=1000, theta=0.4, use_rmax=1, use_ropt=0,
-               eps2=0.0):
+               eps2=0.0, common_box=1):
         """Targets and sources in two trees (examples/serial.cxx IneJ); the run's getters
         read the targets."""
         xt = np.ascontiguousarray(xt, np.float64)
@@ -285,7 +285,7 @@ class Reference:
         xs = np.ascontiguousarray(xs, np.float64)
         qs = np.ascontiguousarray(qs, np.float64)
         h = self.lib.ref_run_ij(len(qt), _ptr(xt), _ptr(qt), len(qs), _ptr(xs), _ptr(qs), ncrit,
-                                nspawn, theta, use_rmax, use_ropt, eps2)
+                                nspawn, theta, use_rmax, use_ropt, eps2, common_box)
         run = RefRun(self.lib, "ref_", h, len(qt), self.nterm, self.spherical)
         run._m2l = np.zeros(self.lib.ref_num_m2l(), np.int64)
         run._p2p = np.zeros(self.lib.ref_num_p2p(), np.int64)

@@ -150,12 +150,12 @@ void* ref_run(int n, const double* x, const double* q, int ncrit, int nspawn, do
   return run;
 }
 
-// examples/serial.cxx with IneJ (:30-55): targets and sources in two trees on the box of
-// their common bounds, both upward passes, dualTreeTraversal(cells, jcells, cycle, false),
+// examples/serial.cxx with IneJ (:30-55): targets and sources in two trees (common_box:
+// on the box of their common bounds), both upward passes, dualTreeTraversal(cells, jcells, cycle, false),
 // the targets' downward pass (serial; lists recorded).  The getters read the targets.
 void* ref_run_ij(int nt, const double* xt, const double* qt, int ns, const double* xs,
                  const double* qs, int ncrit, int nspawn, double theta, int useRmax,
-                 int useRopt, double eps2) {
+                 int useRopt, double eps2, int common_box) {
   RefRun* run = new RefRun();
   auto fill = [](Bodies& b, int n, const double* x, const double* q) {
     b.resize(n);
@@ -183,13 +183,16 @@ void* ref_run_ij(int nt, const double* xt, const double* qt, int ns, const doubl
   for (int k = 0; k < 8; k++) run->t[k] = 0;
   refrec::m2l.clear();
   refrec::p2p.clear();
+  // common_box: examples/serial.cxx IneJ; else each tree on its own bounds, as the petiga
+  // wrapper builds them (wrappers/petiga.cxx:134-139)
   Bounds bounds = boundBox.getBounds(run->bodies);
-  bounds = boundBox.getBounds(run->jbodies, bounds);
+  Bounds jbounds = boundBox.getBounds(run->jbodies);
+  if (common_box) jbounds = bounds = boundBox.getBounds(run->jbodies, bounds);
   run->cells = buildTree.buildTree(run->bodies, run->buffer, bounds);
   run->R_built.resize(run->cells.size());
   for (size_t c = 0; c < run->cells.size(); c++) run->R_built[c] = run->cells[c].R;
   upDownPass.upwardPass(run->cells);
-  run->jcells = buildTree.buildTree(run->jbodies, run->buffer, bounds);
+  run->jcells = buildTree.buildTree(run->jbodies, run->buffer, jbounds);
   upDownPass.upwardPass(run->jcells);
   refrec::enabled = true;
   refrec::Ci0 = run->cells.begin();

@@ -12,8 +12,8 @@ fmm = importlib.import_module("exafmm-dev_b200")
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def header_functions():
-    src = open(os.path.join(ROOT, "include", "exafmm_b200.h")).read()
+def header_functions(header="exafmm_b200.h"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = set(re.findall(r"^\s*(?:const\s+)?(?:(?:unsigned|long)\s+)*[A-Za-z_][A-Za-z0-9_]*\**\s+\**([A-Za-z_][A-Za-z0-9_]*)\s*\(",
                            src, flags=re.M))
@@ -82,3 +82,14 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(fmm.FmmError) as e:
         fmm.Solver(P=10)
     assert e.value.code == fmm.FMM_ERR_NO_DEVICE
+
+
+def test_petiga_wrapper_library_exports_its_header():
+    """The PetIGA wrapper ABI is its own library (its FMM_* names are the gromacs
+    wrapper's); it loads next to libexafmm_b200.so and exports what its header declares."""
+    path = os.path.join(os.path.dirname(fmm.LIB_PATH), "libexafmm_b200_petiga.so")
+    assert os.path.exists(path)
+    lib = C.CDLL(path)
+    names = header_functions("exafmm_b200_petiga.h")
+    assert set(names) >= {"FMM_Init", "FMM_B2B", "FMM_V2B", "FMM_B2V", "FMM_V2V", "Direct"}
+    assert not [n for n in names if not hasattr(lib, n)]

@@ -179,17 +179,18 @@ def test_oracle_ij_matches_golden(golden_dir):
 
 
 @pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) absent")
-@pytest.mark.parametrize("cfg,prec", [("sph_p6_f64", "f64"), ("cart_p5_f32", "f32"),
-                                      ("sph_p10_f32k_mass", "f32")])
-def test_oracle_ij_matches_reference(cfg, prec, datasets):
+@pytest.mark.parametrize("cfg,prec,common", [("sph_p6_f64", "f64", 1), ("cart_p5_f32", "f32", 1),
+                                             ("sph_p10_f32k_mass", "f32", 1),
+                                             ("sph_p8_f32k_mass", "f32", 0)])
+def test_oracle_ij_matches_reference(cfg, prec, common, datasets):
     R = Reference(cfg)
     xt, qt = datasets.make("cube", 2500, seed=3, precision=prec)
     xs, qs = datasets.make("sphere", 3500, seed=4, precision=prec)
     xt = xt * 0.5 + 0.25
     kw = dict(ncrit=32, theta=0.4, use_ropt=0)
-    r = R.run_ij(xt, qt, xs, qs, **kw)
+    r = R.run_ij(xt, qt, xs, qs, common_box=common, **kw)
     o = Oracle(prec).run_ij(xt, qt, xs, qs, basis=SPHERICAL if R.spherical else CARTESIAN,
-                            P=R.P, mass=int(R.mass), kahan=int(R.kahan), **kw)
+                            P=R.P, mass=int(R.mass), kahan=int(R.kahan), common_box=common, **kw)
     assert np.array_equal(r.m2l(), o.m2l())  # visiting order too
     assert np.array_equal(r.p2p(), o.p2p())
     pot, acc = rel_l2(o.trg(), r.trg())

@@ -41,7 +41,8 @@ class Config(C.Structure):
     _fields_ = [("basis", C.c_int), ("P", C.c_int), ("theta", C.c_double),
                 ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
                 ("use_ropt", C.c_int), ("precision", C.c_int), ("eps2", C.c_double),
-                ("images", C.c_int), ("device", C.c_int), ("cycle", C.c_double)]
+                ("images", C.c_int), ("device", C.c_int), ("cycle", C.c_double),
+                ("mutual", C.c_int)]
 
 
 # every entry point of include/exafmm_b200.h with its ctypes signature
@@ -52,6 +53,7 @@ SIGNATURES = {
     "fmm_b200_destroy": (_i, [_vp]),
     "fmm_b200_set_stream": (_i, [_vp, _vp]),
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
+    "fmm_b200_set_mutual": (_i, [_vp, _i]),
     "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "fmm_b200_solve_ij_host": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
     "fmm_b200_solve_ij_device": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp]),
@@ -192,14 +194,14 @@ class Solver:
 
     def __init__(self, basis="spherical", P=10, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
                  use_ropt=1, precision="f32", eps2=0.0, images=0, device=0,
-                 cycle=2 * np.pi):
+                 cycle=2 * np.pi, mutual=0):
         self.lib = load_library()
         cfg = Config()
         self.lib.fmm_b200_default_config(C.byref(cfg))
         cfg.basis, cfg.P, cfg.theta, cfg.ncrit = _basis(basis), P, theta, ncrit
         cfg.nspawn, cfg.use_rmax, cfg.use_ropt = nspawn, use_rmax, use_ropt
         cfg.precision, cfg.eps2, cfg.images, cfg.device = _prec(precision), eps2, images, device
-        cfg.cycle = cycle
+        cfg.cycle, cfg.mutual = cycle, mutual
         self.cfg = cfg
         self.h = C.c_void_p()
         rc = self.lib.fmm_b200_create(C.byref(cfg), C.byref(self.h))

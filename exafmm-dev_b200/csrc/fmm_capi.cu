@@ -275,6 +275,7 @@ int fmm_b200_default_config(fmm_b200_config* c) {
   c->images = 0;
   c->device = 0;
   c->cycle = 2 * M_PI;
+  c->mutual = 0;
   return FMM_OK;
 }
 
@@ -297,6 +298,10 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
   }
   if (cfg->images < 0 || (cfg->images > 0 && !(cfg->cycle > 0.0))) {
     g_create_error = "images must be >= 0 and cycle > 0 when images > 0";
+    return FMM_ERR_INVALID;
+  }
+  if (cfg->mutual != 0 && cfg->mutual != 1) {
+    g_create_error = "mutual must be 0 or 1";
     return FMM_ERR_INVALID;
   }
   if (cfg->images > 0 && cfg->basis != FMM_SPHERICAL) {
@@ -387,6 +392,13 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     delete h->base;
   }
   delete h;
+  return FMM_OK;
+}
+
+int fmm_b200_set_mutual(fmm_b200_solver* h, int mutual) {
+  if (!h || !h->base || (mutual != 0 && mutual != 1)) return FMM_ERR_INVALID;
+  h->base->cfg.mutual = mutual;
+  h->base->trav_sized = false;
   return FMM_OK;
 }
 

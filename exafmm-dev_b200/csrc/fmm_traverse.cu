@@ -16,15 +16,23 @@
 
 namespace fmmb200 {
 
-enum { PAIR_M2L = 0, PAIR_P2P = 1, PAIR_SPLIT_I = 2, PAIR_SPLIT_J = 3, PAIR_SPLIT_IJ = 4 };
+enum {
+  PAIR_M2L = 0, PAIR_P2P = 1, PAIR_SPLIT_I = 2, PAIR_SPLIT_J = 3, PAIR_SPLIT_IJ = 4,
+  PAIR_SPLIT_SELF = 5  // mutual: a cell against itself, its children pairs (a, b), a <= b
+};
 
 // cj: source cell with the periodic image of the source tree in its top bits (pair_cell,
 // pair_img); the distance is (Xi - Xj) - Xperiodic as the reference rounds it (:38)
+// mutual (dualTreeTraversal's flag, open boundary): each unordered pair is visited once
+// (TraverseRange drops the (latter, former) quarter of a range against itself, :108-113),
+// a cell against itself always splits both sides (:200), and an M2L or a P2P between two
+// different cells is emitted in both directions (the mutual kernels update both cells);
+// *nout counts those outputs
 template <typename T>
 __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
                                         const int* __restrict__ nchild,
                                         const int* __restrict__ nbody, int nspawn, T cycle,
-                                        int* nout) {
+                                        int mutual, int* nout) {
   const int cj = pair_cell((unsigned)cjp);
   T px, py, pz;
   img_shift<T>(pair_img((unsigned)cjp), cycle, px, py, pz);
@@ -33,12 +41,12 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
                  sub_rn(sub_rn(a.z, b.z), pz));
   T Rs = add_rn(a.w, b.w);
   if (R2 > mul_rn(Rs, Rs)) {
-    *nout = 1;
+    *nout = mutual ? 2 : 1;
     return PAIR_M2L;
   }
   int ni = nchild[ci], nj = nchild[cj];
   if (ni == 0 && nj == 0) {
-    *nout = 1;
+    *nout = mutual && ci != cj ? 2 : 1;
     return PAIR_P2P;
   }
   if (nj == 0) {
@@ -48,6 +56,10 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
   if (ni == 0) {
     *nout = nj;
     return PAIR_SPLIT_J;
+  }
+  if (mutual && ci == cj) {
+    *nout = ni * (ni + 1) / 2;
+    return PAIR_SPLIT_SELF;
   }
   if (nbody[ci] + nbody[cj] >= nspawn) {
     *nout = ni * nj;
@@ -65,13 +77,13 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
 template <typename T>
 __global__ void k_trav_count(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
-                             const int* __restrict__ nbody, int nspawn, T cycle,
+                             const int* __restrict__ nbody, int nspawn, T cycle, int mutual,
                              unsigned long long* __restrict__ counters) {
   unsigned long long c[3] = {0, 0, 0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
     int2 p = front[t];
     int k;
-    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, &k);
+    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, mutual, &k);
     c[ty == PAIR_M2L ? 0 : ty == PAIR_P2P ? 1 : 2] += k;
   }
   for (int i = 0; i < 3; i++) {
@@ -103,7 +115,8 @@ template <typename T>
 __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
                              const int* __restrict__ ichild, const int* __restrict__ nbody,
-                             int nspawn, T cycle, unsigned long long* __restrict__ counters,
+                             int nspawn, T cycle, int mutual,
+                             unsigned long long* __restrict__ counters,
                              unsigned long long* __restrict__ m2l,
                              unsigned long long* __restrict__ p2p, int2* __restrict__ next) {
   const int stride = gridDim.x * blockDim.x;
@@ -116,17 +129,26 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
     int2 p = make_int2(0, 0);
     if (t < nfront) {
       p = front[t];
-      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, &k);
+      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, mutual, &k);
     }
     const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+    // the reverse of a mutual pair (no periodic image with mutual)
+    const unsigned long long rev = ((unsigned long long)(unsigned)p.y << 32) | (unsigned)p.x;
     const int cj = pair_cell((unsigned)p.y), img = (int)((unsigned)p.y & ~kCellMask);
-    const unsigned long long om = warp_alloc(&counters[0], ty == PAIR_M2L ? 1u : 0u);
-    const unsigned long long op = warp_alloc(&counters[1], ty == PAIR_P2P ? 1u : 0u);
+    const unsigned long long om = warp_alloc(&counters[0], ty == PAIR_M2L ? (unsigned)k : 0u);
+    const unsigned long long op = warp_alloc(&counters[1], ty == PAIR_P2P ? (unsigned)k : 0u);
     const unsigned long long o = warp_alloc(&counters[2], ty >= PAIR_SPLIT_I ? (unsigned)k : 0u);
     if (ty == PAIR_M2L) {
       m2l[om] = packed;
+      if (k == 2) m2l[om + 1] = rev;
     } else if (ty == PAIR_P2P) {
       p2p[op] = packed;
+      if (k == 2) p2p[op + 1] = rev;
+    } else if (ty == PAIR_SPLIT_SELF) {
+      const int c0 = ichild[p.x], n = nchild[p.x];
+      unsigned long long q = o;
+      for (int a = 0; a < n; a++)
+        for (int b = a; b < n; b++) next[q++] = make_int2(c0 + a, c0 + b);
     } else if (ty == PAIR_SPLIT_I) {
       int c0 = ichild[p.x];
       for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
@@ -155,7 +177,7 @@ __global__ void __launch_bounds__(256)
     k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
                 unsigned long long front_cap, const vec4<T>* __restrict__ X,
                 const int* __restrict__ nchild, const int* __restrict__ ichild,
-                const int* __restrict__ nbody, int nspawn, T cycle, int ncells,
+                const int* __restrict__ nbody, int nspawn, T cycle, int mutual, int ncells,
                 unsigned long long* __restrict__ ctr,  // [0] M2L, [1] P2P, [2] bad index
                 unsigned long long* __restrict__ next_count, unsigned long long* __restrict__ m2l,
                 unsigned long long m2l_cap, unsigned long long* __restrict__ p2p,
@@ -170,7 +192,8 @@ __global__ void __launch_bounds__(256)
     const long long t0 = w + (long long)lane * kTravItems;
     int ty[kTravItems], k[kTravItems];
     int2 p[kTravItems];
-    unsigned v = 0;  // packed: M2L in bits 0-7, P2P in 8-15, children in 16-31
+    unsigned v = 0;  // packed: M2L in bits 0-8, P2P in 9-17, children in 18-31 (warp totals:
+                     // <= 256, <= 256, <= 8192)
 #pragma unroll
     for (int u = 0; u < kTravItems; u++) {
       ty[u] = -1;
@@ -183,12 +206,13 @@ __global__ void __launch_bounds__(256)
         if ((unsigned)p[u].x < (unsigned)ncells &&
             (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
             pair_img((unsigned)p[u].y) < 27)
-          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, cycle, &k[u]);
+          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, cycle, mutual, &k[u]);
         else
           atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
       }
-      v += (ty[u] == PAIR_M2L ? 1u : 0u) | (ty[u] == PAIR_P2P ? 1u << 8 : 0u) |
-           (ty[u] >= PAIR_SPLIT_I ? (unsigned)k[u] << 16 : 0u);
+      v += (ty[u] == PAIR_M2L ? (unsigned)k[u] : 0u) |
+           (ty[u] == PAIR_P2P ? (unsigned)k[u] << 9 : 0u) |
+           (ty[u] >= PAIR_SPLIT_I ? (unsigned)k[u] << 18 : 0u);
     }
     unsigned incl = v;
 #pragma unroll
@@ -199,29 +223,39 @@ __global__ void __launch_bounds__(256)
     const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
     unsigned long long bm = 0, bp = 0, bn = 0;
     if (lane == 31) {
-      if (tot & 0xffu) bm = atomicAdd(&ctr[0], (unsigned long long)(tot & 0xffu));
-      if ((tot >> 8) & 0xffu) bp = atomicAdd(&ctr[1], (unsigned long long)((tot >> 8) & 0xffu));
-      if (tot >> 16) bn = atomicAdd(next_count, (unsigned long long)(tot >> 16));
+      if (tot & 0x1ffu) bm = atomicAdd(&ctr[0], (unsigned long long)(tot & 0x1ffu));
+      if ((tot >> 9) & 0x1ffu) bp = atomicAdd(&ctr[1], (unsigned long long)((tot >> 9) & 0x1ffu));
+      if (tot >> 18) bn = atomicAdd(next_count, (unsigned long long)(tot >> 18));
     }
-    bm = __shfl_sync(0xffffffffu, bm, 31) + ((incl - v) & 0xffu);
-    bp = __shfl_sync(0xffffffffu, bp, 31) + (((incl - v) >> 8) & 0xffu);
-    bn = __shfl_sync(0xffffffffu, bn, 31) + ((incl - v) >> 16);
+    bm = __shfl_sync(0xffffffffu, bm, 31) + ((incl - v) & 0x1ffu);
+    bp = __shfl_sync(0xffffffffu, bp, 31) + (((incl - v) >> 9) & 0x1ffu);
+    bn = __shfl_sync(0xffffffffu, bn, 31) + ((incl - v) >> 18);
 #pragma unroll
     for (int u = 0; u < kTravItems; u++) {
       const unsigned long long packed =
           ((unsigned long long)(unsigned)p[u].x << 32) | (unsigned)p[u].y;
+      const unsigned long long rev =
+          ((unsigned long long)(unsigned)p[u].y << 32) | (unsigned)p[u].x;
       if (ty[u] == PAIR_M2L) {
         if (bm < m2l_cap) m2l[bm] = packed;
-        bm++;
+        if (k[u] == 2 && bm + 1 < m2l_cap) m2l[bm + 1] = rev;
+        bm += k[u];
       } else if (ty[u] == PAIR_P2P) {
         if (bp < p2p_cap) p2p[bp] = packed;
-        bp++;
+        if (k[u] == 2 && bp + 1 < p2p_cap) p2p[bp + 1] = rev;
+        bp += k[u];
       } else if (ty[u] >= PAIR_SPLIT_I) {
         // every slot below the capacity is written (the next step reads up to it)
         const unsigned long long o = bn;
         const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k[u], next_cap - o);
         const int cj = pair_cell((unsigned)p[u].y), img = (int)((unsigned)p[u].y & ~kCellMask);
-        if (ty[u] == PAIR_SPLIT_I) {
+        if (ty[u] == PAIR_SPLIT_SELF) {
+          const int c0 = ichild[p[u].x], n = nchild[p[u].x];
+          int w = 0;
+          for (int a = 0; a < n; a++)
+            for (int b = a; b < n; b++, w++)
+              if (w < kw) next[o + w] = make_int2(c0 + a, c0 + b);
+        } else if (ty[u] == PAIR_SPLIT_I) {
           const int c0 = ichild[p[u].x];
           for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p[u].y);
         } else if (ty[u] == PAIR_SPLIT_J) {
@@ -305,6 +339,12 @@ static int bits_for(int n) {
   return b;
 }
 
+// the mutual traversal applies to one tree with an open boundary, as in the reference (the
+// image traversals and dualTreeTraversal(cells, jcells) run with mutual = false)
+static int mutual_of(const SolverBase& s) {
+  return s.cfg.mutual && s.cfg.images == 0 && !s.ij ? 1 : 0;
+}
+
 template <typename T> static void upload_roots(Solver<T>& s) {
   // one (root, root) pair per solve of the batch (lists never cross solves); with periodic
   // images one per shift of the source tree, in the reference's image order (:250-260)
@@ -348,7 +388,8 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     FMM_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s.stream));
     int grid = std::min(ceil_div(nfront, TB), 148 * 16);
     k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
-                                               s.c_nbody.p, s.cfg.nspawn, (T)s.cfg.cycle, cnt);
+                                               s.c_nbody.p, s.cfg.nspawn, (T)s.cfg.cycle,
+                                               mutual_of(s), cnt);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaMemcpyAsync(hc, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s.stream));
@@ -375,7 +416,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     FMM_CUDA(cudaMemcpyAsync(cnt, base, sizeof(base), cudaMemcpyHostToDevice, s.stream));
     k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
                                                s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn,
-                                               (T)s.cfg.cycle, cnt,
+                                               (T)s.cfg.cycle, mutual_of(s), cnt,
                                                s.m2l.p, s.p2p.p, s.front2.p);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
@@ -410,7 +451,8 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
     DevArr<int2>& out = (l & 1) ? s.front : s.front2;
     k_trav_step<T><<<148 * 8, TB, 0, s.stream>>>(
         in.p, ctr + 3 + l, fcap, s.cX.p, s.c_nchild.p, s.c_ichild.p, s.c_nbody.p,
-        s.cfg.nspawn, (T)s.cfg.cycle, s.ncells, ctr, ctr + 4 + l, s.m2l.p, s.m2l.cap, s.p2p.p,
+        s.cfg.nspawn, (T)s.cfg.cycle, mutual_of(s), s.ncells, ctr, ctr + 4 + l, s.m2l.p,
+        s.m2l.cap, s.p2p.p,
         s.p2p.cap,
         out.p, fcap);
     FMM_LAUNCH_CHECK();

@@ -62,6 +62,10 @@ typedef struct fmm_b200_config {
                     * multipole (traversePeriodic); spherical basis only */
   int device;      /* CUDA device ordinal */
   double cycle;    /* period of the box when images > 0 (dualTreeTraversal's cycle) */
+  int mutual;      /* dualTreeTraversal's mutual flag (include/traversal.h:240): each unordered
+                    * cell pair visited once and applied both ways (open boundary, one tree);
+                    * the device evaluates both ways from the target side, so the results are
+                    * the reference's mutual ones to rounding */
 } fmm_b200_config;
 
 typedef struct fmm_b200_solver fmm_b200_solver;
@@ -89,6 +93,8 @@ int fmm_b200_set_stream(fmm_b200_solver* s, void* stream);
 /* Periodic boundary of the next traversals: image levels and period (the arguments the
  * reference passes to Traversal() and dualTreeTraversal(); include/traversal.h:216-264). */
 int fmm_b200_set_periodic(fmm_b200_solver* s, int images, double cycle);
+/* mutual flag of the next traversals (dualTreeTraversal's mutual argument) */
+int fmm_b200_set_mutual(fmm_b200_solver* s, int mutual);
 /* Message of the last failure on this handle (or of the last failed create if s is NULL). */
 const char* fmm_b200_last_error(const fmm_b200_solver* s);
 /* Which P values were compiled for a basis: writes up to cap values, returns the count. */

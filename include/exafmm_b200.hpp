@@ -15,8 +15,10 @@
 //     (phi, grad phi per unit charge, include/types.h:71 and kernels/*CPU.cxx L2P).
 // Run-time parameters replace the reference's compile-time ones (EXPANSION, Spherical /
 // Cartesian, FP64, include/types.h:12-45): set them in a Context before building.
-// Periodic images (spherical basis) are supported, mutual interactions are not;
-// Traversal::direct runs the FP64 direct sum on the GPU (one call per periodic shift).
+// Periodic images (spherical basis) and mutual traversals are supported (mutual: the
+// reference's set of unordered cell pairs, each evaluated in both directions from the
+// target side on the device).  Traversal::direct runs the FP64 direct sum on the GPU (one
+// call per periodic shift).
 #pragma once
 #include <complex>
 #include <cstdint>
@@ -245,7 +247,7 @@ class UpDownPass {
   Context& ctx_;
 };
 
-// Traversal (include/traversal.h:214-337); mutual = false only.
+// Traversal (include/traversal.h:214-337).
 class Traversal {
  public:
   Traversal(int nspawn, int images, real_t eps2, Context& ctx = Context::global()) : ctx_(ctx) {
@@ -257,9 +259,9 @@ class Traversal {
                          real_t remote = 1) {
     (void)jcells;
     (void)remote;
-    if (mutual) throw Error(FMM_ERR_NOT_SUPPORTED, "mutual traversal is not supported");
     if (icells.empty()) return;
     ctx_.check(fmm_b200_set_periodic(ctx_.get(), ctx_.cfg.images, (double)cycle));
+    ctx_.check(fmm_b200_set_mutual(ctx_.get(), mutual ? 1 : 0));
     ctx_.check(fmm_b200_traverse(ctx_.get()));
   }
   // direct sum on the GPU in FP64: TRG of ibodies += contributions of jbodies

@@ -910,7 +910,13 @@ static void push_pair(long long** a, long long* n, long long* cap, int i, int j,
 /* target tree o, source tree oj (the same tree except for oracle_solve_ij) */
 static void traverse(Oracle* o, int ci, Oracle* oj, int cj);
 
-/* TraverseRange::operator() for mutual = false (include/traversal.h:81-123) */
+/* the traversal under way is mutual: one tree, open boundary, the mutual flag */
+static int is_mutual(const Oracle* o, const Oracle* oj) {
+  return o->p.mutual && o == oj && o->p.images == 0;
+}
+
+/* TraverseRange::operator() (include/traversal.h:81-123); mutual drops the (latter, former)
+ * quarter of a range against itself, so each unordered pair is visited once */
 static void traverse_range(Oracle* o, int ib, int ie, Oracle* oj, int jb, int je) {
   if (ie - ib == 1 || je - jb == 1) {
     if (ib == jb && o == oj) {
@@ -924,7 +930,7 @@ static void traverse_range(Oracle* o, int ib, int ie, Oracle* oj, int jb, int je
     traverse_range(o, ib, im, oj, jb, jm);
     traverse_range(o, im, ie, oj, jm, je);
     traverse_range(o, ib, im, oj, jm, je);
-    traverse_range(o, im, ie, oj, jb, jm);
+    if (!is_mutual(o, oj) || ib != jb) traverse_range(o, im, ie, oj, jb, jm);
   }
 }
 
@@ -934,7 +940,7 @@ static void split_cell(Oracle* o, int ci, Oracle* oj, int cj) {
     for (int c = o->ichild[ci]; c < o->ichild[ci] + o->nchild[ci]; c++) traverse(o, c, oj, cj);
   } else if (o->nchild[ci] == 0) {
     for (int c = oj->ichild[cj]; c < oj->ichild[cj] + oj->nchild[cj]; c++) traverse(o, ci, oj, c);
-  } else if (o->cnbody[ci] + oj->cnbody[cj] >= o->p.nspawn) {
+  } else if (o->cnbody[ci] + oj->cnbody[cj] >= o->p.nspawn || (is_mutual(o, oj) && ci == cj)) {
     traverse_range(o, o->ichild[ci], o->ichild[ci] + o->nchild[ci], oj, oj->ichild[cj],
                    oj->ichild[cj] + oj->nchild[cj]);
   } else if (o->R[ci] >= oj->R[cj]) {
@@ -953,9 +959,17 @@ static void traverse(Oracle* o, int ci, Oracle* oj, int cj) {
   if (R2 > Rs * Rs) {
     push_pair(&o->m2l, &o->nm2l, &o->capm2l, ci, cj, o->img);
     if (o->p.basis == ORACLE_SPHERICAL) sph_m2l2(o, ci, oj, cj); else cart_m2l2(o, ci, oj, cj);
+    if (is_mutual(o, oj)) {  /* kernel::M2L with mutual also updates Cj->L */
+      if (o->p.basis == ORACLE_SPHERICAL) sph_m2l2(oj, cj, o, ci); else cart_m2l2(oj, cj, o, ci);
+    }
   } else if (o->nchild[ci] == 0 && oj->nchild[cj] == 0) {
     push_pair(&o->p2p, &o->np2p, &o->capp2p, ci, cj, o->img);
-    if (R2 == 0 && ci == cj && o == oj) p2p_self(o, ci); else p2p_pair2(o, ci, oj, cj);
+    if (R2 == 0 && ci == cj && o == oj) {
+      p2p_self(o, ci);
+    } else {
+      p2p_pair2(o, ci, oj, cj);
+      if (is_mutual(o, oj)) p2p_pair2(oj, cj, o, ci);  /* kernel::P2P mutual: Cj's bodies */
+    }
   } else {
     split_cell(o, ci, oj, cj);
   }

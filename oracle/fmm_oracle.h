@@ -32,6 +32,8 @@ typedef struct oracle_params {
   double eps2;    /* softening; the reference truncates it to int (traversal.h:17) */
   int images;     /* periodic image levels (include/traversal.h:21; 0 = open boundary) */
   double cycle;   /* period of the box (Traversal::dualTreeTraversal's cycle) */
+  int mutual;     /* dualTreeTraversal's mutual flag (open boundary, one tree): each
+                   * unordered cell pair visited once and applied both ways */
 } oracle_params;
 
 /* Pairs in the lists are packed (target << 32) | source | image << 27, image 0 for the

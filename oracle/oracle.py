@@ -22,7 +22,8 @@ class _Params(C.Structure):
     _fields_ = [("basis", C.c_int), ("P", C.c_int), ("theta", C.c_double),
                 ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
                 ("use_ropt", C.c_int), ("mass", C.c_int), ("kahan", C.c_int),
-                ("eps2", C.c_double), ("images", C.c_int), ("cycle", C.c_double)]
+                ("eps2", C.c_double), ("images", C.c_int), ("cycle", C.c_double),
+                ("mutual", C.c_int)]
 
 
 def _ptr(a):
@@ -133,12 +134,13 @@ class Oracle:
         self.precision = precision
 
     def run(self, x, q, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
-            use_ropt=0, mass=0, kahan=0, eps2=0.0, stages=15, images=0, cycle=2 * np.pi):
+            use_ropt=0, mass=0, kahan=0, eps2=0.0, stages=15, images=0, cycle=2 * np.pi,
+            mutual=0):
         x = np.ascontiguousarray(x, np.float64)
         q = np.ascontiguousarray(q, np.float64)
         n = len(q)
         prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2,
-                      images, cycle)
+                      images, cycle, mutual)
         h = self.lib.oracle_new(n, _ptr(x), _ptr(q), C.byref(prm))
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
         run = OracleRun(self.lib, "oracle_", h, n, nterm, basis == SPHERICAL)
@@ -166,7 +168,7 @@ class Oracle:
         xs = np.ascontiguousarray(xs, np.float64)
         qs = np.ascontiguousarray(qs, np.float64)
         prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2, 0,
-                      2 * np.pi)
+                      2 * np.pi, 0)
         hi = self.lib.oracle_new(len(qt), _ptr(xt), _ptr(qt), C.byref(prm))
         hj = self.lib.oracle_new(len(qs), _ptr(xs), _ptr(qs), C.byref(prm))
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
@@ -262,11 +264,11 @@ class Reference:
         self.mass, self.kahan = bool(L.ref_mass()), bool(L.ref_kahan())
 
     def run(self, x, q, ncrit=64, nspawn=1000, theta=0.4, use_rmax=1, use_ropt=0, eps2=0.0,
-            stages=15, record=True, threads=0, images=0, cycle=2 * np.pi):
+            stages=15, record=True, threads=0, images=0, cycle=2 * np.pi, mutual=0):
         x = np.ascontiguousarray(x, np.float64)
         q = np.ascontiguousarray(q, np.float64)
         h = self.lib.ref_run(len(q), _ptr(x), _ptr(q), ncrit, nspawn, theta, use_rmax,
-                             use_ropt, eps2, 0, stages, 1 if record else 0, threads, images,
+                             use_ropt, eps2, mutual, stages, 1 if record else 0, threads, images,
                              cycle)
         run = RefRun(self.lib, "ref_", h, len(q), self.nterm, self.spherical)
         if record:

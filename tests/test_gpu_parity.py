@@ -249,3 +249,41 @@ def test_timings_and_errors(datasets):
     assert e.value.code == fmm.FMM_ERR_NOT_SUPPORTED
     with pytest.raises(fmm.FmmError):
         fmm.Solver(P=3)
+
+
+def symmetric(pairs):
+    """Both directions of each unordered pair (a cell against itself once), sorted."""
+    t, src = pairs >> 32, pairs & 0xffffffff
+    rev = (src << 32) | t
+    return np.sort(np.unique(np.concatenate([pairs, rev])))
+
+
+@pytest.mark.parametrize("prec,P,dist", [("f64", 6, "cube"), ("f32", 8, "plummer")])
+def test_mutual_traversal_matches_oracle(prec, P, dist, datasets):
+    """mutual = 1 (include/traversal.h:70-124, 188-212): the reference's unordered pairs,
+    each evaluated in both directions; the oracle restates the mutual traversal and is
+    pinned against the reference in visiting order."""
+    x, q = datasets.make(dist, 12000, seed=17, precision=prec)
+    kw = dict(ncrit=32, theta=0.4, use_ropt=0, nspawn=500)
+    o = Oracle(prec).run(x, q, P=P, kahan=int(prec == "f32"), mutual=1, **kw)
+    s = fmm.Solver(P=P, precision=prec, mutual=1, **kw)
+    got = s.solve(x, q)
+    m2l, p2p = s.lists()
+    assert np.array_equal(m2l, symmetric(o.m2l()))
+    assert np.array_equal(p2p, symmetric(o.p2p()))
+    pot, acc = rel_l2(got, o.trg())
+    tol = 2e-5 if prec == "f32" else 1e-10
+    assert pot < tol and acc < tol, (pot, acc)
+
+
+@pytest.mark.skipif(not __import__("oracle").have_reference(), reason="reference build absent")
+def test_mutual_traversal_matches_reference(datasets):
+    from oracle import Reference
+    x, q = datasets.make("cube", 12000, seed=17, precision="f64")
+    kw = dict(ncrit=32, theta=0.4, use_ropt=0)
+    r = Reference("sph_p6_f64").run(x, q, mutual=1, **kw)
+    s = fmm.Solver(P=6, precision="f64", mutual=1, **kw)
+    g = s.solve(x, q)
+    assert np.array_equal(s.lists()[0], symmetric(r.m2l()))
+    pot, acc = rel_l2(g, r.trg())
+    assert pot < 5e-7 and acc < 5e-7, (pot, acc)

@@ -196,3 +196,22 @@ def test_oracle_ij_matches_reference(cfg, prec, common, datasets):
     pot, acc = rel_l2(o.trg(), r.trg())
     tol = 2e-6 if prec == "f32" else 5e-7
     assert pot < tol and acc < tol, (pot, acc)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) absent")
+@pytest.mark.parametrize("cfg,prec", [("sph_p6_f64", "f64"), ("cart_p5_f32", "f32"),
+                                      ("sph_p8_f32k_mass", "f32")])
+def test_oracle_mutual_matches_reference(cfg, prec, datasets):
+    """dualTreeTraversal with mutual = true: each unordered pair once (TraverseRange drops
+    the (latter, former) quarter of a range against itself), both cells updated."""
+    R = Reference(cfg)
+    x, q = datasets.make("plummer", 9000, seed=17, precision=prec)
+    kw = dict(ncrit=32, theta=0.4, use_ropt=1, nspawn=500)
+    r = R.run(x, q, mutual=1, **kw)
+    o = Oracle(prec).run(x, q, basis=SPHERICAL if R.spherical else CARTESIAN, P=R.P,
+                         kahan=int(R.kahan), mass=int(R.mass), mutual=1, **kw)
+    assert np.array_equal(r.m2l(), o.m2l())
+    assert np.array_equal(r.p2p(), o.p2p())
+    pot, acc = rel_l2(o.trg(), r.trg())
+    tol = 2e-6 if prec == "f32" else 5e-7
+    assert pot < tol and acc < tol, (pot, acc)

@@ -180,11 +180,58 @@ template <typename T> void stage_down(Solver<T>& s) {
   phase_end(s, FMM_PHASE_TOTAL);
   s.stage = ST_DOWN;
 }
+// A whole solve: the stages in order, except that the L2L levels run on a high-priority
+// side stream while P2P runs (from the end of M2L to the start of L2P).  The L2L levels
+// have few cells each and long dependent chains per cell, so alone they leave most of the
+// GPU idle; with the higher priority their blocks start as soon as SMs free up among the
+// P2P blocks.  The results are the same: P2P writes only the bodies' sums, L2L only the
+// local expansions, and L2P runs after both.
 template <typename T> void solve_all(Solver<T>& s) {
   stage_tree(s);
   stage_up(s);
-  stage_trav(s);
-  stage_down(s);
+  if (!s.side) {
+    int lo = 0, hi = 0;
+    FMM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    FMM_CUDA(cudaStreamCreateWithPriority(&s.side, cudaStreamNonBlocking, hi));
+    FMM_CUDA(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+    FMM_CUDA(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
+  }
+  phase_begin(s, FMM_PHASE_TRAVERSE);
+  build_lists(s);
+  phase_end(s, FMM_PHASE_TRAVERSE);
+  phase_begin(s, FMM_PHASE_M2L);
+  run_m2l(s);
+  phase_end(s, FMM_PHASE_M2L);
+  // fork: the L2L levels on the side stream
+  FMM_CUDA(cudaEventRecord(s.fork, s.stream));
+  FMM_CUDA(cudaStreamWaitEvent(s.side, s.fork, 0));
+  cudaStream_t main = s.stream;
+  s.stream = s.side;
+  try {
+    phase_begin(s, FMM_PHASE_DOWNWARD);
+    downward_l2l(s);
+    FMM_CUDA(cudaEventRecord(s.join, s.stream));
+  } catch (...) {
+    s.stream = main;
+    throw;
+  }
+  s.stream = main;
+  phase_begin(s, FMM_PHASE_P2P);
+  s.trg_s.ensure(std::max(s.n, 1));
+  s.trg_e.ensure(std::max(s.n, 1));
+  if (s.n > 0) {
+    FMM_CUDA(cudaMemsetAsync(s.trg_s.p, 0, sizeof(vec4<T>) * s.n, s.stream));
+    FMM_CUDA(cudaMemsetAsync(s.trg_e.p, 0, sizeof(vec4<T>) * s.n, s.stream));
+  }
+  run_p2p(s);
+  phase_end(s, FMM_PHASE_P2P);
+  s.stage = ST_TRAV;
+  FMM_CUDA(cudaStreamWaitEvent(s.stream, s.join, 0));  // join before L2P reads the locals
+  downward_l2p(s);
+  if (s.n == 0) s.trg_out.ensure(1);
+  phase_end(s, FMM_PHASE_DOWNWARD);
+  phase_end(s, FMM_PHASE_TOTAL);
+  s.stage = ST_DOWN;
 }
 
 }  // namespace
@@ -388,6 +435,9 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     h->base->dtmp.release();
     for (int i = 0; i < 2 * FMM_NUM_PHASES; i++)
       if (s.ev[i]) cudaEventDestroy(s.ev[i]);
+    if (s.fork) cudaEventDestroy(s.fork);
+    if (s.join) cudaEventDestroy(s.join);
+    if (s.side) cudaStreamDestroy(s.side);
     if (s.scal_host) cudaFreeHost(s.scal_host);
     delete h->base;
   }

@@ -80,15 +80,25 @@ template <typename T> void run_m2l(Solver<T>& s) {
   }
 }
 
-template <typename T> void downward_pass(Solver<T>& s) {
+template <typename T> void downward_l2l(Solver<T>& s) {
   if (s.ncells == 0) return;
   ExpansionOps<T> ops = ops_of(s);
   for (int l = 1; l <= s.maxlevel; l++) ops.l2l_level(s, s.level_lo[l], s.level_lo[l + 1]);
+}
+
+template <typename T> void downward_l2p(Solver<T>& s) {
+  if (s.ncells == 0) return;
+  ExpansionOps<T> ops = ops_of(s);
   ops.l2p(s);
   s.trg_out.ensure(s.n);
   k_output<T><<<ceil_div(s.n, 256), 256, 0, s.stream>>>(s.n, s.order.p, s.trg_s.p, s.trg_e.p,
                                                         s.trg_out.p);
   FMM_LAUNCH_CHECK();
+}
+
+template <typename T> void downward_pass(Solver<T>& s) {
+  downward_l2l(s);
+  downward_l2p(s);
 }
 
 template void upward_pass<float>(Solver<float>&);
@@ -97,5 +107,9 @@ template void run_m2l<float>(Solver<float>&);
 template void run_m2l<double>(Solver<double>&);
 template void downward_pass<float>(Solver<float>&);
 template void downward_pass<double>(Solver<double>&);
+template void downward_l2l<float>(Solver<float>&);
+template void downward_l2l<double>(Solver<double>&);
+template void downward_l2p<float>(Solver<float>&);
+template void downward_l2p<double>(Solver<double>&);
 
 }  // namespace fmmb200

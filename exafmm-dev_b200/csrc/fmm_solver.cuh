@@ -15,15 +15,35 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "fmm_common.cuh"
 
 namespace fmmb200 {
 
+// A grow-only device array owned by one solver: freed with it, moved (never copied).
 template <typename U> struct DevArr {
   U* p = nullptr;
   size_t cap = 0;
+  DevArr() = default;
+  DevArr(const DevArr&) = delete;
+  DevArr& operator=(const DevArr&) = delete;
+  DevArr(DevArr&& o) noexcept : p(o.p), cap(o.cap) {
+    o.p = nullptr;
+    o.cap = 0;
+  }
+  DevArr& operator=(DevArr&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      cap = o.cap;
+      o.p = nullptr;
+      o.cap = 0;
+    }
+    return *this;
+  }
+  ~DevArr() { release(); }
   void ensure(size_t n) {
     if (n <= cap) return;
     if (p) cudaFree(p);
@@ -100,6 +120,10 @@ struct SolverBase {
   // phase timing
   cudaEvent_t ev[2 * FMM_NUM_PHASES] = {};
   bool ev_used[FMM_NUM_PHASES] = {};
+  // whole solves run P2P on a side stream, forked after the lists and joined before L2P,
+  // so that it overlaps M2L and the latency-bound L2L levels
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   virtual ~SolverBase() {}
 };
 
@@ -116,6 +140,8 @@ template <typename T> struct Solver : SolverBase {
 template <typename T> void build_tree(Solver<T>& s);          // fmm_tree.cu
 template <typename T> void upward_pass(Solver<T>& s);         // fmm_passes.cu
 template <typename T> void downward_pass(Solver<T>& s);       // fmm_passes.cu
+template <typename T> void downward_l2l(Solver<T>& s);        // fmm_passes.cu: L2L levels
+template <typename T> void downward_l2p(Solver<T>& s);        // fmm_passes.cu: L2P + output
 template <typename T> void build_lists(Solver<T>& s);         // fmm_traverse.cu
 template <typename T> void run_m2l(Solver<T>& s);             // fmm_passes.cu
 template <typename T> void run_p2p(Solver<T>& s);             // fmm_p2p.cu

@@ -401,7 +401,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
       if (nm2l) FMM_CUDA(cudaMemcpyAsync(t.p, s.m2l.p, nm2l * 8, cudaMemcpyDeviceToDevice, s.stream));
       FMM_CUDA(cudaStreamSynchronize(s.stream));
       s.m2l.release();
-      s.m2l = t;
+      s.m2l = std::move(t);
     }
     if (np2p + ap > (long long)s.p2p.cap) {
       DevArr<unsigned long long> t;
@@ -409,7 +409,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
       if (np2p) FMM_CUDA(cudaMemcpyAsync(t.p, s.p2p.p, np2p * 8, cudaMemcpyDeviceToDevice, s.stream));
       FMM_CUDA(cudaStreamSynchronize(s.stream));
       s.p2p.release();
-      s.p2p = t;
+      s.p2p = std::move(t);
     }
     s.front2.ensure(std::max<long long>(an, 1));
     unsigned long long base[3] = {(unsigned long long)nm2l, (unsigned long long)np2p, 0};

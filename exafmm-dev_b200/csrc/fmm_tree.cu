@@ -437,10 +437,7 @@ template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
   b.ensure(n > 2 * a.cap ? n : 2 * a.cap);
   if (a.p) FMM_CUDA(cudaMemcpyAsync(b.p, a.p, a.cap * sizeof(U), cudaMemcpyDeviceToDevice, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
-  a.release();
-  a = b;
-  b.p = nullptr;
-  b.cap = 0;
+  a = std::move(b);
 }
 
 // Sort (key, body) pairs by (root, key), stable: one radix sort on the key over all roots,

@@ -217,12 +217,20 @@ __device__ __forceinline__ void m2m_passes(const T* yr, const T* yi, const T* Mc
 // translates its child with compile-time indices, the group sums in a fixed order, and the
 // monopole is re-summed in child order (the reference's sequence) so that the radii of the
 // error-optimised MAC see the same M[0] bits.
+// Threads per block of the FP32 M2M / L2L kernels; each thread stages the expansion it
+// translates (its child's multipole, its parent's local) in its own row of shared memory
+// first, with all the loads issued at once: read term by term from global memory, their
+// latencies added up along the translation's dependent chain (~40 us per level).
+constexpr int kTrThreads = 64;
+
 template <typename T, int P>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kTrThreads)
     k_m2m_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
               const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
               int ncoef, int use_rmax, T theta) {
-  constexpr int NT = sph::NT(P);
+  constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;  // odd row stride: no bank conflicts
+  __shared__ T rows[kTrThreads * STR];
+  T* row = rows + threadIdx.x * STR;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = lo + (gt >> 3);
   const int slot = gt & 7;
@@ -240,10 +248,13 @@ __global__ void __launch_bounds__(128)
   const T* Mc = M;
   if (has) {
     const int cc = c0 + slot;
+    const T* src = M + (size_t)cc * ncoef;
+#pragma unroll
+    for (int t = 0; t < NT; t++) sph::load_pair(src + 2 * t, row[2 * t], row[2 * t + 1]);
     const vec4<T> Xc = cX[cc];
     sph::Angles<T> a = sph::angles(Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
     sph::multipole<T, P>(a, a.r, yr, yi);
-    Mc = M + (size_t)cc * ncoef;
+    Mc = row;
     rr = add_rn(sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z))), Xc.w);
   }
 #pragma unroll
@@ -278,21 +289,27 @@ __device__ __forceinline__ void l2l_passes(const T* yr, const T* yi, const T* Lp
   }
 }
 
-// FP32 L2L: thread per cell, compile-time indices.
+// FP32 L2L: thread per cell, compile-time indices, the parent's local staged in the
+// thread's shared row.
 template <typename T, int P>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kTrThreads)
     k_l2l_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
               const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
-  constexpr int NT = sph::NT(P);
+  constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;
+  __shared__ T rows[kTrThreads * STR];
+  T* row = rows + threadIdx.x * STR;
   const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= hi) return;
   const int c = npos[v];
   const int p = iparent[c];
+  const T* src = L + (size_t)p * ncoef;
+#pragma unroll
+  for (int t = 0; t < NT; t++) sph::load_pair(src + 2 * t, row[2 * t], row[2 * t + 1]);
   const vec4<T> Xc = cX[c], Xp = cX[p];
   T yr[NT], yi[NT];
   sph::Angles<T> a = sph::angles(Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
   sph::multipole<T, P>(a, a.r, yr, yi);
-  l2l_passes<T, P, 0>(yr, yi, L + (size_t)p * ncoef, L + (size_t)c * ncoef);
+  l2l_passes<T, P, 0>(yr, yi, row, L + (size_t)c * ncoef);
 }
 
 // ---------------------------------------------------------------- M2L
@@ -568,7 +585,7 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
   if constexpr (sizeof(T) == 4) {
-    k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), 128), 128, 0, s.stream>>>(
+    k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), kTrThreads), kTrThreads, 0, s.stream>>>(
         lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
         (T)s.cfg.theta);
     FMM_LAUNCH_CHECK();
@@ -592,8 +609,8 @@ template <typename T, int P> static void m2l_(Solver<T>& s) {
 }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
   if constexpr (sizeof(T) == 4) {
-    k_l2l_reg<T, P><<<ceil_div(hi - lo, 128), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
-                                                                  s.cX.p, s.L.p, s.ncoef);
+    k_l2l_reg<T, P><<<ceil_div(hi - lo, kTrThreads), kTrThreads, 0, s.stream>>>(
+        lo, hi, s.npos.p, s.c_iparent.p, s.cX.p, s.L.p, s.ncoef);
     FMM_LAUNCH_CHECK();
   } else {
     constexpr int W = SphCfg<T>::W;

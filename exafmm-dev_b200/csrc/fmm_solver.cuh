@@ -113,6 +113,7 @@ struct SolverBase {
   int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
+  DevArr<int> seg_cnt;  // pairs per target while a list is grouped by target
   DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches
   int m2l_ntgt = 0;
   DevArr<unsigned long long> p2p_pairs_count;
@@ -120,8 +121,8 @@ struct SolverBase {
   // phase timing
   cudaEvent_t ev[2 * FMM_NUM_PHASES] = {};
   bool ev_used[FMM_NUM_PHASES] = {};
-  // whole solves run P2P on a side stream, forked after the lists and joined before L2P,
-  // so that it overlaps M2L and the latency-bound L2L levels
+  // whole solves run the latency-bound L2L levels on a high-priority side stream, forked
+  // after M2L and joined before L2P, so that they overlap P2P
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   virtual ~SolverBase() {}

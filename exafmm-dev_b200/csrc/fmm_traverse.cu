@@ -8,8 +8,10 @@
 // pairs depends only on each pair, so here the recursion runs breadth first: every
 // iteration classifies a frontier of pairs in parallel (count pass + write pass, exact
 // sizes, no overflow) and emits M2L pairs, P2P pairs and the next frontier.  Lists are
-// then sorted by (target, source) into per-target CSR for the M2L and P2P kernels.
+// then grouped by target (per-target CSR for the M2L and P2P kernels) and sorted by source
+// within each target.
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "fmm_solver.cuh"
@@ -272,19 +274,177 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// CSR offsets of a sorted packed list: off[c] = first pair whose target >= c
-__global__ void k_csr(const unsigned long long* __restrict__ pairs, long long n, int ncells,
-                      int* __restrict__ off) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c > ncells) return;
-  unsigned long long key = (unsigned long long)(unsigned)c << 32;
-  long long a = 0, z = n;
-  while (a < z) {
-    long long m = (a + z) >> 1;
-    if (pairs[m] < key) a = m + 1;
-    else z = m;
+// ---------------------------------------------------------------- grouping by target
+// A list leaves the traversal in the order its pairs were found (atomic slots).  It is
+// grouped by target with a count per target (warp-aggregated atomics), an exclusive scan
+// of the counts into the CSR offsets, and a scatter of every pair's source key
+// (image << b | cell) into its target's range; each range is then sorted in shared memory
+// and written back as (target << 32 | image << 27 | cell).  The result is the order of a
+// global sort of the packed pairs (target, then image, then source cell), so it does not
+// depend on the order in which the traversal emitted them.
+constexpr int kSegWarpCap = 1024;   // keys one warp sorts in its registers
+constexpr int kSegBlockCap = 8192;  // keys one block sorts; longer ranges: global sort
+constexpr int kSegWarps = 8;
+constexpr int kSegBlock = 512;
+
+__global__ void k_seg_count(const unsigned long long* __restrict__ pairs, long long n,
+                            int* __restrict__ cnt) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t0 = blockIdx.x * (long long)blockDim.x; t0 < n; t0 += stride) {
+    const long long t = t0 + threadIdx.x;
+    const unsigned act = __ballot_sync(0xffffffffu, t < n);
+    if (t >= n) continue;
+    const int tgt = (int)(pairs[t] >> 32);
+    const unsigned grp = __match_any_sync(act, tgt);
+    if (lane_id() == __ffs(grp) - 1) atomicAdd(&cnt[tgt], __popc(grp));
   }
-  off[c] = (int)a;
+}
+
+// cnt holds the counts on entry and zeros on exit; each warp's pairs of one target take
+// consecutive slots from the top of the target's remaining range
+__global__ void k_seg_scatter(const unsigned long long* __restrict__ pairs, long long n,
+                              const int* __restrict__ off, int* __restrict__ cnt, int b,
+                              unsigned* __restrict__ keys) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int lane = lane_id();
+  for (long long t0 = blockIdx.x * (long long)blockDim.x; t0 < n; t0 += stride) {
+    const long long t = t0 + threadIdx.x;
+    const unsigned act = __ballot_sync(0xffffffffu, t < n);
+    if (t >= n) continue;
+    const unsigned long long v = pairs[t];
+    const int tgt = (int)(v >> 32);
+    const unsigned src = (unsigned)v;
+    const unsigned grp = __match_any_sync(act, tgt);
+    const int leader = __ffs(grp) - 1, k = __popc(grp);
+    int top = 0;
+    if (lane == leader) top = atomicSub(&cnt[tgt], k);
+    top = __shfl_sync(grp, top, leader);
+    const int rank = __popc(grp & ((1u << lane) - 1));
+    keys[off[tgt] + top - k + rank] = ((unsigned)pair_img(src) << b) | (unsigned)pair_cell(src);
+  }
+}
+
+__device__ __forceinline__ unsigned long long seg_pair(int c, unsigned key, int b) {
+  const unsigned src = ((key >> b) << kImgShift) | (key & ((1u << b) - 1));
+  return ((unsigned long long)(unsigned)c << 32) | src;
+}
+
+// ascending bitonic sort of a[0, n2), n2 a power of two, by nt threads (tid) that sync
+// with __syncthreads (BLOCK) or __syncwarp
+template <bool BLOCK>
+__device__ __forceinline__ void bitonic_sort(unsigned* a, int n2, int tid, int nt) {
+  for (int k = 2; k <= n2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int p = tid; p < (n2 >> 1); p += nt) {
+        const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));  // bit j of i clear
+        const int l = i | j;
+        const unsigned x = a[i], y = a[l];
+        if ((x > y) == ((i & k) == 0)) {
+          a[i] = y;
+          a[l] = x;
+        }
+      }
+      if (BLOCK) __syncthreads();
+      else __syncwarp();
+    }
+}
+
+// A warp's range of n <= 32 K keys sorted in registers: lane l holds keys l K .. l K + K - 1
+// (padded with 0xffffffff), the bitonic network's stages of partner distance j < K run
+// within each lane, those with j >= K pair the lanes l and l ^ (j / K) by shuffles; every
+// index and, for k < K, every direction is a compile-time constant.
+template <int K>
+__device__ __forceinline__ void warp_sort_range(const unsigned* __restrict__ keys, int n, int c,
+                                                int b, unsigned long long* __restrict__ out) {
+  const int lane = lane_id();
+  unsigned v[K];
+#pragma unroll
+  for (int r = 0; r < K; r++) {
+    const int e = lane * K + r;
+    v[r] = e < n ? keys[e] : 0xffffffffu;
+  }
+#pragma unroll
+  for (int k = 2; k <= 32 * K; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j < K) {
+#pragma unroll
+        for (int r = 0; r < K; r++) {
+          if (r & j) continue;
+          const bool up = k < K ? (r & k) == 0 : (lane & (k / K)) == 0;
+          const unsigned x = v[r], y = v[r | j];
+          const unsigned lo = min(x, y), hi = max(x, y);
+          v[r] = up ? lo : hi;
+          v[r | j] = up ? hi : lo;
+        }
+      } else {
+        const bool keep_min = ((lane & (j / K)) == 0) == ((lane & (k / K)) == 0);
+#pragma unroll
+        for (int r = 0; r < K; r++) {
+          const unsigned y = __shfl_xor_sync(0xffffffffu, v[r], j / K);
+          v[r] = keep_min ? min(v[r], y) : max(v[r], y);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < K; r++) {
+    const int e = lane * K + r;
+    if (e < n) out[e] = seg_pair(c, v[r], b);
+  }
+}
+
+// one warp per target with at most kSegWarpCap pairs
+__global__ void __launch_bounds__(32 * kSegWarps)
+    k_seg_sort_warp(int ncells, const int* __restrict__ off, const unsigned* __restrict__ keys,
+                    int b, unsigned long long* __restrict__ out) {
+  const int c = blockIdx.x * kSegWarps + (threadIdx.x >> 5);
+  if (c >= ncells) return;
+  const int s0 = off[c], n = off[c + 1] - s0;
+  if (n == 0 || n > kSegWarpCap) return;
+  keys += s0;
+  out += s0;
+  if (n <= 32) warp_sort_range<1>(keys, n, c, b, out);
+  else if (n <= 64) warp_sort_range<2>(keys, n, c, b, out);
+  else if (n <= 128) warp_sort_range<4>(keys, n, c, b, out);
+  else if (n <= 256) warp_sort_range<8>(keys, n, c, b, out);
+  else if (n <= 512) warp_sort_range<16>(keys, n, c, b, out);
+  else warp_sort_range<32>(keys, n, c, b, out);
+}
+
+// the longer ranges, one block at a time; a range above kSegBlockCap is written unsorted and
+// flagged for the global sort
+__global__ void __launch_bounds__(kSegBlock)
+    k_seg_sort_block(int ncells, const int* __restrict__ off, const unsigned* __restrict__ keys,
+                     int b, unsigned long long* __restrict__ out, int* __restrict__ overflow) {
+  __shared__ unsigned a[kSegBlockCap];
+  __shared__ int todo[kSegBlock];
+  __shared__ int ntodo;
+  for (int base = blockIdx.x * kSegBlock; base < ncells; base += gridDim.x * kSegBlock) {
+    if (threadIdx.x == 0) ntodo = 0;
+    __syncthreads();
+    const int cc = base + threadIdx.x;
+    if (cc < ncells && off[cc + 1] - off[cc] > kSegWarpCap) todo[atomicAdd(&ntodo, 1)] = cc;
+    __syncthreads();
+    const int m = ntodo;
+    for (int q = 0; q < m; q++) {
+      const int c = todo[q];
+      const int s0 = off[c], n = off[c + 1] - s0;
+      if (n > kSegBlockCap) {
+        for (int i = threadIdx.x; i < n; i += kSegBlock) out[s0 + i] = seg_pair(c, keys[s0 + i], b);
+        if (threadIdx.x == 0) atomicExch(overflow, 1);
+        continue;
+      }
+      int n2 = 32;
+      while (n2 < n) n2 <<= 1;
+      for (int i = threadIdx.x; i < n2; i += kSegBlock) a[i] = i < n ? keys[s0 + i] : 0xffffffffu;
+      __syncthreads();
+      bitonic_sort<true>(a, n2, threadIdx.x, kSegBlock);
+      for (int i = threadIdx.x; i < n; i += kSegBlock) out[s0 + i] = seg_pair(c, a[i], b);
+      __syncthreads();
+    }
+    __syncthreads();
+  }
 }
 
 // M2L targets (cells with at least one source) keyed by their number of 32-source batches,
@@ -337,6 +497,43 @@ static int bits_for(int n) {
   int b = 1;
   while ((1LL << b) < (long long)n) b++;
   return b;
+}
+
+// group a list by target (k_seg_*): CSR offsets into off[0, ncells], pairs sorted within
+// each target's range
+static void group_by_target(SolverBase& s, unsigned long long* lst, long long n, int b,
+                            int* off, int* overflow) {
+  const int TB = 256;
+  FMM_CUDA(cudaMemsetAsync(s.seg_cnt.p, 0, (s.ncells + 1) * sizeof(int), s.stream));
+  const int grid = (int)std::max(1LL, std::min<long long>(ceil_div(n, TB), 148 * 16));
+  if (n > 0) {
+    k_seg_count<<<grid, TB, 0, s.stream>>>(lst, n, s.seg_cnt.p);
+    FMM_LAUNCH_CHECK();
+  }
+  exclusive_sum_int(s, s.seg_cnt.p, off, s.ncells + 1);
+  if (n == 0) return;
+  unsigned* keys = (unsigned*)s.list_tmp.p;
+  k_seg_scatter<<<grid, TB, 0, s.stream>>>(lst, n, off, s.seg_cnt.p, b, keys);
+  FMM_LAUNCH_CHECK();
+  k_seg_sort_warp<<<ceil_div(s.ncells, kSegWarps), 32 * kSegWarps, 0, s.stream>>>(s.ncells, off,
+                                                                                 keys, b, lst);
+  FMM_LAUNCH_CHECK();
+  k_seg_sort_block<<<std::min(ceil_div(s.ncells, kSegBlock), 148), kSegBlock, 0, s.stream>>>(
+      s.ncells, off, keys, b, lst, overflow);
+  FMM_LAUNCH_CHECK();
+}
+
+// a whole list sorted on (target << (b + ib) | image << b | source), 2 b + ib key bits:
+// the targets whose ranges were too long for k_seg_sort_block
+static void global_sort_list(SolverBase& s, unsigned long long* lst, long long n, int b, int ib) {
+  const int TB = 256;
+  const int grid = (int)std::min<long long>(ceil_div(n, TB), 148 * 16);
+  k_pack_pairs<<<grid, TB, 0, s.stream>>>(lst, n, b, ib, 1);
+  FMM_LAUNCH_CHECK();
+  sort_keys_u64(s, lst, s.list_tmp.p, (int)n, 2 * b + ib);
+  k_pack_pairs<<<grid, TB, 0, s.stream>>>(s.list_tmp.p, n, b, ib, 0);
+  FMM_LAUNCH_CHECK();
+  FMM_CUDA(cudaMemcpyAsync(lst, s.list_tmp.p, 8 * (size_t)n, cudaMemcpyDeviceToDevice, s.stream));
 }
 
 // the mutual traversal applies to one tree with an open boundary, as in the reference (the
@@ -487,29 +684,17 @@ template <typename T> void build_lists(Solver<T>& s) {
   }
   s.nm2l = nm2l;
   s.np2p = np2p;
-  // sort on (target << (b + ib) | image << b | source) with b = bits(ncells): 2 b + ib key
-  // bits instead of 64
   const int b = bits_for(s.ncells), ib = s.cfg.images > 0 ? 5 : 0;
+  if (std::max(nm2l, np2p) > (long long)INT_MAX)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED, "more than 2^31 - 1 pairs in an interaction list");
   s.list_tmp.ensure(std::max<long long>(std::max(nm2l, np2p), 1));
-  for (int which = 0; which < 2; which++) {
-    DevArr<unsigned long long>& lst = which ? s.p2p : s.m2l;
-    const long long cnt = which ? np2p : nm2l;
-    if (cnt == 0) continue;
-    const int grid = std::min(ceil_div(cnt, TB), 148 * 16);
-    k_pack_pairs<<<grid, TB, 0, s.stream>>>(lst.p, cnt, b, ib, 1);
-    FMM_LAUNCH_CHECK();
-    s.list_tmp.ensure(cnt);
-    sort_keys_u64(s, lst.p, s.list_tmp.p, (int)cnt, 2 * b + ib);
-    k_pack_pairs<<<grid, TB, 0, s.stream>>>(s.list_tmp.p, cnt, b, ib, 0);
-    FMM_LAUNCH_CHECK();
-    std::swap(lst, s.list_tmp);
-  }
   s.m2l_off.ensure(s.ncells + 1);
   s.p2p_off.ensure(s.ncells + 1);
-  k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.m2l.p, nm2l, s.ncells, s.m2l_off.p);
-  FMM_LAUNCH_CHECK();
-  k_csr<<<ceil_div(s.ncells + 1, TB), TB, 0, s.stream>>>(s.p2p.p, np2p, s.ncells, s.p2p_off.p);
-  FMM_LAUNCH_CHECK();
+  s.seg_cnt.ensure(s.ncells + 1);
+  int* overflow = (int*)(cnt + 5);  // per list: a target range too long for the blocks
+  FMM_CUDA(cudaMemsetAsync(overflow, 0, 2 * sizeof(int), s.stream));
+  group_by_target(s, s.m2l.p, nm2l, b, s.m2l_off.p, overflow);
+  group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1);
   // M2L target order: by descending batch count (stable in cell index)
   {
     int* ntgt = (int*)(cnt + 4);
@@ -528,9 +713,15 @@ template <typename T> void build_lists(Solver<T>& s) {
   k_p2p_bodypairs<<<std::max(1, std::min(ceil_div(np2p, TB), 148 * 8)), TB, 0, s.stream>>>(
       s.p2p.p, np2p, s.c_nbody.p, cnt + 3);
   FMM_LAUNCH_CHECK();
-  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                           s.stream));
+  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, 3 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
+  const int* hflow = (const int*)(hc + 5);
+  if (hflow[0] || hflow[1]) {
+    if (hflow[0]) global_sort_list(s, s.m2l.p, nm2l, b, ib);
+    if (hflow[1]) global_sort_list(s, s.p2p.p, np2p, b, ib);
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  }
   s.p2p_body_pairs = (long long)hc[3];
   s.m2l_ntgt = s.scal_host[12];
 }

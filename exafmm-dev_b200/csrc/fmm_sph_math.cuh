@@ -215,6 +215,109 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, cons
   }
 }
 
+// The local harmonics split into a real factor and an azimuthal phase: Y[n, m] =
+// rho[n, m] e^(i m beta) for m >= 0 (rho = the t of local(), the same arithmetic).  rho is
+// stored for the degrees n >= A0 only, at sidx(n, m) - sidx(A0, 0); (cr[m], ci[m]) =
+// e^(i m beta) for m < P.
+template <typename T, int P, int A0>
+__host__ __device__ __forceinline__ void local_rho(const Angles<T>& a, T* rho, T* cr, T* ci) {
+  const T ninvr = -T(1) / a.r;
+  T fact = 1, pn = 1;
+  T rpm = -ninvr;  // (-1)^m / r^(m+1)
+  T er = 1, ei = 0;
+#pragma unroll
+  for (int m = 0; m < P; m++) {
+    cr[m] = er;
+    ci[m] = ei;
+    T q = pn, qm1 = 0;  // Q[m] = P_m^m
+    if (m >= A0) rho[sidx(m, m) - sidx(A0, 0)] = q * rpm;
+    T rpn = rpm;
+#pragma unroll
+    for (int n = m + 1; n < P; n++) {
+      const T qn = fma(T(2 * n - 1) * a.x, q, T(-(n - 1 + m) * (n - 1 - m)) * qm1);
+      qm1 = q;
+      q = qn;
+      rpn *= ninvr;
+      if (n >= A0) rho[sidx(n, m) - sidx(A0, 0)] = q * rpn;
+    }
+    rpm *= ninvr;
+    pn = -pn * fact * a.y;
+    fact += 2;
+    const T tt = er * a.cb - ei * a.sb;
+    ei = er * a.sb + ei * a.cb;
+    er = tt;
+  }
+}
+
+// The M2L of m2l_pair in the source's azimuthal frame.  Every term of output (j, k) carries
+// the phase e^(i (m - k) beta) of its harmonic, so with M'[n, mu] = M[n, mu] e^(i mu beta)
+//   L[j, k] += e^(-i k beta) A[j, k],   A[j, k] = sum over (n, mu) of real rho times M' or
+//   conj(M'),
+// and each term of A is two real multiply-adds instead of a complex one (four): the
+// source is rotated once on entry (one complex product per mu > 0 coefficient) and each
+// output once on exit.  Terms and signs as m2l_pair: mu = 0: (-1)^j rho[a, k] M';
+// m = -mu: (-1)^j rho[a, k + mu] conj(M'); m = +mu: (-1)^(j + min(k, mu)) rho[a, |mu - k|] M'.
+template <typename T, int P, int J0, int J1>
+__host__ __device__ __forceinline__ void m2l_pair_rot(const T* rho, const T* cr, const T* ci,
+                                                      const T* Mj, T* Lr, T* Li) {
+  constexpr int O0 = sidx(J0, 0), NO = sidx(J1, 0) - sidx(J0, 0);
+  T Ar[NO], Ai[NO];
+#pragma unroll
+  for (int t = 0; t < NO; t++) Ar[t] = Ai[t] = T(0);
+#pragma unroll
+  for (int n = 0; n < P - J0; n++) {
+#pragma unroll
+    for (int mu = 0; mu <= n; mu++) {
+      T mr, mi;
+      load_pair(Mj + 2 * sidx(n, mu), mr, mi);
+      if (mu > 0) {
+        const T r = mr * cr[mu] - mi * ci[mu];
+        mi = mr * ci[mu] + mi * cr[mu];
+        mr = r;
+      }
+#pragma unroll
+      for (int j = J0; j < J1; j++) {
+        if (j + n >= P) break;
+        const int a = j + n;
+        const bool oj = (j & 1) != 0;
+#pragma unroll
+        for (int k = 0; k <= j; k++) {
+          const int t = sidx(j, k) - O0;
+          if (mu == 0) {
+            const T p = rho[sidx(a, k) - O0];
+            const T ps = oj ? -p : p;
+            Ar[t] = fma(ps, mr, Ar[t]);
+            Ai[t] = fma(ps, mi, Ai[t]);
+          } else {
+            const T p1 = rho[sidx(a, k + mu) - O0];
+            const T s1 = oj ? -p1 : p1;
+            Ar[t] = fma(s1, mr, Ar[t]);
+            Ai[t] = fma(-s1, mi, Ai[t]);
+            const T p2 = rho[sidx(a, mu >= k ? mu - k : k - mu) - O0];
+            const bool o2 = oj != (((k < mu ? k : mu) & 1) != 0);
+            const T s2 = o2 ? -p2 : p2;
+            Ar[t] = fma(s2, mr, Ar[t]);
+            Ai[t] = fma(s2, mi, Ai[t]);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = J0; j < J1; j++)
+#pragma unroll
+    for (int k = 0; k <= j; k++) {
+      const int t = sidx(j, k) - O0, g = sidx(j, k);
+      if (k == 0) {
+        Lr[g] += Ar[t];
+        Li[g] += Ai[t];
+      } else {
+        Lr[g] = fma(cr[k], Ar[t], fma(ci[k], Ai[t], Lr[g]));
+        Li[g] = fma(cr[k], Ai[t], fma(-ci[k], Ar[t], Li[g]));
+      }
+    }
+}
+
 // Y[a, b] for any sign of b from the m >= 0 store (real parts yr, imaginary parts yi)
 template <typename T>
 __host__ __device__ __forceinline__ void yget(const T* yr, const T* yi, int a, int b, T& r,

@@ -314,71 +314,68 @@ __global__ void __launch_bounds__(kTrThreads)
 
 // ---------------------------------------------------------------- M2L
 // FP32: warp per target, lane per source cell, harmonics and local expansion in registers,
-// one warp reduction per target cell at the end.  The outputs are split into passes over
-// their degree (separate launches) so that each unrolled contraction stays small: the
-// kernel is bound by instruction fetch when one pass holds all of P = 10.
+// one warp reduction per target cell at the end.  Each pair is contracted in the source's
+// azimuthal frame (m2l_pair_rot: real harmonic factors, half the multiply-adds of the
+// complex form).  The outputs are split into passes over their degree (separate launches)
+// so that each pass's registers stay within one block of 15-20 warps per SM.
 constexpr int kM2LWarps = 12;
-// output degrees per FP32 M2L pass: add degrees while the pass stays under ~600 complex
-// multiply-adds (the unrolled code of one pass, and its registers, stay moderate)
+// output degrees per FP32 M2L pass: add degrees while the pass's registers (the real
+// harmonic factors of degrees >= J0, and four per output: the pair's rotated sum and the
+// accumulator, real and imaginary) stay under ~110
 __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
-  int cost = 0, j = J0;
+  const int rho = sph::NT(P) - sph::sidx(J0, 0);
+  int j = J0, outs = 0;
   while (j < P) {
-    const int c = (j + 1) * (P - j) * (P - j);
-    if (j > J0 && cost + c > 600) break;
-    cost += c;
+    const int o = outs + j + 1;
+    if (j > J0 && rho + 4 * o > 110) break;
+    outs = o;
     j++;
   }
   return j;
 }
 
 // warps per block of one FP32 M2L pass: as many as the pass's registers allow in one block
-// per SM without spilling (P = 10: 128, 140 and 165 registers for the passes starting at
-// degrees 0, 3 and 6; ptxas keeps 13-15-warp blocks at 128 registers)
+// per SM without spilling (P = 10: 128, 134, 135 and 98 registers for the passes starting
+// at degrees 0, 4, 6 and 8)
 __host__ __device__ constexpr int m2l_pass_warps(int P, int J0) {
-  return P == 10 ? (J0 == 0 ? 14 : 12) : kM2LWarps;
+  return P == 10 ? (J0 == 0 ? 16 : J0 == 8 ? 20 : 15) : kM2LWarps;
 }
 
-// Warps of a block run in lockstep (a block barrier per batch of 32 sources) so that they
-// execute the same unrolled instructions together and share the fetched instruction lines;
-// targets arrive ordered by their number of batches, so the warps of a block have about
-// the same amount of work.
+// Each warp runs its target's batches of 32 sources on its own; targets arrive ordered by
+// their number of batches, so the warps of a block have about the same amount of work and
+// the block's registers free up together.  (Holding a block's warps in lockstep with a
+// barrier per batch, so that they share fetched instruction lines, measured 3 % slower at
+// P = 10: the warps waited at the barriers.)
 template <typename T, int P, int J0, int J1, int W>
 __global__ void __launch_bounds__(32 * W)
     k_m2l_reg(int ntgt, const int* __restrict__ tgt, const int* __restrict__ off,
               const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
               const T* __restrict__ M, T* __restrict__ L, int ncoef, T cycle) {
   constexpr int NT = sph::NT(P);
-  __shared__ int smax;
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int w = blockIdx.x * W + wl;
-  const int c = w < ntgt ? tgt[w] : 0;
-  const int s0 = w < ntgt ? off[c] : 0, s1 = w < ntgt ? off[c + 1] : 0;
-  const int nbat = (s1 - s0 + 31) >> 5;
-  if (threadIdx.x == 0) smax = 0;
-  __syncthreads();
-  if (lane == 0) atomicMax(&smax, nbat);
-  __syncthreads();
-  const int maxbat = smax;
+  const int lane = lane_id();
+  const int w = blockIdx.x * W + (threadIdx.x >> 5);
+  if (w >= ntgt) return;
+  const int c = tgt[w];
+  const int s0 = off[c], s1 = off[c + 1];
+  if (s1 == s0) return;
   const vec4<T> Xi = cX[c];
   T Lr[NT], Li[NT];
 #pragma unroll
   for (int t = 0; t < NT; t++) Lr[t] = Li[t] = 0;
-  for (int bt = 0; bt < maxbat; bt++) {
-    const int s = s0 + bt * 32 + lane;
+  for (int sb = s0; sb < s1; sb += 32) {
+    const int s = sb + lane;
     if (s < s1) {
       const unsigned src = (unsigned)pairs[s];
       const int j = pair_cell(src);
       T px, py, pz;  // periodic shift of the source (0 without images)
       img_shift<T>(pair_img(src), cycle, px, py, pz);
       const vec4<T> Xj = cX[j];
-      T yr[NT], yi[NT];
+      T rho[NT - sph::sidx(J0, 0)], cr[P], ci[P];
       sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
-      sph::local<T, P>(a, yr, yi);
-      sph::m2l_pair<T, P, J0, J1>(yr, yi, M + (size_t)j * ncoef, Lr, Li);
+      sph::local_rho<T, P, J0>(a, rho, cr, ci);
+      sph::m2l_pair_rot<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
     }
-    __syncthreads();
   }
-  if (nbat == 0) return;
 #pragma unroll
   for (int t = sph::sidx(J0, 0); t < sph::sidx(J1, 0); t++) {
     const T r = warp_sum(Lr[t]);

@@ -126,6 +126,27 @@ def test_solve_matches_oracle_and_direct(name, datasets):
     assert gp < op * 1.05 + 2e-6 and ga < oa * 1.05 + 2e-6, (gp, ga, op, oa)
 
 
+def test_long_list_ranges(datasets):
+    """A small opening angle on leaves of at most two bodies: M2L targets with more than
+    1024 sources (sorted by a block instead of a warp) and P2P targets with more than 8192
+    (left to the global sort); lists bit-exact and results as the oracle's."""
+    x, q = datasets.make("cube", 12000, seed=11, precision="f32")
+    kw = dict(ncrit=2, theta=0.02, use_ropt=0)
+    o = Oracle("f32").run(x, q, P=4, kahan=1, **kw)
+    s = fmm.Solver(P=4, **kw)
+    s.set_bodies(x, q)
+    s.build_tree()
+    s.upward_pass()
+    s.traverse()
+    s.downward_pass()
+    m2l, p2p = s.lists()
+    assert np.bincount(m2l >> 32).max() > 1024 and np.bincount(p2p >> 32).max() > 8192
+    assert np.array_equal(m2l, np.sort(o.m2l()))
+    assert np.array_equal(p2p, np.sort(o.p2p()))
+    pot, acc = rel_l2(s.trg(), o.trg())
+    assert pot < 2e-5 and acc < 2e-5, (pot, acc)
+
+
 @pytest.mark.parametrize("case", ["sph_p6_f64_cube", "sph_p10_f32k_plummer",
                                   "cart_p5_f32_sphere"])
 def test_golden_reference(case, golden_dir):

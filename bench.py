@@ -11,8 +11,10 @@ use_rmax = use_ropt = 1, FP32 expansions with compensated potential/gradient sum
   outside its events.
 * e2e: the same solve through the host C ABI (fmm_b200_solve_host: pinned double x, q in,
   p, f out, host<->device copies inside the timed region).
-* roofline: the M2L kernel (the largest phase), FP32-pipe bound: algorithmic flops
-  8 * sum_{j<P} (j+1)(P-j)^2 per cell pair (= 9,680 at P = 10) over its event-timed duration,
+* roofline: the M2L kernel (the largest phase), FP32-pipe bound: algorithmic flops per cell
+  pair of the contraction in the source's azimuthal frame, 4 * sum_{j<P} (j+1)(P-j)^2 (two
+  real multiply-adds per term) + 6 (P(P+1)/2 - P) (rotating the source) + 8 (P(P+1)/2 - P)
+  + 2 P (rotating the outputs back) = 5,490 at P = 10, over its event-timed duration,
   against the FP32 FMA peak measured on the same GPU by fmm_b200_fp32_peak.
 * cpu_baseline: the reference exafmm-dev CPU FMM (oracle/_ref/perf, compiled from the
   reference's sources) on a bounded sample of the same workload with all host threads.
@@ -48,7 +50,8 @@ REF_SAMPLE_N = 1 << 18            # bodies per reference step (bounded CPU sampl
 
 def m2l_flops_per_pair(P, basis="spherical"):
     if basis == "spherical":
-        return 8 * sum((j + 1) * (P - j) ** 2 for j in range(P))
+        rot = P * (P + 1) // 2 - P
+        return 4 * sum((j + 1) * (P - j) ** 2 for j in range(P)) + 6 * rot + 8 * rot + 2 * P
     # Cartesian: 2 flops per multiply-add of the truncated tensor contraction
     nt = lambda p: p * (p + 1) * (p + 2) // 6
     return 2 * sum(((o + 1) * (o + 2) // 2) * nt(P - o) for o in range(P))

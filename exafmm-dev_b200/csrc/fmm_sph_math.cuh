@@ -318,6 +318,72 @@ __host__ __device__ __forceinline__ void m2l_pair_rot(const T* rho, const T* cr,
     }
 }
 
+// m2l_pair_rot with the loops the other way round: the rotated source coefficients of the
+// degrees n < P - J0 held in registers and each output's sum A[j, k] finished and rotated
+// before the next (the same terms in the same order, so the same results); for the
+// passes of high output degree, which take few source coefficients and many outputs.
+template <typename T, int P, int J0, int J1>
+__host__ __device__ __forceinline__ void m2l_pair_rot_out(const T* rho, const T* cr,
+                                                          const T* ci, const T* Mj, T* Lr,
+                                                          T* Li) {
+  constexpr int O0 = sidx(J0, 0), NIN = sidx(P - J0, 0);
+  T Mr[NIN], Mi[NIN];
+#pragma unroll
+  for (int n = 0; n < P - J0; n++)
+#pragma unroll
+    for (int mu = 0; mu <= n; mu++) {
+      T mr, mi;
+      load_pair(Mj + 2 * sidx(n, mu), mr, mi);
+      if (mu > 0) {
+        const T r = mr * cr[mu] - mi * ci[mu];
+        mi = mr * ci[mu] + mi * cr[mu];
+        mr = r;
+      }
+      Mr[sidx(n, mu)] = mr;
+      Mi[sidx(n, mu)] = mi;
+    }
+#pragma unroll
+  for (int j = J0; j < J1; j++) {
+    const bool oj = (j & 1) != 0;
+#pragma unroll
+    for (int k = 0; k <= j; k++) {
+      T ar = T(0), ai = T(0);
+#pragma unroll
+      for (int n = 0; n < P - j; n++) {
+        const int a = j + n;
+#pragma unroll
+        for (int mu = 0; mu <= n; mu++) {
+          const T mr = Mr[sidx(n, mu)], mi = Mi[sidx(n, mu)];
+          if (mu == 0) {
+            const T p = rho[sidx(a, k) - O0];
+            const T ps = oj ? -p : p;
+            ar = fma(ps, mr, ar);
+            ai = fma(ps, mi, ai);
+          } else {
+            const T p1 = rho[sidx(a, k + mu) - O0];
+            const T s1 = oj ? -p1 : p1;
+            ar = fma(s1, mr, ar);
+            ai = fma(-s1, mi, ai);
+            const T p2 = rho[sidx(a, mu >= k ? mu - k : k - mu) - O0];
+            const bool o2 = oj != (((k < mu ? k : mu) & 1) != 0);
+            const T s2 = o2 ? -p2 : p2;
+            ar = fma(s2, mr, ar);
+            ai = fma(s2, mi, ai);
+          }
+        }
+      }
+      const int g = sidx(j, k);
+      if (k == 0) {
+        Lr[g] += ar;
+        Li[g] += ai;
+      } else {
+        Lr[g] = fma(cr[k], ar, fma(ci[k], ai, Lr[g]));
+        Li[g] = fma(cr[k], ai, fma(-ci[k], ar, Li[g]));
+      }
+    }
+  }
+}
+
 // Y[a, b] for any sign of b from the m >= 0 store (real parts yr, imaginary parts yi)
 template <typename T>
 __host__ __device__ __forceinline__ void yget(const T* yr, const T* yi, int a, int b, T& r,

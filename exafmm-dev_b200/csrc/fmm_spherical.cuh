@@ -317,29 +317,40 @@ __global__ void __launch_bounds__(kTrThreads)
 // one warp reduction per target cell at the end.  Each pair is contracted in the source's
 // azimuthal frame (m2l_pair_rot: real harmonic factors, half the multiply-adds of the
 // complex form).  The outputs are split into passes over their degree (separate launches)
-// so that each pass's registers stay within one block of 15-20 warps per SM.
+// so that each pass's registers stay within one block of 12 warps per SM.
 constexpr int kM2LWarps = 12;
-// output degrees per FP32 M2L pass: add degrees while the pass's registers (the real
-// harmonic factors of degrees >= J0, and four per output: the pair's rotated sum and the
-// accumulator, real and imaginary) stay under ~110
+// FP32 M2L passes over the output degrees.  Registers of a pass [J0, J1) (besides the
+// phases e^(i m beta)): the real harmonic factors of degrees >= J0, the accumulators (two
+// per output), and either the pair's rotated sums A (two per output: source coefficients
+// streamed, m2l_pair_rot) or the rotated source coefficients of degrees < P - J0 (two per
+// coefficient: outputs streamed, m2l_pair_rot_out).  The last pass streams its outputs
+// once the remaining degrees fit kM2LOutRegs; the passes before it stream the source and
+// add degrees while they fit kM2LInRegs.
+constexpr int kM2LInRegs = 115, kM2LOutRegs = 150;
+__host__ __device__ constexpr int m2l_regs_out(int P, int J0) {
+  return sph::NT(P) - sph::sidx(J0, 0) + 2 * (sph::NT(P) - sph::sidx(J0, 0)) +
+         2 * sph::NT(P - J0);
+}
+__host__ __device__ constexpr bool m2l_pass_out(int P, int J0) {
+  return m2l_regs_out(P, J0) <= kM2LOutRegs;
+}
 __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
+  if (m2l_pass_out(P, J0)) return P;
   const int rho = sph::NT(P) - sph::sidx(J0, 0);
   int j = J0, outs = 0;
   while (j < P) {
     const int o = outs + j + 1;
-    if (j > J0 && rho + 4 * o > 110) break;
+    if (j > J0 && (rho + 4 * o > kM2LInRegs || m2l_pass_out(P, j))) break;
     outs = o;
     j++;
   }
   return j;
 }
 
-// warps per block of one FP32 M2L pass: as many as the pass's registers allow in one block
-// per SM without spilling (P = 10: 128, 134, 135 and 98 registers for the passes starting
-// at degrees 0, 4, 6 and 8)
-__host__ __device__ constexpr int m2l_pass_warps(int P, int J0) {
-  return P == 10 ? (J0 == 0 ? 16 : J0 == 8 ? 20 : 15) : kM2LWarps;
-}
+// warps per block of one FP32 M2L pass: 12 (3 per SM sub-partition, whose 16 K registers
+// then allow 168 per thread; P = 10 takes the passes [0, 5) and [5, 10), at 168 registers
+// each, the second with a small spill)
+__host__ __device__ constexpr int m2l_pass_warps(int, int) { return kM2LWarps; }
 
 // Each warp runs its target's batches of 32 sources on its own; targets arrive ordered by
 // their number of batches, so the warps of a block have about the same amount of work and
@@ -373,7 +384,10 @@ __global__ void __launch_bounds__(32 * W)
       T rho[NT - sph::sidx(J0, 0)], cr[P], ci[P];
       sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
       sph::local_rho<T, P, J0>(a, rho, cr, ci);
-      sph::m2l_pair_rot<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
+      if constexpr (m2l_pass_out(P, J0))
+        sph::m2l_pair_rot_out<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
+      else
+        sph::m2l_pair_rot<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
     }
   }
 #pragma unroll

@@ -342,11 +342,14 @@ __host__ __device__ __forceinline__ void m2l_pair_rot_out(const T* rho, const T*
       Mr[sidx(n, mu)] = mr;
       Mi[sidx(n, mu)] = mi;
     }
+  // outputs by order k, then degree: e^(i k beta) advances by one rotation per k, so the
+  // phases need not stay live in registers
+  T er = T(1), ei = T(0);
 #pragma unroll
-  for (int j = J0; j < J1; j++) {
-    const bool oj = (j & 1) != 0;
+  for (int k = 0; k < J1; k++) {
 #pragma unroll
-    for (int k = 0; k <= j; k++) {
+    for (int j = (k > J0 ? k : J0); j < J1; j++) {
+      const bool oj = (j & 1) != 0;
       T ar = T(0), ai = T(0);
 #pragma unroll
       for (int n = 0; n < P - j; n++) {
@@ -377,10 +380,13 @@ __host__ __device__ __forceinline__ void m2l_pair_rot_out(const T* rho, const T*
         Lr[g] += ar;
         Li[g] += ai;
       } else {
-        Lr[g] = fma(cr[k], ar, fma(ci[k], ai, Lr[g]));
-        Li[g] = fma(cr[k], ai, fma(-ci[k], ar, Li[g]));
+        Lr[g] = fma(er, ar, fma(ei, ai, Lr[g]));
+        Li[g] = fma(er, ai, fma(-ei, ar, Li[g]));
       }
     }
+    const T tt = er * cr[1] - ei * ci[1];
+    ei = er * ci[1] + ei * cr[1];
+    er = tt;
   }
 }
 

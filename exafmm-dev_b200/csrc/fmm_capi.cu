@@ -407,7 +407,8 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
                          &s.nnode,    &s.npos,     &s.ncb,      &s.nlevel,  &s.nsplit,     \
                          &s.coff,     &s.leaves,   &s.idx,      &s.idx2,    &s.scal,       \
                          &s.c_iparent, &s.c_ichild, &s.c_nchild, &s.c_ibody, &s.c_nbody,   \
-                         &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off, &s.seg_cnt};   \
+                         &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off, &s.seg_cnt,    \
+                         &s.d_lvl};                                                        \
     for (auto* a : ia) a->release();                                                       \
     s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
     s.p2p.release(); s.list_tmp.release(); s.p2p_pairs_count.release();                   \

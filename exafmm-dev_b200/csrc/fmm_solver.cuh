@@ -106,6 +106,8 @@ struct SolverBase {
   DevArr<int> fs_idx;
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
+  int tree_plan = 0;        // levels of the handle's last tree (0: none; builds level by level)
+  DevArr<int> d_lvl;        // level ends of the planned node build
   // targets and sources in two trees (segments 0 and 1) on a common box, traversed from
   // (target root, source root) only (fmm_b200_solve_ij_*)
   bool ij = false;

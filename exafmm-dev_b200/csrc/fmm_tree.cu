@@ -12,6 +12,8 @@
 // cell contiguous, each child's subtree after the previous child's.
 #include <cfloat>
 
+#include <climits>
+
 #include "fmm_solver.cuh"
 
 namespace fmmb200 {
@@ -173,20 +175,16 @@ __global__ void k_roots(int nroots, const int* __restrict__ root_first, const T*
 
 // One level of BuildNodes (include/build_tree_tbb.h:165-218): a node with more than ncrit
 // bodies gets one child per non-empty octant; octant boundaries by binary search.
-__global__ void k_split(int lo, int hi, int level, int ncrit,
-                        const unsigned long long* __restrict__ keys,
-                        const int* __restrict__ nbegin, const int* __restrict__ ncount,
-                        int* __restrict__ cnt, int* __restrict__ starts) {
-  // one warp per node: the 7 octant boundaries of its sorted key range are found together
-  // by 32-ary searches (32 samples per boundary and round, all loads of a round
-  // independent), so a node of c bodies needs log32(c) dependent rounds instead of the
-  // 7 log2(c) of a binary search per boundary
-  const int lane = lane_id();
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int m = hi - lo;
-  if (w == m && lane == 0) cnt[m] = 0;
-  if (w >= m) return;
-  const int v = lo + (int)w;
+// One warp per node: the 7 octant boundaries of its sorted key range are found together by
+// 32-ary searches (32 samples per boundary and round, all loads of a round independent), so
+// a node of c bodies needs log32(c) dependent rounds instead of the 7 log2(c) of a binary
+// search per boundary.  Node w of the level (v = lo + w): child count into cnt[w], octant
+// starts into starts[9 w ..].
+__device__ __forceinline__ void split_node(int lane, int w, int v, int level, int ncrit,
+                                           const unsigned long long* __restrict__ keys,
+                                           const int* __restrict__ nbegin,
+                                           const int* __restrict__ ncount,
+                                           int* __restrict__ cnt, int* __restrict__ starts) {
   const int b = nbegin[v], c = ncount[v];
   int nch = 0;
   if (c > ncrit && level < kMaxLevel) {
@@ -246,15 +244,49 @@ __global__ void k_split(int lo, int hi, int level, int ncrit,
   if (lane == 0) cnt[w] = nch;
 }
 
+__global__ void k_split(int lo, int hi, int level, int ncrit,
+                        const unsigned long long* __restrict__ keys,
+                        const int* __restrict__ nbegin, const int* __restrict__ ncount,
+                        int* __restrict__ cnt, int* __restrict__ starts) {
+  const int lane = lane_id();
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int m = hi - lo;
+  if (w == m && lane == 0) cnt[m] = 0;
+  if (w >= m) return;
+  split_node(lane, (int)w, lo + (int)w, level, ncrit, keys, nbegin, ncount, cnt, starts);
+}
+
+// k_split with the level's node range read on the device (lvl[level], lvl[level + 1]) for
+// the planned build: a grid-stride loop over the nodes, counts past the level's nodes zeroed
+// up to mcap (the size of the scan that follows); a level of more than mcap nodes flags
+// overflow and is not split.
+__global__ void k_split_planned(const int* __restrict__ lvl, int level, int ncrit, int mcap,
+                                const unsigned long long* __restrict__ keys,
+                                const int* __restrict__ nbegin, const int* __restrict__ ncount,
+                                int* __restrict__ cnt, int* __restrict__ starts,
+                                int* __restrict__ overflow) {
+  const int lane = lane_id();
+  const int lo = lvl[level], m = lvl[level + 1] - lo;
+  const int mm = m <= mcap ? m : 0;
+  if (m > mcap && blockIdx.x == 0 && threadIdx.x == 0) atomicExch(overflow, 1);
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w <= mcap; w += nw) {
+    if (w < mm) split_node(lane, (int)w, lo + (int)w, level, ncrit, keys, nbegin, ncount, cnt, starts);
+    else if (lane == 0) cnt[w] = 0;
+  }
+}
+
+// the children of node t of the level (v = lo + t), from hi + coff[t] on
 template <typename T>
-__global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
-                       const int* __restrict__ coff, const int* __restrict__ starts,
-                       const T* __restrict__ box, int* __restrict__ nbegin,
-                       int* __restrict__ ncount, int* __restrict__ nparent,
-                       int* __restrict__ nchildn, int* __restrict__ nfirst,
-                       int* __restrict__ nlevel, int* __restrict__ nsid, T* __restrict__ nX) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= hi - lo) return;
+__device__ __forceinline__ void emit_node(int t, int lo, int hi, int level,
+                                          const int* __restrict__ cnt,
+                                          const int* __restrict__ coff,
+                                          const int* __restrict__ starts,
+                                          const T* __restrict__ box, int* __restrict__ nbegin,
+                                          int* __restrict__ ncount, int* __restrict__ nparent,
+                                          int* __restrict__ nchildn, int* __restrict__ nfirst,
+                                          int* __restrict__ nlevel, int* __restrict__ nsid,
+                                          T* __restrict__ nX) {
   int v = lo + t;
   int nch = cnt[t];
   nchildn[v] = nch;
@@ -282,6 +314,44 @@ __global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
     nX[4 * u + 2] = add_rn(X2, (o & 4) ? r : -r);
     nX[4 * u + 3] = 0;
   }
+}
+
+template <typename T>
+__global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
+                       const int* __restrict__ coff, const int* __restrict__ starts,
+                       const T* __restrict__ box, int* __restrict__ nbegin,
+                       int* __restrict__ ncount, int* __restrict__ nparent,
+                       int* __restrict__ nchildn, int* __restrict__ nfirst,
+                       int* __restrict__ nlevel, int* __restrict__ nsid, T* __restrict__ nX) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi - lo) return;
+  emit_node<T>(t, lo, hi, level, cnt, coff, starts, box, nbegin, ncount, nparent, nchildn,
+               nfirst, nlevel, nsid, nX);
+}
+
+// k_emit of the planned build: the level's range and its child total (coff[m]) read on the
+// device; the next level's end is written to lvl[level + 2]; children that would not fit
+// the node arrays (ncap) flag overflow and are not emitted.
+template <typename T>
+__global__ void k_emit_planned(int* __restrict__ lvl, int level, int ncap,
+                               const int* __restrict__ cnt, const int* __restrict__ coff,
+                               const int* __restrict__ starts, const T* __restrict__ box,
+                               int* __restrict__ nbegin, int* __restrict__ ncount,
+                               int* __restrict__ nparent, int* __restrict__ nchildn,
+                               int* __restrict__ nfirst, int* __restrict__ nlevel,
+                               int* __restrict__ nsid, T* __restrict__ nX,
+                               int* __restrict__ overflow) {
+  const int lo = lvl[level], hi = lvl[level + 1], m = hi - lo;
+  const int total = m > 0 ? coff[m] : 0;
+  const bool fits = (long long)hi + total <= ncap && *overflow == 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    lvl[level + 2] = fits ? hi + total : hi;
+    if (!fits) atomicExch(overflow, 1);
+  }
+  if (!fits) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x)
+    emit_node<T>(t, lo, hi, level, cnt, coff, starts, box, nbegin, ncount, nparent, nchildn,
+                 nfirst, nlevel, nsid, nX);
 }
 
 // leaf nodes: chain-less nodes at the deepest level of the last pass
@@ -470,6 +540,56 @@ static void forest_sort(Solver<T>& s, const unsigned long long* kin, unsigned lo
   FMM_LAUNCH_CHECK();
 }
 
+// The levels of the node build without a host round trip per level, for a handle whose
+// previous tree had s.tree_plan levels: tree_plan + 1 levels of k_split_planned, a scan of
+// the counts and k_emit_planned run back to back with the level ranges kept on the device,
+// then one read of the ranges.  Returns false (and the levels are built again level by
+// level) if the node arrays overflowed or the tree went deeper than planned.
+template <typename T>
+static bool planned_levels(Solver<T>& s, int nroots, DevArr<int>** narr, int nnarr) {
+  const int TB = 256;
+  const int L = s.tree_plan + 1;
+  size_t cap = s.nX.cap / 4;
+  for (int i = 0; i < nnarr; i++) cap = std::min(cap, narr[i]->cap);
+  const int ncap = (int)std::min<size_t>(cap, INT_MAX / 16);
+  const int mcap = ncap;  // a level holds no more nodes than the arrays
+  s.nsplit.ensure(9 * (size_t)(mcap + 1));
+  s.coff.ensure((size_t)mcap + 2);
+  s.idx.ensure(std::max((size_t)s.n, (size_t)mcap + 1));
+  s.d_lvl.ensure(L + 2);
+  int* cnt = s.idx.p;
+  int* lvl = s.d_lvl.p;
+  int* ovf = (int*)((unsigned long long*)s.scal.p + 6);
+  int* hl = s.scal_host + 400;  // pinned: L + 2 level ends, then the overflow flag
+  if (L + 3 > 512 - 400) return false;
+  hl[0] = 0;
+  hl[1] = nroots;
+  FMM_CUDA(cudaMemcpyAsync(lvl, hl, 2 * sizeof(int), cudaMemcpyHostToDevice, s.stream));
+  FMM_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int), s.stream));
+  const int gs = (int)std::min<long long>(ceil_div(32LL * (mcap + 1), TB), 148 * 16);
+  const int ge = (int)std::min<long long>(ceil_div((long long)mcap, TB), 148 * 8);
+  for (int level = 0; level < L; level++) {
+    k_split_planned<<<gs, TB, 0, s.stream>>>(lvl, level, s.cfg.ncrit, mcap, s.keys2.p,
+                                              s.nbegin.p, s.ncount.p, cnt, s.nsplit.p, ovf);
+    FMM_LAUNCH_CHECK();
+    exclusive_sum_int(s, cnt, s.coff.p, mcap + 1);
+    k_emit_planned<T><<<ge, TB, 0, s.stream>>>(lvl, level, ncap, cnt, s.coff.p, s.nsplit.p,
+                                               s.box.p, s.nbegin.p, s.ncount.p, s.nparent.p,
+                                               s.nchildn.p, s.nfirst.p, s.nlevel.p, s.nsid.p,
+                                               s.nX.p, ovf);
+    FMM_LAUNCH_CHECK();
+  }
+  FMM_CUDA(cudaMemcpyAsync(hl, lvl, (L + 2) * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  FMM_CUDA(cudaMemcpyAsync(hl + L + 2, ovf, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  if (hl[L + 2] != 0 || hl[L + 1] != hl[L]) return false;
+  // levels 0 .. d, d the first level without children
+  int d = 0;
+  while (hl[d + 2] != hl[d + 1]) d++;
+  s.level_lo.assign(hl, hl + d + 2);
+  return true;
+}
+
 template <typename T> void build_tree(Solver<T>& s) {
   const int n = s.n;
   const int TB = 256;
@@ -544,7 +664,8 @@ template <typename T> void build_tree(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
   s.level_lo.push_back(0);
   s.level_lo.push_back(nroots);
-  for (int level = 0;; level++) {
+  const bool planned = s.tree_plan > 0 && planned_levels(s, nroots, narr, sizeof(narr) / sizeof(*narr));
+  for (int level = 0; !planned; level++) {
     int lo = s.level_lo[level], hi = s.level_lo[level + 1];
     int m = hi - lo;
     s.nsplit.ensure(9 * (size_t)m);
@@ -576,6 +697,7 @@ template <typename T> void build_tree(Solver<T>& s) {
   }
   const int nlev = (int)s.level_lo.size() - 1;
   const int nnodes = s.level_lo.back();
+  s.tree_plan = nlev;
   s.maxlevel = nlev - 1;
   s.ncells = nnodes;
   for (int l = nlev - 1; l >= 0; l--) {

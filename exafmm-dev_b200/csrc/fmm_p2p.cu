@@ -5,12 +5,14 @@
 // small leaf still keeps the warp busy: each group holds one target body and its G lanes
 // take every G-th source; a leaf of 33..64 bodies gives each lane two targets that share
 // every staged source.  Source leaves stream through shared memory 32 bodies at a time
-// (one coalesced 16-byte load per lane, read back as a broadcast), the inner loop is
-// FP32 FMA + one rsqrt per pair (no r^2 == 0 test outside the target leaf itself), and
-// each source leaf's plain FP32 partial sum is folded into a compensated (TwoSum)
-// accumulator, so the accumulation error does not grow with the number of source leaves.  Pairs with r^2 == 0 are skipped, as the reference does
-// (:149); the result is per unit target charge (the reference multiplies by q_i in P2P
-// and divides again in L2P / normalize).
+// (one coalesced 16-byte load per lane); in FP32 the staged sources are taken two at a time
+// with the packed two-wide instructions of sm_100 (half the issue slots of the scalar pair
+// arithmetic).  The inner loop is FMA + one rsqrt per pair (no r^2 == 0 test outside the
+// target leaf itself), and each source leaf's plain partial sum is folded into a
+// compensated (TwoSum) accumulator, so the accumulation error does not grow with the number
+// of source leaves.  Pairs with r^2 == 0 are skipped, as the reference does (:149); the
+// result is per unit target charge (the reference multiplies by q_i in P2P and divides
+// again in L2P / normalize).
 #include <algorithm>
 
 #include "fmm_solver.cuh"
@@ -51,6 +53,81 @@ __device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, 
   az = fma(dz, inv3, az);
 }
 
+// FP32 source leaf: the staged sources are taken two at a time with the packed two-wide
+// instructions of sm_100 (add.f32x2, mul.f32x2, fma.f32x2: one instruction for both, each
+// component rounded as the scalar operation, so each pair's terms are those of p2p_accum);
+// a target's two partial sums are added at the end of the leaf.  The warp's row holds
+// A[i] = (x, x', y, y') and B[i] = (z, z', q, q') for the sources 2i and 2i + 1; a missing
+// partner is a far-away zero charge, which adds exactly zero.
+template <int TPL, bool EXACT, bool SHIFT>
+__device__ __forceinline__ void source_leaf_pairs(int lane, float4* row, int sub, int G, int j0,
+                                                  int nj, const vec4<float>* __restrict__ bodies,
+                                                  float eps2, const vec4<float>* xi, float* pot,
+                                                  float* ax, float* ay, float* az, float px,
+                                                  float py, float pz) {
+  float4* A = row;
+  float4* B = row + 16;
+  float2 nx[TPL], ny[TPL], nz[TPL], sp[TPL], sx[TPL], sy[TPL], sz[TPL];
+#pragma unroll
+  for (int u = 0; u < TPL; u++) {
+    nx[u] = make_float2(-xi[u].x, -xi[u].x);
+    ny[u] = make_float2(-xi[u].y, -xi[u].y);
+    nz[u] = make_float2(-xi[u].z, -xi[u].z);
+    sp[u] = sx[u] = sy[u] = sz[u] = make_float2(0.f, 0.f);
+  }
+  const float2 e2 = make_float2(eps2, eps2);
+  const float2 p2x = make_float2(px, px), p2y = make_float2(py, py), p2z = make_float2(pz, pz);
+  for (int jb = 0; jb < nj; jb += 32) {
+    const int cnt = min(32, nj - jb);
+    __syncwarp();
+    {
+      const vec4<float> b =
+          lane < cnt ? bodies[j0 + jb + lane] : make_v4<float>(1e30f, 1e30f, 1e30f, 0.f);
+      float* a = reinterpret_cast<float*>(&A[lane >> 1]);
+      float* c = reinterpret_cast<float*>(&B[lane >> 1]);
+      const int h = lane & 1;
+      a[h] = b.x;
+      a[2 + h] = b.y;
+      c[h] = b.z;
+      c[2 + h] = b.w;
+    }
+    __syncwarp();
+    const int np = (cnt + 1) >> 1;
+#pragma unroll 2
+    for (int i = sub; i < np; i += G) {
+      const float4 a = A[i], c = B[i];
+      const float2 x2 = make_float2(a.x, a.y), y2 = make_float2(a.z, a.w);
+      const float2 z2 = make_float2(c.x, c.y), q2 = make_float2(c.z, c.w);
+#pragma unroll
+      for (int u = 0; u < TPL; u++) {
+        float2 dx = __fadd2_rn(x2, nx[u]), dy = __fadd2_rn(y2, ny[u]), dz = __fadd2_rn(z2, nz[u]);
+        if (SHIFT) {
+          dx = __fadd2_rn(dx, p2x);
+          dy = __fadd2_rn(dy, p2y);
+          dz = __fadd2_rn(dz, p2z);
+        }
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+        float2 inv;
+        inv.x = EXACT ? (r2.x > 0.f ? rsqrt_(r2.x) : 0.f) : rsqrt_ftz(r2.x);
+        inv.y = EXACT ? (r2.y > 0.f ? rsqrt_(r2.y) : 0.f) : rsqrt_ftz(r2.y);
+        const float2 qinv = __fmul2_rn(q2, inv);
+        const float2 inv3 = __fmul2_rn(__fmul2_rn(qinv, inv), inv);
+        sp[u] = __fadd2_rn(sp[u], qinv);
+        sx[u] = __ffma2_rn(dx, inv3, sx[u]);
+        sy[u] = __ffma2_rn(dy, inv3, sy[u]);
+        sz[u] = __ffma2_rn(dz, inv3, sz[u]);
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < TPL; u++) {
+    pot[u] = sp[u].x + sp[u].y;
+    ax[u] = sx[u].x + sx[u].y;
+    ay[u] = sy[u].x + sy[u].y;
+    az[u] = sz[u].x + sz[u].y;
+  }
+}
+
 // all bodies of one source leaf (first body j0, nj bodies) on the lane's TPL targets, its
 // sums started from zero; sources are staged through the warp's shared row 32 at a time
 template <typename T, int TPL, bool EXACT, bool SHIFT = false>
@@ -58,6 +135,10 @@ __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32],
                                             int j0, int nj, const vec4<T>* __restrict__ bodies,
                                             T eps2, const vec4<T>* xi, T* pot, T* ax, T* ay,
                                             T* az, T px = 0, T py = 0, T pz = 0) {
+  if constexpr (sizeof(T) == 4) {
+    source_leaf_pairs<TPL, EXACT, SHIFT>(lane, reinterpret_cast<float4*>(sh[wl]), sub, G, j0,
+                                         nj, bodies, eps2, xi, pot, ax, ay, az, px, py, pz);
+  } else {
 #pragma unroll
   for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
   for (int jb = 0; jb < nj; jb += 32) {
@@ -72,6 +153,7 @@ __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32],
       for (int u = 0; u < TPL; u++)
         p2p_accum<T, EXACT, SHIFT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u], px, py, pz);
     }
+  }
   }
 }
 

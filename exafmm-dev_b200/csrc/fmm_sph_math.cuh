@@ -57,7 +57,8 @@ template <typename T> __host__ __device__ __forceinline__ Angles<T> angles(T dx,
 }
 
 // evalMultipole (:29-65) without the theta derivative: Y[n, m] = rho^n P_n^m e^(i m beta)
-// / (-1)^n (n + m)!-style normalisation of the reference.
+// / (-1)^n (n + m)!-style normalisation of the reference; its divisions by -(n + m) and
+// (2m + 2)(2m + 1) are multiplications by the reciprocals here.
 template <typename T, int P>
 __host__ __device__ __forceinline__ void multipole(const Angles<T>& a, T rho, T* yr, T* yi) {
   T fact = 1, pn = 1, rhom = 1;
@@ -73,7 +74,7 @@ __host__ __device__ __forceinline__ void multipole(const Angles<T>& a, T rho, T*
     T rhon = rhom;
 #pragma unroll
     for (int n = m + 1; n < P; n++) {
-      rhon /= -(n + m);
+      rhon *= T(-1) / T(n + m);
       yr[sidx(n, m)] = rhon * p * er;
       yi[sidx(n, m)] = rhon * p * ei;
       T p2 = p1;
@@ -81,7 +82,7 @@ __host__ __device__ __forceinline__ void multipole(const Angles<T>& a, T rho, T*
       p = (a.x * (2 * n + 1) * p1 - (n + m) * p2) * (T(1) / T(n - m + 1));
       rhon *= rho;
     }
-    rhom /= -(2 * m + 2) * (2 * m + 1);
+    rhom *= T(-1) / T((2 * m + 2) * (2 * m + 1));
     pn = -pn * fact * a.y;
     fact += 2;
     T t = er * a.cb - ei * a.sb;
@@ -522,8 +523,10 @@ __host__ __device__ __forceinline__ void l2l_range(const T* yr, const T* yi, con
 template <typename T, int P>
 __host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, T& pot, T& gx,
                                                   T& gy, T& gz) {
+  // the divisions of the reference (by rho per term, by -(n+m) and (2m+2)(2m+1) per
+  // step) are multiplications by reciprocals here: one division per body
   Angles<T> a = angles(dx, dy, dz);
-  const T rho = a.r;
+  const T rho = a.r, invrho = T(1) / rho;
   T s0 = 0, s1 = 0, s2 = 0, ph = 0;
   T fact = 1, pn = 1, rhom = 1;
   T er = 1, ei = 0;
@@ -541,7 +544,7 @@ __host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, 
       const T Lr = L[2 * sidx(m, m)], Li = L[2 * sidx(m, m) + 1];
       const T re = Lr * er - Li * ei, im = Lr * ei + Li * er;  // L * e^(i m beta)
       ph += w * yv * re;
-      s0 += w * yv * re / rho * m;
+      s0 += w * yv * re * invrho * m;
       s1 += w * tv * re;
       s2 -= w * yv * im * m;
     }
@@ -549,7 +552,7 @@ __host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, 
     T rhon = rhom;
 #pragma unroll
     for (int n = m + 1; n < P; n++) {
-      rhon /= -(n + m);
+      rhon *= T(-1) / T(n + m);
       const T yv = rhon * p;
       T p2 = p1;
       p1 = p;
@@ -558,12 +561,12 @@ __host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, 
       const T Lr = L[2 * sidx(n, m)], Li = L[2 * sidx(n, m) + 1];
       const T re = Lr * er - Li * ei, im = Lr * ei + Li * er;
       ph += w * yv * re;
-      s0 += w * yv * re / rho * n;
+      s0 += w * yv * re * invrho * n;
       s1 += w * tv * re;
       s2 -= w * yv * im * m;
       rhon *= rho;
     }
-    rhom /= -(2 * m + 2) * (2 * m + 1);
+    rhom *= T(-1) / T((2 * m + 2) * (2 * m + 1));
     pn = -pn * fact * a.y;
     fact += 2;
     T t = er * a.cb - ei * a.sb;
@@ -572,9 +575,9 @@ __host__ __device__ __forceinline__ void l2p_body(T dx, T dy, T dz, const T* L, 
   }
   // sph2cart (:17-26)
   pot = ph;
-  gx = a.y * a.cb * s0 + a.x * a.cb / rho * s1 - a.sb / rho * invy * s2;
-  gy = a.y * a.sb * s0 + a.x * a.sb / rho * s1 + a.cb / rho * invy * s2;
-  gz = a.x * s0 - a.y / rho * s1;
+  gx = a.y * a.cb * s0 + a.x * a.cb * invrho * s1 - a.sb * invrho * invy * s2;
+  gy = a.y * a.sb * s0 + a.x * a.sb * invrho * s1 + a.cb * invrho * invy * s2;
+  gz = a.x * s0 - a.y * invrho * s1;
 }
 
 }  // namespace sph

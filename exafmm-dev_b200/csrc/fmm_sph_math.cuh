@@ -56,6 +56,39 @@ template <typename T> __host__ __device__ __forceinline__ Angles<T> angles(T dx,
   return a;
 }
 
+// 1 / sqrt(v): the device's reciprocal square root (rsqrtf, rsqrt), the quotient on the host
+template <typename T> __host__ __device__ __forceinline__ T hrsqrt(T v) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(T) == 4) return rsqrtf(v);
+  else return rsqrt(v);
+#else
+  return T(1) / std::sqrt(v);
+#endif
+}
+
+// angles() for an offset of nonzero length with reciprocal square roots instead of two
+// square roots and two divisions (r = r^2 / sqrt(r^2)); invr = 1 / r.  For the M2L pairs,
+// whose cells are well separated.
+template <typename T>
+__host__ __device__ __forceinline__ Angles<T> angles_rs(T dx, T dy, T dz, T& invr) {
+  Angles<T> a;
+  const T rxy2 = dx * dx + dy * dy, r2 = rxy2 + dz * dz;
+  invr = hrsqrt(r2);
+  a.r = r2 * invr;
+  a.x = dz * invr;
+  if (rxy2 > T(0)) {
+    const T ixy = hrsqrt(rxy2);
+    a.y = rxy2 * ixy * invr;
+    a.cb = dx * ixy;
+    a.sb = dy * ixy;
+  } else {
+    a.y = T(0);
+    a.cb = dx < T(0) ? T(-1) : T(1);
+    a.sb = T(0);
+  }
+  return a;
+}
+
 // evalMultipole (:29-65) without the theta derivative: Y[n, m] = rho^n P_n^m e^(i m beta)
 // / (-1)^n (n + m)!-style normalisation of the reference; its divisions by -(n + m) and
 // (2m + 2)(2m + 1) are multiplications by the reciprocals here.
@@ -217,12 +250,13 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* yr, const T* yi, cons
 }
 
 // The local harmonics split into a real factor and an azimuthal phase: Y[n, m] =
-// rho[n, m] e^(i m beta) for m >= 0 (rho = the t of local(), the same arithmetic).  rho is
-// stored for the degrees n >= A0 only, at sidx(n, m) - sidx(A0, 0); (cr[m], ci[m]) =
-// e^(i m beta) for m < P.
+// rho[n, m] e^(i m beta) for m >= 0 (rho = the t of local(), the same arithmetic given
+// invr = 1 / r).  rho is stored for the degrees n >= A0 only, at sidx(n, m) - sidx(A0, 0);
+// (cr[m], ci[m]) = e^(i m beta) for m < P.
 template <typename T, int P, int A0>
-__host__ __device__ __forceinline__ void local_rho(const Angles<T>& a, T* rho, T* cr, T* ci) {
-  const T ninvr = -T(1) / a.r;
+__host__ __device__ __forceinline__ void local_rho(const Angles<T>& a, T invr, T* rho, T* cr,
+                                                   T* ci) {
+  const T ninvr = -invr;
   T fact = 1, pn = 1;
   T rpm = -ninvr;  // (-1)^m / r^(m+1)
   T er = 1, ei = 0;

@@ -382,8 +382,10 @@ __global__ void __launch_bounds__(32 * W)
       img_shift<T>(pair_img(src), cycle, px, py, pz);
       const vec4<T> Xj = cX[j];
       T rho[NT - sph::sidx(J0, 0)], cr[P], ci[P];
-      sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
-      sph::local_rho<T, P, J0>(a, rho, cr, ci);
+      T invr;
+      sph::Angles<T> a =
+          sph::angles_rs(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz, invr);
+      sph::local_rho<T, P, J0>(a, invr, rho, cr, ci);
       if constexpr (m2l_pass_out(P, J0))
         sph::m2l_pair_rot_out<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
       else

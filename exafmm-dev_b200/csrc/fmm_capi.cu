@@ -180,15 +180,18 @@ template <typename T> void stage_down(Solver<T>& s) {
   phase_end(s, FMM_PHASE_TOTAL);
   s.stage = ST_DOWN;
 }
-// A whole solve: the stages in order, except that the L2L levels run on a high-priority
-// side stream while P2P runs (from the end of M2L to the start of L2P).  The L2L levels
-// have few cells each and long dependent chains per cell, so alone they leave most of the
-// GPU idle; with the higher priority their blocks start as soon as SMs free up among the
-// P2P blocks.  The results are the same: P2P writes only the bodies' sums, L2L only the
-// local expansions, and L2P runs after both.
+// A whole solve: the stages in order, with two overlaps on a high-priority side stream.
+// (1) Spherical basis: the expansions of the upward pass (P2M, M2M) run on the side stream
+// while the main stream sets the cell radii in a pass of their own (structure_pass: the
+// same radii, monopoles and error-optimised radii as the expansion kernels would set) and
+// runs the traversal, which needs the radii but not the expansions; M2L waits for both.
+// (2) The L2L levels run on the side stream while P2P runs (from the end of M2L to the
+// start of L2P).  The L2L levels have few cells each and long dependent chains per cell, so
+// alone they leave most of the GPU idle; with the higher priority their blocks start as
+// soon as SMs free up.  The results are the same as stage by stage: P2P writes only the
+// bodies' sums, L2L only the local expansions, and L2P runs after both.
 template <typename T> void solve_all(Solver<T>& s) {
   stage_tree(s);
-  stage_up(s);
   if (!s.side) {
     int lo = 0, hi = 0;
     FMM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -196,16 +199,42 @@ template <typename T> void solve_all(Solver<T>& s) {
     FMM_CUDA(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
     FMM_CUDA(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
   }
-  phase_begin(s, FMM_PHASE_TRAVERSE);
-  build_lists(s);
-  phase_end(s, FMM_PHASE_TRAVERSE);
+  cudaStream_t main = s.stream;
+  if (s.cfg.basis == FMM_SPHERICAL && s.ncells > 0) {
+    FMM_CUDA(cudaEventRecord(s.fork, s.stream));
+    FMM_CUDA(cudaStreamWaitEvent(s.side, s.fork, 0));
+    s.stream = s.side;
+    s.write_r = 0;
+    try {
+      phase_begin(s, FMM_PHASE_UPWARD);
+      upward_expansions(s);
+      phase_end(s, FMM_PHASE_UPWARD);
+      FMM_CUDA(cudaEventRecord(s.join, s.stream));
+    } catch (...) {
+      s.stream = main;
+      s.write_r = 1;
+      throw;
+    }
+    s.stream = main;
+    s.write_r = 1;
+    s.stage = ST_UP;
+    phase_begin(s, FMM_PHASE_TRAVERSE);
+    structure_pass(s);
+    build_lists(s);
+    phase_end(s, FMM_PHASE_TRAVERSE);
+    FMM_CUDA(cudaStreamWaitEvent(s.stream, s.join, 0));  // the multipoles, before M2L
+  } else {
+    stage_up(s);
+    phase_begin(s, FMM_PHASE_TRAVERSE);
+    build_lists(s);
+    phase_end(s, FMM_PHASE_TRAVERSE);
+  }
   phase_begin(s, FMM_PHASE_M2L);
   run_m2l(s);
   phase_end(s, FMM_PHASE_M2L);
   // fork: the L2L levels on the side stream
   FMM_CUDA(cudaEventRecord(s.fork, s.stream));
   FMM_CUDA(cudaStreamWaitEvent(s.side, s.fork, 0));
-  cudaStream_t main = s.stream;
   s.stream = s.side;
   try {
     phase_begin(s, FMM_PHASE_DOWNWARD);

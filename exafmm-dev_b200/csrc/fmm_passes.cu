@@ -15,6 +15,8 @@ namespace fmmb200 {
 // the reference's mix of real_t and double arithmetic.  Multipoles stay unnormalised
 // here (the reference's MASS normalisation M[i] /= M[0] is a change of scale that the
 // M2L / L2L of the MASS build undo again), so only |M[0]| enters.
+// The monopole of each cell is read at M[c * stride] (the multipoles, stride ncoef, or the
+// monopoles of the structure pass, stride 1).
 template <typename T>
 __global__ void k_ropt(int ncells, vec4<T>* __restrict__ cX, const T* __restrict__ M,
                        const int* __restrict__ croot, int ncoef, int P, T theta) {
@@ -36,6 +38,61 @@ __global__ void k_ropt(int ncells, vec4<T>* __restrict__ cX, const T* __restrict
   cX[c].w = mul_rn(cX[c].w, mul_rn(x, theta));
 }
 
+// The cell radii of the upward pass and the monopoles, without the expansions (the
+// structure pass): setRmax and R /= theta (include/up_down_pass.h:45-84) with the same
+// rounded arithmetic as the P2M / M2M kernels, and each monopole as the sum the P2M / M2M
+// kernels form for M[0] (a leaf's charges in body order, then its children's monopoles in
+// child order), so that radii, monopoles and the error-optimised radii match those of the
+// expansion passes bit for bit.  It lets the traversal start while the expansions are
+// still being formed.
+template <typename T>
+__global__ void k_struct_leaves(const int* __restrict__ leaves, int nleaves,
+                                const int* __restrict__ ibody, const int* __restrict__ nbody,
+                                vec4<T>* __restrict__ cX, const vec4<T>* __restrict__ bodies,
+                                T* __restrict__ m0, int use_rmax, T theta) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nleaves) return;
+  const int c = leaves[w];
+  const int b0 = ibody[c], nb = nbody[c];
+  const vec4<T> C = cX[c];
+  T rmax = 0, q = 0;
+  for (int i = 0; i < nb; i++) {
+    const vec4<T> b = bodies[b0 + i];
+    const T r = sqrt_rn(norm_rn(sub_rn(C.x, b.x), sub_rn(C.y, b.y), sub_rn(C.z, b.z)));
+    rmax = r > rmax ? r : rmax;
+    q = add_rn(q, b.w);
+  }
+  T R = C.w;
+  if (use_rmax) R = rmax < R ? rmax : R;
+  cX[c].w = div_rn(R, theta);
+  m0[c] = q;
+}
+
+template <typename T>
+__global__ void k_struct_level(int lo, int hi, const int* __restrict__ npos,
+                               const int* __restrict__ ichild, const int* __restrict__ nchild,
+                               vec4<T>* __restrict__ cX, T* __restrict__ m0, int use_rmax,
+                               T theta) {
+  const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= hi) return;
+  const int c = npos[v], nch = nchild[c];
+  if (nch == 0) return;
+  const int c0 = ichild[c];
+  const vec4<T> Xp = cX[c];
+  T rr = 0, q = 0;
+  for (int k = 0; k < nch; k++) {
+    const vec4<T> Xc = cX[c0 + k];
+    const T d = add_rn(sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z))),
+                       Xc.w);
+    rr = d > rr ? d : rr;
+    q = add_rn(q, m0[c0 + k]);
+  }
+  T R = Xp.w;
+  if (use_rmax) R = rr < R ? rr : R;
+  cX[c].w = div_rn(R, theta);
+  m0[c] = q;
+}
+
 template <typename T>
 __global__ void k_output(int n, const int* __restrict__ order, const vec4<T>* __restrict__ s,
                          const vec4<T>* __restrict__ e, vec4<T>* __restrict__ out) {
@@ -53,7 +110,9 @@ template <typename T> static ExpansionOps<T> ops_of(const Solver<T>& s) {
   return ops;
 }
 
-template <typename T> void upward_pass(Solver<T>& s) {
+// the expansions of the upward pass (P2M, M2M); with s.write_r the kernels also set the
+// cell radii (setRmax, R /= theta), else the structure pass has set them
+template <typename T> void upward_expansions(Solver<T>& s) {
   if (s.ncells == 0) return;
   ExpansionOps<T> ops = ops_of(s);
   const size_t ne = (size_t)s.ncells * s.ncoef;
@@ -63,9 +122,38 @@ template <typename T> void upward_pass(Solver<T>& s) {
   FMM_CUDA(cudaMemsetAsync(s.L.p, 0, ne * sizeof(T), s.stream));
   ops.p2m(s);
   for (int l = s.maxlevel - 1; l >= 0; l--) ops.m2m_level(s, s.level_lo[l], s.level_lo[l + 1]);
+}
+
+template <typename T> void upward_pass(Solver<T>& s) {
+  if (s.ncells == 0) return;
+  s.write_r = 1;
+  upward_expansions(s);
   if (s.cfg.use_ropt) {
     k_ropt<T><<<ceil_div(s.ncells, 256), 256, 0, s.stream>>>(s.ncells, s.cX.p, s.M.p, s.c_root.p,
                                                             s.ncoef, s.cfg.P, (T)s.cfg.theta);
+    FMM_LAUNCH_CHECK();
+  }
+}
+
+// the final cell radii (radii, then the error-optimised radii) without the expansions
+template <typename T> void structure_pass(Solver<T>& s) {
+  if (s.ncells == 0) return;
+  const int TB = 128;
+  s.m0.ensure(s.ncells);
+  k_struct_leaves<T><<<ceil_div(s.nleaves, TB), TB, 0, s.stream>>>(
+      s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.m0.p,
+      s.cfg.use_rmax, (T)s.cfg.theta);
+  FMM_LAUNCH_CHECK();
+  for (int l = s.maxlevel - 1; l >= 0; l--) {
+    const int lo = s.level_lo[l], hi = s.level_lo[l + 1];
+    k_struct_level<T><<<ceil_div(hi - lo, TB), TB, 0, s.stream>>>(
+        lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.m0.p, s.cfg.use_rmax,
+        (T)s.cfg.theta);
+    FMM_LAUNCH_CHECK();
+  }
+  if (s.cfg.use_ropt) {
+    k_ropt<T><<<ceil_div(s.ncells, 256), 256, 0, s.stream>>>(s.ncells, s.cX.p, s.m0.p, s.c_root.p,
+                                                            1, s.cfg.P, (T)s.cfg.theta);
     FMM_LAUNCH_CHECK();
   }
 }
@@ -103,6 +191,10 @@ template <typename T> void downward_pass(Solver<T>& s) {
 
 template void upward_pass<float>(Solver<float>&);
 template void upward_pass<double>(Solver<double>&);
+template void upward_expansions<float>(Solver<float>&);
+template void upward_expansions<double>(Solver<double>&);
+template void structure_pass<float>(Solver<float>&);
+template void structure_pass<double>(Solver<double>&);
 template void run_m2l<float>(Solver<float>&);
 template void run_m2l<double>(Solver<double>&);
 template void downward_pass<float>(Solver<float>&);

@@ -107,6 +107,7 @@ struct SolverBase {
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
   int tree_plan = 0;        // levels of the handle's last tree (0: none; builds level by level)
+  int write_r = 1;          // P2M / M2M set the cell radii (else the structure pass did)
   DevArr<int> d_lvl;        // level ends of the planned node build
   // targets and sources in two trees (segments 0 and 1) on a common box, traversed from
   // (target root, source root) only (fmm_b200_solve_ij_*)
@@ -134,6 +135,7 @@ template <typename T> struct Solver : SolverBase {
   DevArr<vec4<T>> bodies_in, bodies, trg_s, trg_e, trg_out, cX;
   DevArr<T> box;  // per root, 16 values: X0[3], R0, Xmin[3], Xmax[3]
   DevArr<T> M, L, nX;
+  DevArr<T> m0;  // monopole per cell (structure pass)
   DevArr<T> pM, pM2, pC;  // periodic cell multipoles and per-shift M2L terms
   DevArr<int> c_root_cells;
   DevArr<T> minmax_part;
@@ -142,6 +144,8 @@ template <typename T> struct Solver : SolverBase {
 // ---- stage implementations (one translation unit each) ---------------------------------
 template <typename T> void build_tree(Solver<T>& s);          // fmm_tree.cu
 template <typename T> void upward_pass(Solver<T>& s);         // fmm_passes.cu
+template <typename T> void upward_expansions(Solver<T>& s);   // fmm_passes.cu: P2M, M2M
+template <typename T> void structure_pass(Solver<T>& s);      // fmm_passes.cu: radii, ropt
 template <typename T> void downward_pass(Solver<T>& s);       // fmm_passes.cu
 template <typename T> void downward_l2l(Solver<T>& s);        // fmm_passes.cu: L2L levels
 template <typename T> void downward_l2p(Solver<T>& s);        // fmm_passes.cu: L2P + output

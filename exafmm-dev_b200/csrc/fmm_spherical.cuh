@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(32 * P2MCfg<T, P>::W)
     k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
           const int* __restrict__ nbody, vec4<T>* __restrict__ cX,
           const vec4<T>* __restrict__ bodies, T* __restrict__ M, int ncoef, int use_rmax,
-          T theta) {
+          T theta, int write_r) {
   constexpr int NT = sph::NT(P), NC = 2 * NT, RS = NC | 1, KA = (NC + 31) / 32;
   constexpr int W = P2MCfg<T, P>::W;
   __shared__ T rows[W][32 * RS];
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(32 * P2MCfg<T, P>::W)
     const T v = __shfl_xor_sync(0xffffffffu, rmax, o);
     rmax = v > rmax ? v : rmax;
   }
-  if (lane == 0) {
+  if (lane == 0 && write_r) {
     T R = C.w;
     if (use_rmax) R = rmax < R ? rmax : R;
     cX[c].w = div_rn(R, theta);
@@ -115,7 +115,7 @@ template <typename T, int P>
 __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     k_m2m(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
           const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
-          int ncoef, int use_rmax, T theta) {
+          int ncoef, int use_rmax, T theta, int write_r) {
   constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
   constexpr int W = SphCfg<T>::W;
   __shared__ T sy[W][NC], sm[W][NC];
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     const T x = __shfl_xor_sync(0xffffffffu, rmax, o);
     rmax = x > rmax ? x : rmax;
   }
-  if (lane == 0) {
+  if (lane == 0 && write_r) {
     T R = Xp.w;
     if (use_rmax) R = rmax < R ? rmax : R;
     cX[c].w = div_rn(R, theta);
@@ -227,7 +227,7 @@ template <typename T, int P>
 __global__ void __launch_bounds__(kTrThreads)
     k_m2m_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
               const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
-              int ncoef, int use_rmax, T theta) {
+              int ncoef, int use_rmax, T theta, int write_r) {
   constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;  // odd row stride: no bank conflicts
   __shared__ T rows[kTrThreads * STR];
   T* row = rows + threadIdx.x * STR;
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kTrThreads)
     for (int k = 0; k < nch; k++) m0 = add_rn(m0, M[(size_t)(c0 + k) * ncoef]);
   const bool write = v < hi && nch > 0;
   m2m_passes<T, P, 0>(yr, yi, Mc, has, slot, write ? M + (size_t)c * ncoef : nullptr, m0);
-  if (write && slot == 0) {
+  if (write && slot == 0 && write_r) {
     T R = Xp.w;
     if (use_rmax) R = rr < R ? rr : R;
     cX[c].w = div_rn(R, theta);
@@ -593,20 +593,20 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
   if (!s.nleaves) return;
   k_p2m<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.M.p, s.ncoef,
-      s.cfg.use_rmax, (T)s.cfg.theta);
+      s.cfg.use_rmax, (T)s.cfg.theta, s.write_r);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
   if constexpr (sizeof(T) == 4) {
     k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), kTrThreads), kTrThreads, 0, s.stream>>>(
         lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
-        (T)s.cfg.theta);
+        (T)s.cfg.theta, s.write_r);
     FMM_LAUNCH_CHECK();
   } else {
     constexpr int W = SphCfg<T>::W;
     k_m2m<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(
         lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
-        (T)s.cfg.theta);
+        (T)s.cfg.theta, s.write_r);
     FMM_LAUNCH_CHECK();
   }
 }

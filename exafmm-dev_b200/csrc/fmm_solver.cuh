@@ -176,7 +176,8 @@ void set_call_error(const char* msg);
 
 // CUB wrappers compiled once (fmm_sort.cu)
 void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
-                    const int* vin, int* vout, int n, int end_bit);
+                    const int* vin, int* vout, int n, int end_bit,
+                    int begin_bit = 0);
 void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
                    int n, int end_bit);
 void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,

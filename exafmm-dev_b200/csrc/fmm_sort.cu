@@ -7,14 +7,14 @@
 namespace fmmb200 {
 
 void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
-                    const int* vin, int* vout, int n, int end_bit) {
+                    const int* vin, int* vout, int n, int end_bit, int begin_bit) {
   if (n <= 0) return;
   size_t bytes = 0;
-  FMM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit,
-                                           s.stream));
-  s.cub_tmp.ensure(bytes);
-  FMM_CUDA(cub::DeviceRadixSort::SortPairs(s.cub_tmp.p, bytes, kin, kout, vin, vout, n, 0,
+  FMM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, begin_bit,
                                            end_bit, s.stream));
+  s.cub_tmp.ensure(bytes);
+  FMM_CUDA(cub::DeviceRadixSort::SortPairs(s.cub_tmp.p, bytes, kin, kout, vin, vout, n,
+                                           begin_bit, end_bit, s.stream));
 }
 
 void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,

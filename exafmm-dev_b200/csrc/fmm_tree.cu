@@ -516,9 +516,10 @@ template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
 // sort gives each segment one thread block, which is slow for a few large segments.)
 template <typename T>
 static void forest_sort(Solver<T>& s, const unsigned long long* kin, unsigned long long* kout,
-                        const int* vin, int* vout, int n, int nroots, int end_bit) {
+                        const int* vin, int* vout, int n, int nroots, int end_bit,
+                        int begin_bit = 0) {
   if (nroots == 1) {
-    sort_pairs_u64(s, kin, kout, vin, vout, n, end_bit);
+    sort_pairs_u64(s, kin, kout, vin, vout, n, end_bit, begin_bit);
     return;
   }
   const int TB = 256;
@@ -528,7 +529,7 @@ static void forest_sort(Solver<T>& s, const unsigned long long* kin, unsigned lo
   s.fs_root2.ensure(n);
   s.fs_pos.ensure(n);
   s.fs_pos2.ensure(n);
-  sort_pairs_u64(s, kin, s.fs_keys.p, vin, s.fs_idx.p, n, end_bit);
+  sort_pairs_u64(s, kin, s.fs_keys.p, vin, s.fs_idx.p, n, end_bit, begin_bit);
   k_root_of<<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.fs_idx.p, s.d_root_first.p, nroots,
                                                   s.fs_root.p, s.fs_pos.p);
   FMM_LAUNCH_CHECK();
@@ -648,10 +649,16 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.keys2.ensure(n);
   s.idx.ensure(n);
   s.idx2.ensure(n);
+  // With a plan of L levels to split, the keys are sorted on their top L digits only: the
+  // splits read no deeper digit, and the bodies of a leaf are put in input order afterwards
+  // whatever the order of their deeper digits.  If the plan fails, they are sorted again on
+  // every digit for the level-by-level build.
+  const int plan_levels = s.tree_plan > 0 ? s.tree_plan + 1 : kMaxLevel;
+  const int begin_bit = plan_levels < kMaxLevel ? 3 * (kMaxLevel - plan_levels) : 0;
   k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, s.d_root_first.p,
                                                   nroots, s.keys.p, s.idx.p);
   FMM_LAUNCH_CHECK();
-  forest_sort(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots, 3 * kMaxLevel);
+  forest_sort(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots, 3 * kMaxLevel, begin_bit);
   // nodes, level by level
   size_t cap0 = (size_t)std::max(1024, 4 * (n / std::max(1, s.cfg.ncrit)) + 64 + nroots);
   DevArr<int>* narr[] = {&s.nbegin, &s.ncount, &s.nparent, &s.nchildn, &s.nfirst,
@@ -665,6 +672,17 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.level_lo.push_back(0);
   s.level_lo.push_back(nroots);
   const bool planned = s.tree_plan > 0 && planned_levels(s, nroots, narr, sizeof(narr) / sizeof(*narr));
+  if (!planned && begin_bit > 0) {
+    k_keys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p,
+                                                    s.d_root_first.p, nroots, s.keys.p, s.idx.p);
+    FMM_LAUNCH_CHECK();
+    forest_sort(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, nroots, 3 * kMaxLevel);
+    k_roots<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(nroots, s.d_root_first.p, s.box.p,
+                                                          s.nbegin.p, s.ncount.p, s.nparent.p,
+                                                          s.nlevel.p, s.nsid.p, s.nX.p);
+    FMM_LAUNCH_CHECK();
+    s.level_lo.assign({0, nroots});
+  }
   for (int level = 0; !planned; level++) {
     int lo = s.level_lo[level], hi = s.level_lo[level + 1];
     int m = hi - lo;

@@ -126,6 +126,32 @@ def test_solve_matches_oracle_and_direct(name, datasets):
     assert gp < op * 1.05 + 2e-6 and ga < oa * 1.05 + 2e-6, (gp, ga, op, oa)
 
 
+@pytest.mark.parametrize("prec,P,dist,kw", [
+    ("f32", 10, "plummer", dict(ncrit=64, theta=0.35, use_ropt=1)),
+    ("f64", 6, "cube", dict(ncrit=32, theta=0.4, use_ropt=0)),
+    ("f32", 8, "cube", dict(ncrit=32, theta=0.4, use_ropt=1, images=2, cycle=2.0))])
+def test_whole_solve_equals_stages(prec, P, dist, kw, datasets):
+    """A whole solve forms the multipoles on a side stream while a structure pass sets the
+    cell radii for the traversal: radii, lists and results bitwise those of the stages run
+    one after the other (where the expansion kernels set the radii)."""
+    x, q = datasets.make(dist, 30000, seed=17, precision=prec)
+    if kw.get("images"):
+        x = np.clip(x, -0.999, 0.999)
+    s = fmm.Solver(P=P, precision=prec, **kw)
+    s.set_bodies(x, q)
+    s.build_tree()
+    s.upward_pass()
+    s.traverse()
+    s.downward_pass()
+    staged, R, lists = s.trg(), s.cells()["R"], s.lists()
+    w = fmm.Solver(P=P, precision=prec, **kw)
+    whole = w.solve(x, q)
+    assert np.array_equal(w.cells()["R"], R)
+    m2l, p2p = w.lists()
+    assert np.array_equal(m2l, lists[0]) and np.array_equal(p2p, lists[1])
+    assert np.array_equal(whole, staged)
+
+
 def test_long_list_ranges(datasets):
     """A small opening angle on leaves of at most two bodies: M2L targets with more than
     1024 sources (sorted by a block instead of a warp) and P2P targets with more than 8192

@@ -440,6 +440,7 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
                          &s.d_lvl};                                                        \
     for (auto* a : ia) a->release();                                                       \
     s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
+    s.c_info.release();                                                                    \
     s.p2p.release(); s.list_tmp.release(); s.p2p_pairs_count.release();                   \
     s.cub_tmp.release(); s.front.release(); s.front2.release();                           \
   } while (0)

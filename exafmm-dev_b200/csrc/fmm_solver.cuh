@@ -97,6 +97,7 @@ struct SolverBase {
   int* scal_host = nullptr;  // pinned mirror of scal
   // cells
   DevArr<int> c_iparent, c_ichild, c_nchild, c_ibody, c_nbody, c_level;
+  DevArr<int4> c_info;  // per cell (NCHILD, ICHILD, NBODY, 0): one load for the traversal
   DevArr<unsigned long long> c_icell;
   DevArr<int> order;
   // interaction lists

@@ -30,15 +30,17 @@ enum {
 // a cell against itself always splits both sides (:200), and an M2L or a P2P between two
 // different cells is emitted in both directions (the mutual kernels update both cells);
 // *nout counts those outputs
+// The pair's cell data (centres with radii, and (NCHILD, ICHILD, NBODY)) are loaded
+// together, so that a pair costs one round trip to memory rather than one per decision.
 template <typename T>
 __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
-                                        const int* __restrict__ nchild,
-                                        const int* __restrict__ nbody, int nspawn, T cycle,
+                                        const int4* __restrict__ info, int nspawn, T cycle,
                                         int mutual, int* nout) {
   const int cj = pair_cell((unsigned)cjp);
   T px, py, pz;
   img_shift<T>(pair_img((unsigned)cjp), cycle, px, py, pz);
-  vec4<T> a = X[ci], b = X[cj];
+  const vec4<T> a = X[ci], b = X[cj];
+  const int4 fi = info[ci], fj = info[cj];
   T R2 = norm_rn(sub_rn(sub_rn(a.x, b.x), px), sub_rn(sub_rn(a.y, b.y), py),
                  sub_rn(sub_rn(a.z, b.z), pz));
   T Rs = add_rn(a.w, b.w);
@@ -46,7 +48,7 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
     *nout = mutual ? 2 : 1;
     return PAIR_M2L;
   }
-  int ni = nchild[ci], nj = nchild[cj];
+  const int ni = fi.x, nj = fj.x;
   if (ni == 0 && nj == 0) {
     *nout = mutual && ci != cj ? 2 : 1;
     return PAIR_P2P;
@@ -63,7 +65,7 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
     *nout = ni * (ni + 1) / 2;
     return PAIR_SPLIT_SELF;
   }
-  if (nbody[ci] + nbody[cj] >= nspawn) {
+  if (fi.z + fj.z >= nspawn) {
     *nout = ni * nj;
     return PAIR_SPLIT_IJ;
   }
@@ -78,14 +80,14 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
 // pass 1: per-block totals of (M2L, P2P, children) added to three device counters
 template <typename T>
 __global__ void k_trav_count(const int2* __restrict__ front, int nfront,
-                             const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
-                             const int* __restrict__ nbody, int nspawn, T cycle, int mutual,
+                             const vec4<T>* __restrict__ X, const int4* __restrict__ info,
+                             int nspawn, T cycle, int mutual,
                              unsigned long long* __restrict__ counters) {
   unsigned long long c[3] = {0, 0, 0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
     int2 p = front[t];
     int k;
-    int ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, mutual, &k);
+    int ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, &k);
     c[ty == PAIR_M2L ? 0 : ty == PAIR_P2P ? 1 : 2] += k;
   }
   for (int i = 0; i < 3; i++) {
@@ -115,8 +117,7 @@ __device__ __forceinline__ unsigned long long warp_alloc(unsigned long long* cou
 
 template <typename T>
 __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
-                             const vec4<T>* __restrict__ X, const int* __restrict__ nchild,
-                             const int* __restrict__ ichild, const int* __restrict__ nbody,
+                             const vec4<T>* __restrict__ X, const int4* __restrict__ info,
                              int nspawn, T cycle, int mutual,
                              unsigned long long* __restrict__ counters,
                              unsigned long long* __restrict__ m2l,
@@ -131,7 +132,7 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
     int2 p = make_int2(0, 0);
     if (t < nfront) {
       p = front[t];
-      ty = classify<T>(p.x, p.y, X, nchild, nbody, nspawn, cycle, mutual, &k);
+      ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, &k);
     }
     const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
     // the reverse of a mutual pair (no periodic image with mutual)
@@ -147,19 +148,19 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
       p2p[op] = packed;
       if (k == 2) p2p[op + 1] = rev;
     } else if (ty == PAIR_SPLIT_SELF) {
-      const int c0 = ichild[p.x], n = nchild[p.x];
+      const int c0 = info[p.x].y, n = info[p.x].x;
       unsigned long long q = o;
       for (int a = 0; a < n; a++)
         for (int b = a; b < n; b++) next[q++] = make_int2(c0 + a, c0 + b);
     } else if (ty == PAIR_SPLIT_I) {
-      int c0 = ichild[p.x];
+      int c0 = info[p.x].y;
       for (int i = 0; i < k; i++) next[o + i] = make_int2(c0 + i, p.y);
     } else if (ty == PAIR_SPLIT_J) {
-      int c0 = ichild[cj];
+      int c0 = info[cj].y;
       for (int j = 0; j < k; j++) next[o + j] = make_int2(p.x, (c0 + j) | img);
     } else if (ty == PAIR_SPLIT_IJ) {
-      int ci0 = ichild[p.x], cj0 = ichild[cj];
-      int nj = nchild[cj];
+      int ci0 = info[p.x].y, cj0 = info[cj].y;
+      int nj = info[cj].x;
       for (int i = 0; i < k; i++) next[o + i] = make_int2(ci0 + i / nj, (cj0 + i % nj) | img);
     }
   }
@@ -178,8 +179,7 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
                 unsigned long long front_cap, const vec4<T>* __restrict__ X,
-                const int* __restrict__ nchild, const int* __restrict__ ichild,
-                const int* __restrict__ nbody, int nspawn, T cycle, int mutual, int ncells,
+                const int4* __restrict__ info, int nspawn, T cycle, int mutual, int ncells,
                 unsigned long long* __restrict__ ctr,  // [0] M2L, [1] P2P, [2] bad index
                 unsigned long long* __restrict__ next_count, unsigned long long* __restrict__ m2l,
                 unsigned long long m2l_cap, unsigned long long* __restrict__ p2p,
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256)
         if ((unsigned)p[u].x < (unsigned)ncells &&
             (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
             pair_img((unsigned)p[u].y) < 27)
-          ty[u] = classify<T>(p[u].x, p[u].y, X, nchild, nbody, nspawn, cycle, mutual, &k[u]);
+          ty[u] = classify<T>(p[u].x, p[u].y, X, info, nspawn, cycle, mutual, &k[u]);
         else
           atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
       }
@@ -252,19 +252,19 @@ __global__ void __launch_bounds__(256)
         const int kw = o >= next_cap ? 0 : (int)min((unsigned long long)k[u], next_cap - o);
         const int cj = pair_cell((unsigned)p[u].y), img = (int)((unsigned)p[u].y & ~kCellMask);
         if (ty[u] == PAIR_SPLIT_SELF) {
-          const int c0 = ichild[p[u].x], n = nchild[p[u].x];
+          const int c0 = info[p[u].x].y, n = info[p[u].x].x;
           int w = 0;
           for (int a = 0; a < n; a++)
             for (int b = a; b < n; b++, w++)
               if (w < kw) next[o + w] = make_int2(c0 + a, c0 + b);
         } else if (ty[u] == PAIR_SPLIT_I) {
-          const int c0 = ichild[p[u].x];
+          const int c0 = info[p[u].x].y;
           for (int i = 0; i < kw; i++) next[o + i] = make_int2(c0 + i, p[u].y);
         } else if (ty[u] == PAIR_SPLIT_J) {
-          const int c0 = ichild[cj];
+          const int c0 = info[cj].y;
           for (int j = 0; j < kw; j++) next[o + j] = make_int2(p[u].x, (c0 + j) | img);
         } else {
-          const int ci0 = ichild[p[u].x], cj0 = ichild[cj], nj = nchild[cj];
+          const int ci0 = info[p[u].x].y, cj0 = info[cj].y, nj = info[cj].x;
           for (int i = 0; i < kw; i++)
             next[o + i] = make_int2(ci0 + i / nj, (cj0 + i % nj) | img);
         }
@@ -584,8 +584,8 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
   while (nfront > 0) {
     FMM_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s.stream));
     int grid = std::min(ceil_div(nfront, TB), 148 * 16);
-    k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
-                                               s.c_nbody.p, s.cfg.nspawn, (T)s.cfg.cycle,
+    k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_info.p,
+                                               s.cfg.nspawn, (T)s.cfg.cycle,
                                                mutual_of(s), cnt);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaMemcpyAsync(hc, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -611,8 +611,8 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     s.front2.ensure(std::max<long long>(an, 1));
     unsigned long long base[3] = {(unsigned long long)nm2l, (unsigned long long)np2p, 0};
     FMM_CUDA(cudaMemcpyAsync(cnt, base, sizeof(base), cudaMemcpyHostToDevice, s.stream));
-    k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_nchild.p,
-                                               s.c_ichild.p, s.c_nbody.p, s.cfg.nspawn,
+    k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_info.p,
+                                               s.cfg.nspawn,
                                                (T)s.cfg.cycle, mutual_of(s), cnt,
                                                s.m2l.p, s.p2p.p, s.front2.p);
     FMM_LAUNCH_CHECK();
@@ -647,7 +647,7 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
     DevArr<int2>& in = (l & 1) ? s.front2 : s.front;
     DevArr<int2>& out = (l & 1) ? s.front : s.front2;
     k_trav_step<T><<<148 * 8, TB, 0, s.stream>>>(
-        in.p, ctr + 3 + l, fcap, s.cX.p, s.c_nchild.p, s.c_ichild.p, s.c_nbody.p,
+        in.p, ctr + 3 + l, fcap, s.cX.p, s.c_info.p,
         s.cfg.nspawn, (T)s.cfg.cycle, mutual_of(s), s.ncells, ctr, ctr + 4 + l, s.m2l.p,
         s.m2l.cap, s.p2p.p,
         s.p2p.cap,

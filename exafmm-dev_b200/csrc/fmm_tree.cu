@@ -398,6 +398,14 @@ __global__ void k_pos(int lo, int hi, const int* __restrict__ nchildn,
   }
 }
 
+// (NCHILD, ICHILD, NBODY) of every cell in one 16-byte record, for the traversal
+__global__ void k_cell_info(int ncells, const int* __restrict__ nchild,
+                            const int* __restrict__ ichild, const int* __restrict__ nbody,
+                            int4* __restrict__ info) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncells) info[c] = make_int4(nchild[c], ichild[c], nbody[c], 0);
+}
+
 // Cell records (Nodes2cells::operator(), include/build_tree_tbb.h:250-262) with the
 // Morton index of getKey (:240-249) in 64-bit arithmetic.
 template <typename T>
@@ -747,6 +755,10 @@ template <typename T> void build_tree(Solver<T>& s) {
       nnodes, s.box.p, s.nbegin.p, s.ncount.p, s.nparent.p, s.nchildn.p, s.nlevel.p, s.nsid.p,
       s.cbase.p, s.npos.p, s.ncb.p, s.nX.p, s.c_iparent.p, s.c_ichild.p, s.c_nchild.p,
       s.c_ibody.p, s.c_nbody.p, s.c_level.p, s.c_icell.p, s.cX.p, s.c_root.p);
+  FMM_LAUNCH_CHECK();
+  s.c_info.ensure(nnodes);
+  k_cell_info<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.c_nchild.p, s.c_ichild.p,
+                                                         s.c_nbody.p, s.c_info.p);
   FMM_LAUNCH_CHECK();
   // bodies inside a leaf in input order (the stable partitions of the reference keep it)
   s.order.ensure(n);

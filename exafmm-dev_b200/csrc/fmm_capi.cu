@@ -180,13 +180,13 @@ template <typename T> void stage_down(Solver<T>& s) {
   phase_end(s, FMM_PHASE_TOTAL);
   s.stage = ST_DOWN;
 }
-// A whole solve: the stages in order, with two overlaps on a high-priority side stream.
-// (1) Spherical basis: the expansions of the upward pass (P2M, M2M) run on the side stream
+// A whole solve: the stages in order, with two overlaps on side streams.  (1) Spherical
+// basis: the expansions of the upward pass (P2M, M2M) run on a lowest-priority stream
 // while the main stream sets the cell radii in a pass of their own (structure_pass: the
 // same radii, monopoles and error-optimised radii as the expansion kernels would set) and
 // runs the traversal, which needs the radii but not the expansions; M2L waits for both.
-// (2) The L2L levels run on the side stream while P2P runs (from the end of M2L to the
-// start of L2P).  The L2L levels have few cells each and long dependent chains per cell, so
+// (2) The L2L levels run on a high-priority stream while P2P runs (from the end of M2L to
+// the start of L2P).  The L2L levels have few cells each and long dependent chains per cell, so
 // alone they leave most of the GPU idle; with the higher priority their blocks start as
 // soon as SMs free up.  The results are the same as stage by stage: P2P writes only the
 // bodies' sums, L2L only the local expansions, and L2P runs after both.
@@ -196,14 +196,15 @@ template <typename T> void solve_all(Solver<T>& s) {
     int lo = 0, hi = 0;
     FMM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     FMM_CUDA(cudaStreamCreateWithPriority(&s.side, cudaStreamNonBlocking, hi));
+    FMM_CUDA(cudaStreamCreateWithPriority(&s.side_lo, cudaStreamNonBlocking, lo));
     FMM_CUDA(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
     FMM_CUDA(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
   }
   cudaStream_t main = s.stream;
   if (s.cfg.basis == FMM_SPHERICAL && s.ncells > 0) {
     FMM_CUDA(cudaEventRecord(s.fork, s.stream));
-    FMM_CUDA(cudaStreamWaitEvent(s.side, s.fork, 0));
-    s.stream = s.side;
+    FMM_CUDA(cudaStreamWaitEvent(s.side_lo, s.fork, 0));
+    s.stream = s.side_lo;  // below the traversal, which is on the critical path
     s.write_r = 0;
     try {
       phase_begin(s, FMM_PHASE_UPWARD);
@@ -469,6 +470,7 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     if (s.fork) cudaEventDestroy(s.fork);
     if (s.join) cudaEventDestroy(s.join);
     if (s.side) cudaStreamDestroy(s.side);
+    if (s.side_lo) cudaStreamDestroy(s.side_lo);
     if (s.scal_host) cudaFreeHost(s.scal_host);
     delete h->base;
   }

@@ -128,6 +128,7 @@ struct SolverBase {
   // whole solves run the latency-bound L2L levels on a high-priority side stream, forked
   // after M2L and joined before L2P, so that they overlap P2P
   cudaStream_t side = nullptr;
+  cudaStream_t side_lo = nullptr;  // lowest priority: the upward expansions beside the traversal
   cudaEvent_t fork = nullptr, join = nullptr;
   virtual ~SolverBase() {}
 };

@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(kSegBlock)
 }
 
 // M2L targets (cells with at least one source) keyed by their number of 32-source batches,
-// largest first, for the lockstep M2L kernels
+// largest first, so that the warps of an M2L block have about the same amount of work
 __global__ void k_m2l_targets(int ncells, const int* __restrict__ off,
                               unsigned long long* __restrict__ key, int* __restrict__ cell,
                               int* __restrict__ count) {

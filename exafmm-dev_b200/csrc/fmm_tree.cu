@@ -257,9 +257,10 @@ __global__ void k_split(int lo, int hi, int level, int ncrit,
 }
 
 // k_split with the level's node range read on the device (lvl[level], lvl[level + 1]) for
-// the planned build: a grid-stride loop over the nodes, counts past the level's nodes zeroed
-// up to mcap (the size of the scan that follows); a level of more than mcap nodes flags
-// overflow and is not split.
+// the planned build: a grid-stride loop over the level's nodes.  The counts past them are
+// zero (cnt is cleared before the first level, and k_emit_planned clears the counts it has
+// used), as the scan over mcap + 1 entries that follows needs; a level of more than mcap
+// nodes flags overflow and is not split.
 __global__ void k_split_planned(const int* __restrict__ lvl, int level, int ncrit, int mcap,
                                 const unsigned long long* __restrict__ keys,
                                 const int* __restrict__ nbegin, const int* __restrict__ ncount,
@@ -270,10 +271,8 @@ __global__ void k_split_planned(const int* __restrict__ lvl, int level, int ncri
   const int mm = m <= mcap ? m : 0;
   if (m > mcap && blockIdx.x == 0 && threadIdx.x == 0) atomicExch(overflow, 1);
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w <= mcap; w += nw) {
-    if (w < mm) split_node(lane, (int)w, lo + (int)w, level, ncrit, keys, nbegin, ncount, cnt, starts);
-    else if (lane == 0) cnt[w] = 0;
-  }
+  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < mm; w += nw)
+    split_node(lane, (int)w, lo + (int)w, level, ncrit, keys, nbegin, ncount, cnt, starts);
 }
 
 // the children of node t of the level (v = lo + t), from hi + coff[t] on
@@ -334,7 +333,7 @@ __global__ void k_emit(int lo, int hi, int level, const int* __restrict__ cnt,
 // the node arrays (ncap) flag overflow and are not emitted.
 template <typename T>
 __global__ void k_emit_planned(int* __restrict__ lvl, int level, int ncap,
-                               const int* __restrict__ cnt, const int* __restrict__ coff,
+                               int* __restrict__ cnt, const int* __restrict__ coff,
                                const int* __restrict__ starts, const T* __restrict__ box,
                                int* __restrict__ nbegin, int* __restrict__ ncount,
                                int* __restrict__ nparent, int* __restrict__ nchildn,
@@ -348,10 +347,12 @@ __global__ void k_emit_planned(int* __restrict__ lvl, int level, int ncap,
     lvl[level + 2] = fits ? hi + total : hi;
     if (!fits) atomicExch(overflow, 1);
   }
-  if (!fits) return;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x)
-    emit_node<T>(t, lo, hi, level, cnt, coff, starts, box, nbegin, ncount, nparent, nchildn,
-                 nfirst, nlevel, nsid, nX);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    if (fits)
+      emit_node<T>(t, lo, hi, level, cnt, coff, starts, box, nbegin, ncount, nparent, nchildn,
+                   nfirst, nlevel, nsid, nX);
+    if (t < ncap) cnt[t] = 0;  // cleared for the next level's scan
+  }
 }
 
 // leaf nodes: chain-less nodes at the deepest level of the last pass
@@ -575,6 +576,7 @@ static bool planned_levels(Solver<T>& s, int nroots, DevArr<int>** narr, int nna
   hl[1] = nroots;
   FMM_CUDA(cudaMemcpyAsync(lvl, hl, 2 * sizeof(int), cudaMemcpyHostToDevice, s.stream));
   FMM_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int), s.stream));
+  FMM_CUDA(cudaMemsetAsync(cnt, 0, ((size_t)mcap + 1) * sizeof(int), s.stream));
   const int gs = (int)std::min<long long>(ceil_div(32LL * (mcap + 1), TB), 148 * 16);
   const int ge = (int)std::min<long long>(ceil_div((long long)mcap, TB), 148 * 8);
   for (int level = 0; level < L; level++) {

@@ -808,7 +808,10 @@ int fmm_b200_num_lists(fmm_b200_solver* h, long long* nm2l, long long* np2p, lon
     if (h->base->stage < ST_TRAV) throw FmmError(FMM_ERR_STATE, "traversal not done");
     if (nm2l) *nm2l = h->base->nm2l;
     if (np2p) *np2p = h->base->np2p;
-    if (bp) *bp = h->base->p2p_body_pairs;
+    if (bp) {
+      if (h->base->p2p_body_pairs < 0) h->base->p2p_body_pairs = count_p2p_body_pairs(*h->base);
+      *bp = h->base->p2p_body_pairs;
+    }
   });
 }
 

@@ -84,7 +84,7 @@ struct SolverBase {
   // tree shape (host copies of the few scalars the level loops need)
   int ncells = 0, maxlevel = 0, nleaves = 0;
   std::vector<int> level_lo;  // node index range of level l: [level_lo[l], level_lo[l+1])
-  long long nm2l = 0, np2p = 0, p2p_body_pairs = 0;
+  long long nm2l = 0, np2p = 0, p2p_body_pairs = 0;  // body pairs: -1 until counted
   // node arrays (breadth-first)
   DevArr<int> nbegin, ncount, nparent, nchildn, nfirst, nnode, npos, ncb, nlevel, nsplit;
   DevArr<int> coff;
@@ -145,6 +145,7 @@ template <typename T> struct Solver : SolverBase {
 
 // ---- stage implementations (one translation unit each) ---------------------------------
 template <typename T> void build_tree(Solver<T>& s);          // fmm_tree.cu
+long long count_p2p_body_pairs(SolverBase& s);              // fmm_traverse.cu
 template <typename T> void upward_pass(Solver<T>& s);         // fmm_passes.cu
 template <typename T> void upward_expansions(Solver<T>& s);   // fmm_passes.cu: P2M, M2M
 template <typename T> void structure_pass(Solver<T>& s);      // fmm_passes.cu: radii, ropt

@@ -555,6 +555,8 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
 }
 
 // ---------------------------------------------------------------- L2P
+// Half a warp per leaf (two leaves per warp), lane per body: most leaves hold fewer than
+// 32 bodies, so a whole warp per leaf would leave half its lanes idle.
 template <typename T, int P>
 __global__ void __launch_bounds__(32 * SphCfg<T>::W)
     k_l2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
@@ -563,19 +565,19 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
           vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
   constexpr int NT = sph::NT(P), NC = 2 * NT;
   constexpr int W = SphCfg<T>::W;
-  __shared__ T sl[W][NC];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int w = blockIdx.x * W + wl;
-  if (w >= nleaves) return;
-  const int c = leaves[w];
-  const int b0 = ibody[c], nb = nbody[c];
+  __shared__ T sl[W][2][NC];
+  const int wl = threadIdx.x >> 5, lane = lane_id(), h = lane >> 4, hl = lane & 15;
+  const int w = 2 * (blockIdx.x * W + wl) + h;
+  const int c = w < nleaves ? leaves[w] : 0;
+  const int b0 = w < nleaves ? ibody[c] : 0, nb = w < nleaves ? nbody[c] : 0;
   const vec4<T> C = cX[c];
-  for (int t = lane; t < NC; t += 32) sl[wl][t] = L[(size_t)c * ncoef + t];
+  if (w < nleaves)
+    for (int t = hl; t < NC; t += 16) sl[wl][h][t] = L[(size_t)c * ncoef + t];
   __syncwarp();
-  for (int i = lane; i < nb; i += 32) {
+  for (int i = hl; i < nb; i += 16) {
     const vec4<T> b = bodies[b0 + i];
     T pot, gx, gy, gz;
-    sph::l2p_body<T, P>(b.x - C.x, b.y - C.y, b.z - C.z, sl[wl], pot, gx, gy, gz);
+    sph::l2p_body<T, P>(b.x - C.x, b.y - C.y, b.z - C.z, sl[wl][h], pot, gx, gy, gz);
     vec4<T> s = trg_s[b0 + i], e = trg_e[b0 + i];
     Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
     comp_add(a0, pot);
@@ -635,7 +637,7 @@ template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   constexpr int W = SphCfg<T>::W;
   if (!s.nleaves) return;
-  k_l2p<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
+  k_l2p<T, P><<<ceil_div(s.nleaves, 2 * W), 32 * W, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef,
       s.trg_s.p, s.trg_e.p);
   FMM_LAUNCH_CHECK();

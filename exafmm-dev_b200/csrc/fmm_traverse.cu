@@ -709,10 +709,6 @@ template <typename T> void build_lists(Solver<T>& s) {
     sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.m2l_tgt.p, s.ncells, 10);
     FMM_CUDA(cudaMemcpyAsync(s.scal_host + 12, ntgt, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
   }
-  FMM_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned long long), s.stream));
-  k_p2p_bodypairs<<<std::max(1, std::min(ceil_div(np2p, TB), 148 * 8)), TB, 0, s.stream>>>(
-      s.p2p.p, np2p, s.c_nbody.p, cnt + 3);
-  FMM_LAUNCH_CHECK();
   FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, 3 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
@@ -722,8 +718,24 @@ template <typename T> void build_lists(Solver<T>& s) {
     if (hflow[1]) global_sort_list(s, s.p2p.p, np2p, b, ib);
     FMM_CUDA(cudaStreamSynchronize(s.stream));
   }
-  s.p2p_body_pairs = (long long)hc[3];
+  s.p2p_body_pairs = -1;  // counted when asked for (count_p2p_body_pairs)
   s.m2l_ntgt = s.scal_host[12];
+}
+
+// the body pairs of the P2P list, for the statistics (not needed by the solve itself)
+long long count_p2p_body_pairs(SolverBase& s) {
+  if (s.np2p == 0) return 0;
+  const int TB = 256;
+  unsigned long long* cnt = (unsigned long long*)s.scal.p;
+  unsigned long long* hc = (unsigned long long*)s.scal_host;
+  FMM_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned long long), s.stream));
+  k_p2p_bodypairs<<<std::max(1, std::min(ceil_div(s.np2p, TB), 148 * 8)), TB, 0, s.stream>>>(
+      s.p2p.p, s.np2p, s.c_nbody.p, cnt + 3);
+  FMM_LAUNCH_CHECK();
+  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           s.stream));
+  FMM_CUDA(cudaStreamSynchronize(s.stream));
+  return (long long)hc[3];
 }
 
 template void build_lists<float>(Solver<float>&);

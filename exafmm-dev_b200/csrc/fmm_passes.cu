@@ -45,27 +45,41 @@ __global__ void k_ropt(int ncells, vec4<T>* __restrict__ cX, const T* __restrict
 // child order), so that radii, monopoles and the error-optimised radii match those of the
 // expansion passes bit for bit.  It lets the traversal start while the expansions are
 // still being formed.
+// a warp per leaf: the bodies' distances to the centre 32 at a time (their maximum by
+// shuffles: max is exact), the charges added in body order by lane 0 from shuffles
 template <typename T>
 __global__ void k_struct_leaves(const int* __restrict__ leaves, int nleaves,
                                 const int* __restrict__ ibody, const int* __restrict__ nbody,
                                 vec4<T>* __restrict__ cX, const vec4<T>* __restrict__ bodies,
                                 T* __restrict__ m0, int use_rmax, T theta) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = lane_id();
   if (w >= nleaves) return;
   const int c = leaves[w];
   const int b0 = ibody[c], nb = nbody[c];
   const vec4<T> C = cX[c];
   T rmax = 0, q = 0;
-  for (int i = 0; i < nb; i++) {
-    const vec4<T> b = bodies[b0 + i];
+  for (int base = 0; base < nb; base += 32) {
+    const int cnt = min(32, nb - base);
+    vec4<T> b = make_v4<T>(C.x, C.y, C.z, 0);
+    if (lane < cnt) b = bodies[b0 + base + lane];
     const T r = sqrt_rn(norm_rn(sub_rn(C.x, b.x), sub_rn(C.y, b.y), sub_rn(C.z, b.z)));
     rmax = r > rmax ? r : rmax;
-    q = add_rn(q, b.w);
+    for (int i = 0; i < cnt; i++) {
+      const T qi = __shfl_sync(0xffffffffu, b.w, i);
+      q = add_rn(q, qi);
+    }
   }
-  T R = C.w;
-  if (use_rmax) R = rmax < R ? rmax : R;
-  cX[c].w = div_rn(R, theta);
-  m0[c] = q;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T v = __shfl_xor_sync(0xffffffffu, rmax, o);
+    rmax = v > rmax ? v : rmax;
+  }
+  if (lane == 0) {
+    T R = C.w;
+    if (use_rmax) R = rmax < R ? rmax : R;
+    cX[c].w = div_rn(R, theta);
+    m0[c] = q;
+  }
 }
 
 template <typename T>
@@ -140,7 +154,7 @@ template <typename T> void structure_pass(Solver<T>& s) {
   if (s.ncells == 0) return;
   const int TB = 128;
   s.m0.ensure(s.ncells);
-  k_struct_leaves<T><<<ceil_div(s.nleaves, TB), TB, 0, s.stream>>>(
+  k_struct_leaves<T><<<ceil_div(32LL * s.nleaves, TB), TB, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.m0.p,
       s.cfg.use_rmax, (T)s.cfg.theta);
   FMM_LAUNCH_CHECK();

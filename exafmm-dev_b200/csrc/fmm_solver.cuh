@@ -107,6 +107,7 @@ struct SolverBase {
   DevArr<int> fs_idx;
   DevArr<int2> front, front2;
   bool trav_sized = false;  // list / frontier buffers sized by a counted traversal
+  int trav_steps = 0, trav_maxlevel = 0;  // the last traversal's steps, and its tree depth
   int tree_plan = 0;        // levels of the handle's last tree (0: none; builds level by level)
   int write_r = 1;          // P2M / M2M set the cell radii (else the structure pass did)
   DevArr<int> d_lvl;        // level ends of the planned node build

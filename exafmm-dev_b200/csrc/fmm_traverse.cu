@@ -577,6 +577,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
   unsigned long long* hc = (unsigned long long*)s.scal_host;
   upload_roots(s);
   long long nfront = s.nfront0, maxfront = s.nfront0;
+  int steps = 0;
   nm2l = np2p = 0;
   // first sizes from typical list lengths per cell; grown below when they fall short
   s.m2l.ensure(std::max(1024LL, 64LL * s.ncells));
@@ -622,18 +623,26 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     nfront = an;
     maxfront = std::max(maxfront, an);
     std::swap(s.front, s.front2);
+    steps++;
   }
+  s.trav_steps = steps;
+  s.trav_maxlevel = s.maxlevel;
   return maxfront;
 }
 
-// Traversal on buffers sized by an earlier solve: a fixed number of steps (enough for the
-// deepest pair of cells), frontier sizes kept on the device, one host read at the end.
-// Returns false, with the lists incomplete, when a buffer was too small or the steps did
-// not reach the end.
+// Traversal on buffers sized by an earlier solve: a fixed number of steps, frontier sizes
+// kept on the device, one host read at the end.  The steps: those of the handle's last
+// traversal, two more per level that the tree has grown by since, and two to spare, at most
+// enough for the deepest pair of cells.  Returns false, with the lists incomplete, when a
+// buffer was too small or the steps did not reach the end.
 template <typename T>
 static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
   const int TB = 256;
-  const int steps = 2 * (s.maxlevel + 1) + 2;
+  const int bound = 2 * (s.maxlevel + 1) + 2;
+  const int steps =
+      s.trav_steps > 0
+          ? std::min(bound, s.trav_steps + 2 * std::max(0, s.maxlevel - s.trav_maxlevel) + 2)
+          : bound;
   // [0] M2L total, [1] P2P total, [2] invalid-index flag, [3 + l] frontier size of step l
   unsigned long long* ctr = (unsigned long long*)s.scal.p + 32;
   unsigned long long* hctr = (unsigned long long*)s.scal_host + 32;
@@ -663,6 +672,10 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
   if (hctr[0] > s.m2l.cap || hctr[1] > s.p2p.cap || hctr[3 + steps] != 0) return false;
   for (int l = 0; l <= steps; l++)
     if (hctr[3 + l] > fcap) return false;
+  int used = 0;  // steps with a non-empty frontier
+  while (used < steps && hctr[3 + used] != 0) used++;
+  s.trav_steps = used;
+  s.trav_maxlevel = s.maxlevel;
   return true;
 }
 

@@ -221,13 +221,13 @@ template <typename T> void solve_all(Solver<T>& s) {
     s.stage = ST_UP;
     phase_begin(s, FMM_PHASE_TRAVERSE);
     structure_pass(s);
-    build_lists(s);
+    build_lists(s, true);
     phase_end(s, FMM_PHASE_TRAVERSE);
     FMM_CUDA(cudaStreamWaitEvent(s.stream, s.join, 0));  // the multipoles, before M2L
   } else {
     stage_up(s);
     phase_begin(s, FMM_PHASE_TRAVERSE);
-    build_lists(s);
+    build_lists(s, true);
     phase_end(s, FMM_PHASE_TRAVERSE);
   }
   phase_begin(s, FMM_PHASE_M2L);
@@ -253,6 +253,7 @@ template <typename T> void solve_all(Solver<T>& s) {
     FMM_CUDA(cudaMemsetAsync(s.trg_s.p, 0, sizeof(vec4<T>) * s.n, s.stream));
     FMM_CUDA(cudaMemsetAsync(s.trg_e.p, 0, sizeof(vec4<T>) * s.n, s.stream));
   }
+  finish_p2p_list(s);  // grouped on the side stream while M2L ran
   run_p2p(s);
   phase_end(s, FMM_PHASE_P2P);
   s.stage = ST_TRAV;
@@ -438,12 +439,13 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
                          &s.coff,     &s.leaves,   &s.idx,      &s.idx2,    &s.scal,       \
                          &s.c_iparent, &s.c_ichild, &s.c_nchild, &s.c_ibody, &s.c_nbody,   \
                          &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off, &s.seg_cnt,    \
-                         &s.d_lvl};                                                        \
+                         &s.d_lvl,    &s.seg_cnt2};                                        \
     for (auto* a : ia) a->release();                                                       \
     s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
     s.c_info.release();                                                                    \
     s.p2p.release(); s.list_tmp.release(); s.p2p_pairs_count.release();                   \
     s.cub_tmp.release(); s.front.release(); s.front2.release();                           \
+    s.seg_keys2.release(); s.cub_tmp2.release();                                           \
   } while (0)
 
 int fmm_b200_destroy(fmm_b200_solver* h) {
@@ -471,6 +473,7 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     if (s.join) cudaEventDestroy(s.join);
     if (s.side) cudaStreamDestroy(s.side);
     if (s.side_lo) cudaStreamDestroy(s.side_lo);
+    if (s.p2p_ready) cudaEventDestroy(s.p2p_ready);
     if (s.scal_host) cudaFreeHost(s.scal_host);
     delete h->base;
   }

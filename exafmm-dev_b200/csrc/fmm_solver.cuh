@@ -119,6 +119,12 @@ struct SolverBase {
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
   DevArr<int> seg_cnt;  // pairs per target while a list is grouped by target
+  // the P2P list's grouping when it runs on the side stream beside M2L (whole solves)
+  DevArr<int> seg_cnt2;
+  DevArr<unsigned> seg_keys2;
+  DevArr<char> cub_tmp2;
+  bool p2p_pending = false;
+  cudaEvent_t p2p_ready = nullptr;
   DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches
   int m2l_ntgt = 0;
   DevArr<unsigned long long> p2p_pairs_count;
@@ -153,7 +159,8 @@ template <typename T> void structure_pass(Solver<T>& s);      // fmm_passes.cu: 
 template <typename T> void downward_pass(Solver<T>& s);       // fmm_passes.cu
 template <typename T> void downward_l2l(Solver<T>& s);        // fmm_passes.cu: L2L levels
 template <typename T> void downward_l2p(Solver<T>& s);        // fmm_passes.cu: L2P + output
-template <typename T> void build_lists(Solver<T>& s);         // fmm_traverse.cu
+template <typename T> void build_lists(Solver<T>& s, bool defer_p2p = false);  // fmm_traverse.cu
+void finish_p2p_list(SolverBase& s);  // fmm_traverse.cu: after build_lists(s, true)
 template <typename T> void run_m2l(Solver<T>& s);             // fmm_passes.cu
 template <typename T> void run_p2p(Solver<T>& s);             // fmm_p2p.cu
 
@@ -186,7 +193,9 @@ void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long l
                    int n, int end_bit);
 void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,
                     int* vout, int n, int end_bit);
-void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n);
+// scratch: s.cub_tmp, or tmp for a scan that may run beside other CUB calls of the solver
+void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n,
+                       DevArr<char>* tmp = nullptr);
 void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
                               unsigned long long* kout, const int* vin, int* vout, int n,
                               int nseg, const int* begin, const int* end, int end_bit);

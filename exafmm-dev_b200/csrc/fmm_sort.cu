@@ -50,12 +50,13 @@ void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const in
                                            end_bit, s.stream));
 }
 
-void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n) {
+void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n, DevArr<char>* tmp) {
   if (n <= 0) return;
+  DevArr<char>& t = tmp ? *tmp : s.cub_tmp;
   size_t bytes = 0;
   FMM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s.stream));
-  s.cub_tmp.ensure(bytes);
-  FMM_CUDA(cub::DeviceScan::ExclusiveSum(s.cub_tmp.p, bytes, in, out, n, s.stream));
+  t.ensure(bytes);
+  FMM_CUDA(cub::DeviceScan::ExclusiveSum(t.p, bytes, in, out, n, s.stream));
 }
 
 void sum_u64(SolverBase& s, const unsigned long long* in, unsigned long long* out, int n) {

@@ -501,19 +501,20 @@ static int bits_for(int n) {
 
 // group a list by target (k_seg_*): CSR offsets into off[0, ncells], pairs sorted within
 // each target's range
+// scratch: segcnt (ncells + 1 ints), keys (n), tmp (CUB scan scratch, or s.cub_tmp if null)
 static void group_by_target(SolverBase& s, unsigned long long* lst, long long n, int b,
-                            int* off, int* overflow) {
+                            int* off, int* overflow, int* segcnt, unsigned* keys,
+                            DevArr<char>* tmp) {
   const int TB = 256;
-  FMM_CUDA(cudaMemsetAsync(s.seg_cnt.p, 0, (s.ncells + 1) * sizeof(int), s.stream));
+  FMM_CUDA(cudaMemsetAsync(segcnt, 0, (s.ncells + 1) * sizeof(int), s.stream));
   const int grid = (int)std::max(1LL, std::min<long long>(ceil_div(n, TB), 148 * 16));
   if (n > 0) {
-    k_seg_count<<<grid, TB, 0, s.stream>>>(lst, n, s.seg_cnt.p);
+    k_seg_count<<<grid, TB, 0, s.stream>>>(lst, n, segcnt);
     FMM_LAUNCH_CHECK();
   }
-  exclusive_sum_int(s, s.seg_cnt.p, off, s.ncells + 1);
+  exclusive_sum_int(s, segcnt, off, s.ncells + 1, tmp);
   if (n == 0) return;
-  unsigned* keys = (unsigned*)s.list_tmp.p;
-  k_seg_scatter<<<grid, TB, 0, s.stream>>>(lst, n, off, s.seg_cnt.p, b, keys);
+  k_seg_scatter<<<grid, TB, 0, s.stream>>>(lst, n, off, segcnt, b, keys);
   FMM_LAUNCH_CHECK();
   k_seg_sort_warp<<<ceil_div(s.ncells, kSegWarps), 32 * kSegWarps, 0, s.stream>>>(s.ncells, off,
                                                                                  keys, b, lst);
@@ -679,7 +680,24 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
   return true;
 }
 
-template <typename T> void build_lists(Solver<T>& s) {
+// the P2P list of a build_lists(s, true): wait (on the host) for its grouping on the side
+// stream, sort it globally if a target's range was too long for the blocks, and make the
+// main stream wait for it
+void finish_p2p_list(SolverBase& s) {
+  if (!s.p2p_pending) return;
+  s.p2p_pending = false;
+  FMM_CUDA(cudaEventSynchronize(s.p2p_ready));
+  const int* hflow = (const int*)((unsigned long long*)s.scal_host + 5);
+  if (hflow[1]) {
+    FMM_CUDA(cudaStreamWaitEvent(s.stream, s.p2p_ready, 0));
+    global_sort_list(s, s.p2p.p, s.np2p, bits_for(s.ncells), s.cfg.images > 0 ? 5 : 0);
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+  } else {
+    FMM_CUDA(cudaStreamWaitEvent(s.stream, s.p2p_ready, 0));
+  }
+}
+
+template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
   const int TB = 256;
   s.nm2l = s.np2p = s.p2p_body_pairs = 0;
   if (s.ncells == 0) return;
@@ -706,8 +724,34 @@ template <typename T> void build_lists(Solver<T>& s) {
   s.seg_cnt.ensure(s.ncells + 1);
   int* overflow = (int*)(cnt + 5);  // per list: a target range too long for the blocks
   FMM_CUDA(cudaMemsetAsync(overflow, 0, 2 * sizeof(int), s.stream));
-  group_by_target(s, s.m2l.p, nm2l, b, s.m2l_off.p, overflow);
-  group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1);
+  group_by_target(s, s.m2l.p, nm2l, b, s.m2l_off.p, overflow, s.seg_cnt.p,
+                  (unsigned*)s.list_tmp.p, nullptr);
+  s.p2p_pending = defer_p2p && s.side != nullptr;
+  if (s.p2p_pending) {
+    // the P2P list is grouped on the side stream with scratch of its own, beside M2L; its
+    // overflow flag reaches the host through the pinned mirror (finish_p2p_list)
+    s.seg_cnt2.ensure(s.ncells + 1);
+    s.seg_keys2.ensure(std::max<long long>(np2p, 1));
+    if (!s.p2p_ready) FMM_CUDA(cudaEventCreateWithFlags(&s.p2p_ready, cudaEventDisableTiming));
+    FMM_CUDA(cudaEventRecord(s.fork, s.stream));
+    FMM_CUDA(cudaStreamWaitEvent(s.side, s.fork, 0));
+    cudaStream_t main = s.stream;
+    s.stream = s.side;
+    try {
+      group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1, s.seg_cnt2.p,
+                      s.seg_keys2.p, &s.cub_tmp2);
+      FMM_CUDA(cudaMemcpyAsync((int*)(hc + 5) + 1, overflow + 1, sizeof(int),
+                               cudaMemcpyDeviceToHost, s.stream));
+      FMM_CUDA(cudaEventRecord(s.p2p_ready, s.stream));
+    } catch (...) {
+      s.stream = main;
+      throw;
+    }
+    s.stream = main;
+  } else {
+    group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1, s.seg_cnt.p,
+                    (unsigned*)s.list_tmp.p, nullptr);
+  }
   // M2L target order: by descending batch count (stable in cell index)
   {
     int* ntgt = (int*)(cnt + 4);
@@ -722,13 +766,16 @@ template <typename T> void build_lists(Solver<T>& s) {
     sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.m2l_tgt.p, s.ncells, 10);
     FMM_CUDA(cudaMemcpyAsync(s.scal_host + 12, ntgt, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
   }
-  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, 3 * sizeof(unsigned long long),
+  FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, 2 * sizeof(unsigned long long) + sizeof(int),
                            cudaMemcpyDeviceToHost, s.stream));
+  if (!s.p2p_pending)
+    FMM_CUDA(cudaMemcpyAsync((int*)(hc + 5) + 1, overflow + 1, sizeof(int),
+                             cudaMemcpyDeviceToHost, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
   const int* hflow = (const int*)(hc + 5);
-  if (hflow[0] || hflow[1]) {
+  if (hflow[0] || (!s.p2p_pending && hflow[1])) {
     if (hflow[0]) global_sort_list(s, s.m2l.p, nm2l, b, ib);
-    if (hflow[1]) global_sort_list(s, s.p2p.p, np2p, b, ib);
+    if (!s.p2p_pending && hflow[1]) global_sort_list(s, s.p2p.p, np2p, b, ib);
     FMM_CUDA(cudaStreamSynchronize(s.stream));
   }
   s.p2p_body_pairs = -1;  // counted when asked for (count_p2p_body_pairs)
@@ -751,7 +798,7 @@ long long count_p2p_body_pairs(SolverBase& s) {
   return (long long)hc[3];
 }
 
-template void build_lists<float>(Solver<float>&);
-template void build_lists<double>(Solver<double>&);
+template void build_lists<float>(Solver<float>&, bool);
+template void build_lists<double>(Solver<double>&, bool);
 
 }  // namespace fmmb200

@@ -4,13 +4,13 @@
 // One warp owns one target leaf.  Its lanes split into groups of G (1, 2 or 4) so that a
 // small leaf still keeps the warp busy: each group holds one target body and its G lanes
 // take every G-th source; a leaf of 33..64 bodies gives each lane two targets that share
-// every staged source.  Source leaves stream through shared memory 32 bodies at a time
-// (one coalesced 16-byte load per lane); in FP32 the staged sources are taken two at a time
-// with the packed two-wide instructions of sm_100 (half the issue slots of the scalar pair
-// arithmetic).  The inner loop is FMA + one rsqrt per pair (no r^2 == 0 test outside the
-// target leaf itself), and each source leaf's plain partial sum is folded into a
-// compensated (TwoSum) accumulator, so the accumulation error does not grow with the number
-// of source leaves.  Pairs with r^2 == 0 are skipped, as the reference does (:149); the
+// every staged source.  Sources stream through shared memory 32 bodies at a time (one
+// coalesced 16-byte load per lane); in FP32 a chunk of 32 runs on across source leaves, and
+// the staged sources are taken two at a time with the packed two-wide instructions of
+// sm_100 (half the issue slots of the scalar pair arithmetic).  The inner loop is FMA + one
+// rsqrt per pair (no r^2 == 0 test away from the target leaf itself), and each chunk's (FP64:
+// each source leaf's) plain partial sum is folded into a compensated (TwoSum) accumulator,
+// so the accumulation error does not grow with the length of the list.  Pairs with r^2 == 0 are skipped, as the reference does (:149); the
 // result is per unit target charge (the reference multiplies by q_i in P2P and divides
 // again in L2P / normalize).
 #include <algorithm>
@@ -53,78 +53,46 @@ __device__ __forceinline__ void p2p_accum(const vec4<T>& sj, const vec4<T>& xi, 
   az = fma(dz, inv3, az);
 }
 
-// FP32 source leaf: the staged sources are taken two at a time with the packed two-wide
+// FP32 rows: the staged sources are taken two at a time with the packed two-wide
 // instructions of sm_100 (add.f32x2, mul.f32x2, fma.f32x2: one instruction for both, each
-// component rounded as the scalar operation, so each pair's terms are those of p2p_accum);
-// a target's two partial sums are added at the end of the leaf.  The warp's row holds
-// A[i] = (x, x', y, y') and B[i] = (z, z', q, q') for the sources 2i and 2i + 1; a missing
-// partner is a far-away zero charge, which adds exactly zero.
+// component rounded as the scalar operation, so each pair's terms are those of p2p_accum).
+// A warp's row holds A[i] = (x, x', y, y') and B[i] = (z, z', q, q') for the sources 2i and
+// 2i + 1 (A in float4 0..15, B in 16..31); a missing partner is a far-away zero charge,
+// which adds exactly zero.
+
+// the pairs of one staged row (np source pairs) on the lane's TPL targets, added to the
+// two-wide sums; nx, ny, nz are the negated target coordinates in both halves
 template <int TPL, bool EXACT, bool SHIFT>
-__device__ __forceinline__ void source_leaf_pairs(int lane, float4* row, int sub, int G, int j0,
-                                                  int nj, const vec4<float>* __restrict__ bodies,
-                                                  float eps2, const vec4<float>* xi, float* pot,
-                                                  float* ax, float* ay, float* az, float px,
-                                                  float py, float pz) {
-  float4* A = row;
-  float4* B = row + 16;
-  float2 nx[TPL], ny[TPL], nz[TPL], sp[TPL], sx[TPL], sy[TPL], sz[TPL];
-#pragma unroll
-  for (int u = 0; u < TPL; u++) {
-    nx[u] = make_float2(-xi[u].x, -xi[u].x);
-    ny[u] = make_float2(-xi[u].y, -xi[u].y);
-    nz[u] = make_float2(-xi[u].z, -xi[u].z);
-    sp[u] = sx[u] = sy[u] = sz[u] = make_float2(0.f, 0.f);
-  }
-  const float2 e2 = make_float2(eps2, eps2);
-  const float2 p2x = make_float2(px, px), p2y = make_float2(py, py), p2z = make_float2(pz, pz);
-  for (int jb = 0; jb < nj; jb += 32) {
-    const int cnt = min(32, nj - jb);
-    __syncwarp();
-    {
-      const vec4<float> b =
-          lane < cnt ? bodies[j0 + jb + lane] : make_v4<float>(1e30f, 1e30f, 1e30f, 0.f);
-      float* a = reinterpret_cast<float*>(&A[lane >> 1]);
-      float* c = reinterpret_cast<float*>(&B[lane >> 1]);
-      const int h = lane & 1;
-      a[h] = b.x;
-      a[2 + h] = b.y;
-      c[h] = b.z;
-      c[2 + h] = b.w;
-    }
-    __syncwarp();
-    const int np = (cnt + 1) >> 1;
+__device__ __forceinline__ void row_pairs(const float4* row, int sub, int G, int np,
+                                          const float2* nx, const float2* ny, const float2* nz,
+                                          float2 e2, float2 p2x, float2 p2y, float2 p2z,
+                                          float2* sp, float2* sx, float2* sy, float2* sz) {
+  const float4* A = row;
+  const float4* B = row + 16;
 #pragma unroll 2
-    for (int i = sub; i < np; i += G) {
-      const float4 a = A[i], c = B[i];
-      const float2 x2 = make_float2(a.x, a.y), y2 = make_float2(a.z, a.w);
-      const float2 z2 = make_float2(c.x, c.y), q2 = make_float2(c.z, c.w);
+  for (int i = sub; i < np; i += G) {
+    const float4 a = A[i], c = B[i];
+    const float2 x2 = make_float2(a.x, a.y), y2 = make_float2(a.z, a.w);
+    const float2 z2 = make_float2(c.x, c.y), q2 = make_float2(c.z, c.w);
 #pragma unroll
-      for (int u = 0; u < TPL; u++) {
-        float2 dx = __fadd2_rn(x2, nx[u]), dy = __fadd2_rn(y2, ny[u]), dz = __fadd2_rn(z2, nz[u]);
-        if (SHIFT) {
-          dx = __fadd2_rn(dx, p2x);
-          dy = __fadd2_rn(dy, p2y);
-          dz = __fadd2_rn(dz, p2z);
-        }
-        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
-        float2 inv;
-        inv.x = EXACT ? (r2.x > 0.f ? rsqrt_(r2.x) : 0.f) : rsqrt_ftz(r2.x);
-        inv.y = EXACT ? (r2.y > 0.f ? rsqrt_(r2.y) : 0.f) : rsqrt_ftz(r2.y);
-        const float2 qinv = __fmul2_rn(q2, inv);
-        const float2 inv3 = __fmul2_rn(__fmul2_rn(qinv, inv), inv);
-        sp[u] = __fadd2_rn(sp[u], qinv);
-        sx[u] = __ffma2_rn(dx, inv3, sx[u]);
-        sy[u] = __ffma2_rn(dy, inv3, sy[u]);
-        sz[u] = __ffma2_rn(dz, inv3, sz[u]);
+    for (int u = 0; u < TPL; u++) {
+      float2 dx = __fadd2_rn(x2, nx[u]), dy = __fadd2_rn(y2, ny[u]), dz = __fadd2_rn(z2, nz[u]);
+      if (SHIFT) {
+        dx = __fadd2_rn(dx, p2x);
+        dy = __fadd2_rn(dy, p2y);
+        dz = __fadd2_rn(dz, p2z);
       }
+      const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+      float2 inv;
+      inv.x = EXACT ? (r2.x > 0.f ? rsqrt_(r2.x) : 0.f) : rsqrt_ftz(r2.x);
+      inv.y = EXACT ? (r2.y > 0.f ? rsqrt_(r2.y) : 0.f) : rsqrt_ftz(r2.y);
+      const float2 qinv = __fmul2_rn(q2, inv);
+      const float2 inv3 = __fmul2_rn(__fmul2_rn(qinv, inv), inv);
+      sp[u] = __fadd2_rn(sp[u], qinv);
+      sx[u] = __ffma2_rn(dx, inv3, sx[u]);
+      sy[u] = __ffma2_rn(dy, inv3, sy[u]);
+      sz[u] = __ffma2_rn(dz, inv3, sz[u]);
     }
-  }
-#pragma unroll
-  for (int u = 0; u < TPL; u++) {
-    pot[u] = sp[u].x + sp[u].y;
-    ax[u] = sx[u].x + sx[u].y;
-    ay[u] = sy[u].x + sy[u].y;
-    az[u] = sz[u].x + sz[u].y;
   }
 }
 
@@ -135,10 +103,6 @@ __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32],
                                             int j0, int nj, const vec4<T>* __restrict__ bodies,
                                             T eps2, const vec4<T>* xi, T* pot, T* ax, T* ay,
                                             T* az, T px = 0, T py = 0, T pz = 0) {
-  if constexpr (sizeof(T) == 4) {
-    source_leaf_pairs<TPL, EXACT, SHIFT>(lane, reinterpret_cast<float4*>(sh[wl]), sub, G, j0,
-                                         nj, bodies, eps2, xi, pot, ax, ay, az, px, py, pz);
-  } else {
 #pragma unroll
   for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
   for (int jb = 0; jb < nj; jb += 32) {
@@ -153,7 +117,6 @@ __device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32],
       for (int u = 0; u < TPL; u++)
         p2p_accum<T, EXACT, SHIFT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u], px, py, pz);
     }
-  }
   }
 }
 
@@ -262,13 +225,193 @@ __device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], in
   }
 }
 
+// FP32 target leaf: the bodies of its source leaves, taken in list order, are staged 32 at
+// a time whatever the leaves' sizes (a chunk runs on into the next source leaf, and ends
+// early only where the periodic image changes or after 32 source leaves), so that the rows
+// are full and the per-chunk work (staging, the finite test, the compensated fold) is
+// shared by all of its source leaves.  The source leaves' descriptors (first body, count,
+// image) are read 32 at a time, one per lane; a lane finds the leaf of its chunk position
+// by a scan of the counts and a binary search over the lanes.  A chunk that holds bodies of
+// the target leaf itself is summed in the exact form; any other chunk in the fast form,
+// and again in the exact form (from the same row) if a sum is not finite, so the results
+// are those of the exact form throughout.
+template <bool COMP, int TPL>
+__device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int nb, int base,
+                                             int G, int s0, int s1,
+                                             const unsigned long long* __restrict__ pairs,
+                                             const int* __restrict__ ibody,
+                                             const int* __restrict__ nbody,
+                                             const vec4<float>* __restrict__ bodies, float eps2,
+                                             float cycle, vec4<float>* __restrict__ trg_s,
+                                             vec4<float>* __restrict__ trg_e) {
+  const unsigned full = 0xffffffffu;
+  const int tpp = 32 / G;
+  const int sub = lane % G;
+  int ti[TPL];
+  bool act[TPL];
+  float2 nx[TPL], ny[TPL], nz[TPL];
+  Comp<float> acc[TPL][4];
+#pragma unroll
+  for (int u = 0; u < TPL; u++) {
+    ti[u] = base + u * tpp + lane / G;
+    act[u] = ti[u] < nb;
+    const vec4<float> x = act[u] ? bodies[b0 + ti[u]] : make_v4<float>(0, 0, 0, 0);
+    nx[u] = make_float2(-x.x, -x.x);
+    ny[u] = make_float2(-x.y, -x.y);
+    nz[u] = make_float2(-x.z, -x.z);
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[u][d] = Comp<float>{0, 0};
+  }
+  const float2 e2 = make_float2(eps2, eps2);
+  float4* A = row;
+  float4* B = row + 16;
+  for (int sb = s0; sb < s1; sb += 32) {
+    // lane k: source leaf sb + k (image -1 past the end of the list)
+    int dj0 = 0, dnj = 0, dimg = -1;
+    if (sb + lane < s1) {
+      const unsigned src = (unsigned)pairs[sb + lane];
+      dj0 = ibody[pair_cell(src)];
+      dnj = nbody[pair_cell(src)];
+      dimg = pair_img(src);
+    }
+    int k = 0, o = 0;  // the chunk starts at body o of leaf k
+    while (k < 32) {
+      const int img = __shfl_sync(full, dimg, k);
+      if (img < 0) break;
+      const unsigned other = ~__ballot_sync(full, dimg == img) & (full << k);
+      const int cut = other ? __ffs(other) - 1 : 32;  // leaves k .. cut - 1 share the image
+      const int avail = lane >= k && lane < cut ? dnj - (lane == k ? o : 0) : 0;
+      int incl = avail;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(full, incl, d);
+        if (lane >= d) incl += v;
+      }
+      const int total = __shfl_sync(full, incl, 31);
+      const int cnt = min(32, total);
+      // f: the leaf of chunk position `lane` (the number of leaves whose counts end at or
+      // before it)
+      int f = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1)
+        if (__shfl_sync(full, incl, f + step - 1) <= lane) f += step;
+      const int ex = __shfl_sync(full, incl - avail, f);
+      const int jf = __shfl_sync(full, dj0 + (lane == k ? o : 0), f);
+      const int bj = jf + lane - ex;
+      const vec4<float> b =
+          lane < cnt ? bodies[bj] : make_v4<float>(1e30f, 1e30f, 1e30f, 0.f);
+      const bool self = __any_sync(full, lane < cnt && img == 0 && bj >= b0 && bj < b0 + nb);
+      __syncwarp();
+      {
+        float* a = reinterpret_cast<float*>(&A[lane >> 1]);
+        float* c = reinterpret_cast<float*>(&B[lane >> 1]);
+        const int h = lane & 1;
+        a[h] = b.x;
+        a[2 + h] = b.y;
+        c[h] = b.z;
+        c[2 + h] = b.w;
+      }
+      __syncwarp();
+      const int np = (cnt + 1) >> 1;
+      float2 sp[TPL], sx[TPL], sy[TPL], sz[TPL];
+      auto zero = [&]() {
+#pragma unroll
+        for (int u = 0; u < TPL; u++) sp[u] = sx[u] = sy[u] = sz[u] = make_float2(0.f, 0.f);
+      };
+      auto finite = [&]() {
+        bool bad = false;
+#pragma unroll
+        for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(sp[u].x + sp[u].y);
+        return !__any_sync(full, bad);
+      };
+      zero();
+      if (img != 0) {
+        float px, py, pz;
+        img_shift<float>(img, cycle, px, py, pz);
+        const float2 p2x = make_float2(px, px), p2y = make_float2(py, py),
+                     p2z = make_float2(pz, pz);
+        row_pairs<TPL, false, true>(row, sub, G, np, nx, ny, nz, e2, p2x, p2y, p2z, sp, sx, sy,
+                                    sz);
+        if (!finite()) {
+          zero();
+          row_pairs<TPL, true, true>(row, sub, G, np, nx, ny, nz, e2, p2x, p2y, p2z, sp, sx, sy,
+                                     sz);
+        }
+      } else {
+        const float2 z2 = make_float2(0.f, 0.f);
+        if (self) {
+          row_pairs<TPL, true, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx, sy,
+                                      sz);
+        } else {
+          row_pairs<TPL, false, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx, sy,
+                                       sz);
+          if (!finite()) {
+            zero();
+            row_pairs<TPL, true, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx,
+                                        sy, sz);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < TPL; u++) {
+        const float pot = sp[u].x + sp[u].y, ax = sx[u].x + sx[u].y, ay = sy[u].x + sy[u].y,
+                    az = sz[u].x + sz[u].y;
+        if (COMP) {
+          comp_add(acc[u][0], pot);
+          comp_add(acc[u][1], ax);
+          comp_add(acc[u][2], ay);
+          comp_add(acc[u][3], az);
+        } else {
+          acc[u][0].s += pot;
+          acc[u][1].s += ax;
+          acc[u][2].s += ay;
+          acc[u][3].s += az;
+        }
+      }
+      // the next chunk: past leaves k .. cut - 1, or inside the leaf holding position 32
+      if (total <= 32) {
+        k = cut;
+        o = 0;
+      } else {
+        const int kn = __popc(__ballot_sync(full, lane < cut && incl <= 32));
+        const int exn = __shfl_sync(full, incl - avail, kn);
+        o = (kn == k ? o : 0) + 32 - exn;
+        k = kn;
+      }
+    }
+  }
+  for (int o = 1; o < G; o <<= 1) {
+#pragma unroll
+    for (int u = 0; u < TPL; u++)
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        Comp<float> r;
+        r.s = __shfl_xor_sync(full, acc[u][d].s, o);
+        r.e = __shfl_xor_sync(full, acc[u][d].e, o);
+        if (COMP) comp_merge(acc[u][d], r);
+        else acc[u][d].s += r.s;
+      }
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int u = 0; u < TPL; u++)
+      if (act[u]) {
+        trg_s[b0 + ti[u]] =
+            make_v4<float>(acc[u][0].s, acc[u][1].s, acc[u][2].s, acc[u][3].s);
+        trg_e[b0 + ti[u]] =
+            make_v4<float>(acc[u][0].e, acc[u][1].e, acc[u][2].e, acc[u][3].e);
+      }
+  }
+}
+
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(32 * kP2PWarps)
     k_p2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ off,
           const unsigned long long* __restrict__ pairs, const int* __restrict__ ibody,
           const int* __restrict__ nbody, const vec4<T>* __restrict__ bodies, T eps2, T cycle,
           vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
-  __shared__ vec4<T> sh[kP2PWarps][32];
+  // one row of 32 sources per warp
+  __shared__ __align__(16) unsigned char smem[kP2PWarps][32 * sizeof(vec4<T>)];
   const int wl = threadIdx.x >> 5;
   const int w = blockIdx.x * kP2PWarps + wl;
   if (w >= nleaves) return;
@@ -277,13 +420,26 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
   const int b0 = ibody[c], nb = nbody[c];
   const int G = nb <= 8 ? 4 : (nb <= 16 ? 2 : 1);
   const int s0 = off[c], s1 = off[c + 1];
-  if (nb <= 32) {
-    p2p_leaf<T, COMP, 1>(lane, wl, sh, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
-                         cycle, trg_s, trg_e);
+  if constexpr (sizeof(T) == 4) {
+    float4* row = reinterpret_cast<float4*>(smem[wl]);
+    if (nb <= 32) {
+      p2p_leaf_f32<COMP, 1>(lane, row, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
+                            cycle, trg_s, trg_e);
+    } else {
+      for (int base = 0; base < nb; base += 64)
+        p2p_leaf_f32<COMP, 2>(lane, row, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
+                              eps2, cycle, trg_s, trg_e);
+    }
   } else {
-    for (int base = 0; base < nb; base += 64)
-      p2p_leaf<T, COMP, 2>(lane, wl, sh, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
-                           eps2, cycle, trg_s, trg_e);
+    vec4<T>(*sh)[32] = reinterpret_cast<vec4<T>(*)[32]>(&smem[0][0]);
+    if (nb <= 32) {
+      p2p_leaf<T, COMP, 1>(lane, wl, sh, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
+                           cycle, trg_s, trg_e);
+    } else {
+      for (int base = 0; base < nb; base += 64)
+        p2p_leaf<T, COMP, 2>(lane, wl, sh, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
+                             eps2, cycle, trg_s, trg_e);
+    }
   }
 }
 

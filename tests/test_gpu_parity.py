@@ -28,6 +28,10 @@ CASES = {
     "sph8_f64_plummer": ("spherical", 8, "f64", "plummer", 12000,
                          dict(ncrit=48, theta=0.4, use_ropt=1)),
     "sph4_f32_sphere": ("spherical", 4, "f32", "sphere", 20000, dict(ncrit=16, theta=0.5, use_ropt=0)),
+    # leaves of 1 to 196 bodies: FP32 P2P chunks that start inside a source leaf, and target
+    # leaves of more than 64 bodies (several passes of two targets per lane)
+    "sph6_f32_plummer_bigleaf": ("spherical", 6, "f32", "plummer", 20000,
+                                 dict(ncrit=200, theta=0.5, use_ropt=0)),
     "cart5_f32_sphere": ("cartesian", 5, "f32", "sphere", 30000, dict(ncrit=32, theta=0.5, use_ropt=0)),
     "cart4_f64_cube": ("cartesian", 4, "f64", "cube", 10000, dict(ncrit=16, theta=0.6, use_ropt=0)),
 }
@@ -223,6 +227,21 @@ def test_edge_cases(datasets):
     ok = np.isfinite(ref).all(axis=1)
     assert np.allclose(trg[ok], ref[ok], rtol=1e-9, atol=1e-9)
     assert np.array_equal(np.isfinite(trg), np.isfinite(ref))
+
+
+def test_edge_cases_f32(datasets):
+    """FP32: 100 coincident bodies beyond the depth cap (one leaf of 100 bodies at ncrit = 16,
+    its pairs at r^2 = 0 skipped) inside a random cloud, against the FP32 oracle."""
+    s = fmm.Solver(basis="spherical", P=6, theta=0.4, ncrit=16, use_ropt=0, precision="f32")
+    xr, qr = datasets.make("cube", 2000, seed=5, precision="f32")
+    xs = np.concatenate([xr, np.tile(np.array([[0.25, -0.125, 0.5]], xr.dtype), (100, 1))])
+    qs = np.concatenate([qr, np.full(100, np.float32(0.01), qr.dtype)])
+    trg = s.solve(xs, qs)
+    ref = Oracle("f32").run(xs, qs, P=6, theta=0.4, ncrit=16, kahan=1).trg()
+    assert np.array_equal(np.isfinite(trg), np.isfinite(ref))
+    ok = np.isfinite(ref).all(axis=1)
+    pot, acc = rel_l2(trg[ok], ref[ok])
+    assert pot < 2e-5 and acc < 2e-5, (pot, acc)
 
 
 def test_ncrit_one_and_reuse(datasets):

@@ -289,12 +289,21 @@ __device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int 
       }
       const int total = __shfl_sync(full, incl, 31);
       const int cnt = min(32, total);
-      // f: the leaf of chunk position `lane` (the number of leaves whose counts end at or
-      // before it)
-      int f = 0;
+      // f: the leaf of chunk position `lane`.  Each leaf of the chunk sets the bit of its
+      // first position; f is k plus the number of bits at or below `lane`, less one (with
+      // an empty leaf in the range, whose start would coincide with the next one's: the
+      // number of leaves whose counts end at or before `lane`, by binary search)
+      int f;
+      if (!__any_sync(full, lane >= k && lane < cut && avail == 0)) {
+        const unsigned starts =
+            __reduce_or_sync(full, avail > 0 && incl - avail < 32 ? 1u << (incl - avail) : 0u);
+        f = k + __popc(starts & (full >> (31 - lane))) - 1;
+      } else {
+        f = 0;
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1)
-        if (__shfl_sync(full, incl, f + step - 1) <= lane) f += step;
+        for (int step = 16; step >= 1; step >>= 1)
+          if (__shfl_sync(full, incl, f + step - 1) <= lane) f += step;
+      }
       const int ex = __shfl_sync(full, incl - avail, f);
       const int jf = __shfl_sync(full, dj0 + (lane == k ? o : 0), f);
       const int bj = jf + lane - ex;

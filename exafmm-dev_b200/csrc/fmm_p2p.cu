@@ -69,7 +69,7 @@ __device__ __forceinline__ void row_pairs(const float4* row, int sub, int G, int
                                           float2* sp, float2* sx, float2* sy, float2* sz) {
   const float4* A = row;
   const float4* B = row + 16;
-#pragma unroll 2
+#pragma unroll (4 / TPL)
   for (int i = sub; i < np; i += G) {
     const float4 a = A[i], c = B[i];
     const float2 x2 = make_float2(a.x, a.y), y2 = make_float2(a.z, a.w);

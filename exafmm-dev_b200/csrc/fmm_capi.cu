@@ -382,10 +382,6 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
     g_create_error = "mutual must be 0 or 1";
     return FMM_ERR_INVALID;
   }
-  if (cfg->images > 0 && cfg->basis != FMM_SPHERICAL) {
-    g_create_error = "periodic images are supported on the spherical basis only";
-    return FMM_ERR_NOT_SUPPORTED;
-  }
   std::vector<int> ords = cfg->basis == FMM_CARTESIAN ? cartesian_orders() : spherical_orders();
   if (std::find(ords.begin(), ords.end(), cfg->P) == ords.end()) {
     g_create_error = "expansion order P=" + std::to_string(cfg->P) + " not compiled for this basis";
@@ -491,7 +487,6 @@ int fmm_b200_set_mutual(fmm_b200_solver* h, int mutual) {
 int fmm_b200_set_periodic(fmm_b200_solver* h, int images, double cycle) {
   if (!h || !h->base) return FMM_ERR_INVALID;
   if (images < 0 || (images > 0 && !(cycle > 0.0))) return FMM_ERR_INVALID;
-  if (images > 0 && h->base->cfg.basis != FMM_SPHERICAL) return FMM_ERR_NOT_SUPPORTED;
   h->base->cfg.images = images;
   h->base->cfg.cycle = cycle;
   return FMM_OK;

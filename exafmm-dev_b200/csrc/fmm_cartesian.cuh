@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(128)
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_cm2l(int ncells, const int* __restrict__ off, const unsigned long long* __restrict__ pairs,
-           const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L, int ncoef) {
+           const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L, int ncoef,
+           T cycle) {
   constexpr int NT = cart::NT(P);
   const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = lane_id();
@@ -154,9 +155,13 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int t = 0; t < NT; t++) acc[t] = 0;
   for (int s = s0 + lane; s < s1; s += 32) {
-    const int j = pair_cell((unsigned)pairs[s]);  // no periodic images on this basis
+    const unsigned src = (unsigned)pairs[s];
+    const int j = pair_cell(src);
+    T px, py, pz;  // periodic shift of the source (0 without images)
+    img_shift<T>(pair_img(src), cycle, px, py, pz);
     const vec4<T> Xj = cX[j];
-    const T dx = Xi.x - Xj.x, dy = Xi.y - Xj.y, dz = Xi.z - Xj.z;
+    // dX = Xi - Xj - Xperiodic (kernels/LaplaceCartesianCPU.cxx:658-673)
+    const T dx = Xi.x - Xj.x - px, dy = Xi.y - Xj.y - py, dz = Xi.z - Xj.z - pz;
     const T invR2 = T(1) / (dx * dx + dy * dy + dz * dz);
     T C[NT];
     cart::derivs<T, P>(C, dx, dy, dz, invR2, sqrt(invR2));
@@ -248,7 +253,8 @@ template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
 }
 template <typename T, int P> static void m2l_(Solver<T>& s) {
   k_cm2l<T, P><<<ceil_div(s.ncells, 4), 128, 0, s.stream>>>(s.ncells, s.m2l_off.p, s.m2l.p,
-                                                              s.cX.p, s.M.p, s.L.p, s.ncoef);
+                                                              s.cX.p, s.M.p, s.L.p, s.ncoef,
+                                                              (T)s.cfg.cycle);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
@@ -264,10 +270,138 @@ template <typename T, int P> static void l2p_(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
 }
 
+// ---------------------------------------------------------------- periodic far field
+// Traversal::traversePeriodic (include/traversal.h:127-185) on this basis, one root per
+// solve of the batch.  Per sub-level of images: the periodic cell (the root's multipole, at
+// the root's centre) sends M2L into the root from the 26 x 27 shifts (3 ix + cx, ...) cycle,
+// |i|, |c| <= 1, (ix, iy, iz) != 0 (k_cper_m2l: one thread per shift, the whole local
+// expansion in registers as in k_cm2l; k_cper_reduce adds the 702 terms to the root's local
+// expansion in the reference's loop order); then the periodic cell becomes the M2M of its
+// 26 copies shifted by (ix, iy, iz) cycle, (ix, iy, iz) != 0 (k_cper_m2m; the unshifted copy
+// is not among them, as in the reference), and the period grows three times.
+constexpr int kCPerShifts = 26 * 27;
+
+__device__ __forceinline__ void cper_outer(int o, int& ix, int& iy, int& iz) {
+  const int q = o < 13 ? o : o + 1;  // the 26 of {-1,0,1}^3 other than (0,0,0), loop order
+  ix = q / 9 - 1;
+  iy = (q / 3) % 3 - 1;
+  iz = q % 3 - 1;
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(128)
+    k_cper_m2l(int nroots, const T* __restrict__ Mp, T cycle, int ncoef, T* __restrict__ contrib) {
+  constexpr int NT = cart::NT(P);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nroots * kCPerShifts) return;
+  const int r = t / kCPerShifts, sidx = t % kCPerShifts;
+  int ix, iy, iz;
+  cper_outer(sidx / 27, ix, iy, iz);
+  const int c = sidx % 27, cx = c / 9 - 1, cy = (c / 3) % 3 - 1, cz = c % 3 - 1;
+  // dX = Ci0->X - Ci->X - Xperiodic with Ci at the root's own centre: -Xperiodic
+  const T dx = T(0) - (T)(ix * 3 + cx) * cycle, dy = T(0) - (T)(iy * 3 + cy) * cycle,
+          dz = T(0) - (T)(iz * 3 + cz) * cycle;
+  const T invR2 = T(1) / (dx * dx + dy * dy + dz * dz);
+  T C[NT], acc[NT];
+  cart::derivs<T, P>(C, dx, dy, dz, invR2, sqrt(invR2));
+#pragma unroll
+  for (int u = 0; u < NT; u++) acc[u] = 0;
+  cart::m2l_pair<T, P>(C, Mp + (size_t)r * ncoef, acc);
+  T* out = contrib + (size_t)t * NT;
+#pragma unroll
+  for (int u = 0; u < NT; u++) out[u] = acc[u];
+}
+
+template <typename T>
+__global__ void k_cper_reduce(int nroots, int nt, const int* __restrict__ root_cell,
+                              const T* __restrict__ contrib, T* __restrict__ L, int ncoef) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nroots * nt) return;
+  const int r = t / nt, e = t % nt;
+  T acc = L[(size_t)root_cell[r] * ncoef + e];
+  for (int q = 0; q < kCPerShifts; q++) acc += contrib[((size_t)r * kCPerShifts + q) * nt + e];
+  L[(size_t)root_cell[r] * ncoef + e] = acc;
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(32)
+    k_cper_m2m(const T* __restrict__ Mp, const int* __restrict__ root_cell,
+               const vec4<T>* __restrict__ cX, T cycle, int ncoef, T* __restrict__ Mout) {
+  constexpr int NT = cart::NT(P), KO = (NT + 31) / 32;
+  __shared__ T sc[NT], sm[NT];
+  const int lane = lane_id(), r = blockIdx.x;
+  const vec4<T> X = cX[root_cell[r]];
+  for (int t = lane; t < NT; t += 32) sm[t] = Mp[(size_t)r * ncoef + t];
+  T acc[KO];
+  int ox[KO], oy[KO], oz[KO];
+#pragma unroll
+  for (int i = 0; i < KO; i++) {
+    acc[i] = 0;
+    cart::mi_of(lane + 32 * i, ox[i], oy[i], oz[i]);
+  }
+  for (int o = 0; o < 26; o++) {
+    int ix, iy, iz;
+    cper_outer(o, ix, iy, iz);
+    // child centre X + (ix, iy, iz) cycle, then dX = Xparent - Xchild as the reference rounds
+    const T xc = X.x + (T)ix * cycle, yc = X.y + (T)iy * cycle, zc = X.z + (T)iz * cycle;
+    {
+      T C[NT];
+      C[0] = 1;
+      cart::power<T, P>(C, X.x - xc, X.y - yc, X.z - zc);
+      __syncwarp();
+      spread_c<T, NT>(C, sc, lane);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KO; i++)
+      if (lane + 32 * i < NT) acc[i] += cart::m2m_term<T>(ox[i], oy[i], oz[i], sc, sm);
+  }
+#pragma unroll
+  for (int i = 0; i < KO; i++)
+    if (lane + 32 * i < NT) Mout[(size_t)r * ncoef + lane + 32 * i] = acc[i];
+}
+
+template <typename T>
+__global__ void k_cper_init(int nroots, const int* __restrict__ root_cell,
+                            const T* __restrict__ M, int ncoef, T* __restrict__ Mp) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nroots * ncoef) return;
+  const int r = t / ncoef, e = t % ncoef;
+  Mp[t] = M[(size_t)root_cell[r] * ncoef + e];
+}
+
+template <typename T, int P> static void cperiodic_(Solver<T>& s) {
+  constexpr int NT = cart::NT(P);
+  const int R = s.nroots;
+  if (s.cfg.images < 2 || R == 0) return;
+  s.pM.ensure((size_t)R * s.ncoef);
+  s.pM2.ensure((size_t)R * s.ncoef);
+  s.pC.ensure((size_t)R * kCPerShifts * NT);
+  s.c_root_cells.ensure(R);
+  FMM_CUDA(cudaMemcpyAsync(s.c_root_cells.p, s.root_cell.data(), sizeof(int) * R,
+                           cudaMemcpyHostToDevice, s.stream));
+  k_cper_init<T><<<ceil_div((long long)R * s.ncoef, 256), 256, 0, s.stream>>>(
+      R, s.c_root_cells.p, s.M.p, s.ncoef, s.pM.p);
+  FMM_LAUNCH_CHECK();
+  T cycle = (T)s.cfg.cycle;
+  for (int level = 0; level < s.cfg.images - 1; level++) {
+    k_cper_m2l<T, P><<<ceil_div(R * kCPerShifts, 128), 128, 0, s.stream>>>(R, s.pM.p, cycle,
+                                                                            s.ncoef, s.pC.p);
+    FMM_LAUNCH_CHECK();
+    k_cper_reduce<T><<<ceil_div((long long)R * NT, 128), 128, 0, s.stream>>>(
+        R, NT, s.c_root_cells.p, s.pC.p, s.L.p, s.ncoef);
+    FMM_LAUNCH_CHECK();
+    k_cper_m2m<T, P><<<R, 32, 0, s.stream>>>(s.pM.p, s.c_root_cells.p, s.cX.p, cycle, s.ncoef,
+                                             s.pM2.p);
+    FMM_LAUNCH_CHECK();
+    std::swap(s.pM, s.pM2);
+    cycle = cycle * (T)3;
+  }
+}
 
 // fill the dispatch table for one (precision, order); one object file per instantiation
 template <typename T, int P> void cart_fill(ExpansionOps<T>* ops) {
-  ops->periodic = nullptr;  // periodic images are spherical-basis only
+  ops->periodic = &cperiodic_<T, P>;
   ops->p2m = &p2m_<T, P>;
   ops->m2m_level = &m2m_<T, P>;
   ops->m2l = &m2l_<T, P>;

@@ -32,7 +32,7 @@ extern "C" {
 #define FMM_OK 0
 #define FMM_ERR_INVALID 1        /* bad argument or configuration */
 #define FMM_ERR_CUDA 2           /* CUDA runtime error (message in fmm_b200_last_error) */
-#define FMM_ERR_NOT_SUPPORTED 3  /* e.g. periodic images > 0 */
+#define FMM_ERR_NOT_SUPPORTED 3  /* e.g. periodic images with separate target/source sets */
 #define FMM_ERR_NO_MEMORY 4      /* device allocation failed */
 #define FMM_ERR_STATE 5          /* stage called out of order */
 #define FMM_ERR_NO_DEVICE 6      /* no CUDA device / kernels not built for it */
@@ -59,7 +59,7 @@ typedef struct fmm_b200_config {
   int images;      /* periodic image levels (Traversal::images, include/traversal.h:21):
                     * 0 open boundary; k > 0: the 27 nearest copies of the box through the
                     * tree and k - 1 levels of 3x3x3 super-cells of copies through the root
-                    * multipole (traversePeriodic); spherical basis only */
+                    * multipole (traversePeriodic); either basis */
   int device;      /* CUDA device ordinal */
   double cycle;    /* period of the box when images > 0 (dualTreeTraversal's cycle) */
   int mutual;      /* dualTreeTraversal's mutual flag (include/traversal.h:240): each unordered

@@ -51,9 +51,9 @@ def test_create_validates_before_touching_a_device():
     h = C.c_void_p()
     cfg.images = 1
     cfg.basis = fmm.CARTESIAN
-    cfg.P = 5
-    assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_NOT_SUPPORTED
-    assert b"periodic" in lib.fmm_b200_last_error(None)
+    cfg.P = 2
+    assert lib.fmm_b200_create(C.byref(cfg), C.byref(h)) == fmm.FMM_ERR_INVALID
+    assert b"expansion order" in lib.fmm_b200_last_error(None)
     cfg.basis = fmm.SPHERICAL
     cfg.P = 10
     cfg.cycle = 0.0

@@ -310,9 +310,6 @@ def test_timings_and_errors(datasets):
     s.solve(x, q)
     t = s.timings()
     assert t["total"] > 0 and t["m2l"] > 0 and t["p2p"] > 0
-    with pytest.raises(fmm.FmmError) as e:
-        fmm.Solver(basis="cartesian", P=5, images=1)
-    assert e.value.code == fmm.FMM_ERR_NOT_SUPPORTED
     with pytest.raises(fmm.FmmError):
         fmm.Solver(P=3)
 

@@ -13,19 +13,22 @@ import os
 import numpy as np
 import pytest
 
-from oracle import Oracle, rel_l2
+from oracle import CARTESIAN, SPHERICAL, Oracle, rel_l2
 
 pytestmark = pytest.mark.gpu
 fmm = importlib.import_module("exafmm-dev_b200")
 
 
-@pytest.mark.parametrize("prec,images,P", [("f64", 1, 6), ("f64", 3, 6), ("f32", 2, 8),
-                                           ("f32", 4, 10)])
-def test_periodic_matches_oracle(prec, images, P, datasets):
+@pytest.mark.parametrize("prec,images,P,basis", [
+    ("f64", 1, 6, "spherical"), ("f64", 3, 6, "spherical"), ("f32", 2, 8, "spherical"),
+    ("f32", 4, 10, "spherical"), ("f64", 1, 5, "cartesian"), ("f64", 3, 5, "cartesian"),
+    ("f32", 2, 6, "cartesian")])
+def test_periodic_matches_oracle(prec, images, P, basis, datasets):
     x, q = datasets.make("cube", 6000, seed=21, precision=prec)
     kw = dict(ncrit=32, theta=0.4, use_ropt=0)
-    o = Oracle(prec).run(x, q, P=P, kahan=int(prec == "f32"), images=images, cycle=2.0, **kw)
-    s = fmm.Solver(P=P, precision=prec, images=images, cycle=2.0, **kw)
+    o = Oracle(prec).run(x, q, P=P, kahan=int(prec == "f32"), images=images, cycle=2.0,
+                         basis=SPHERICAL if basis == "spherical" else CARTESIAN, **kw)
+    s = fmm.Solver(basis=basis, P=P, precision=prec, images=images, cycle=2.0, **kw)
     s.set_bodies(x, q)
     s.build_tree()
     s.upward_pass()

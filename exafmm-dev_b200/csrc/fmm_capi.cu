@@ -435,7 +435,7 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
                          &s.coff,     &s.leaves,   &s.idx,      &s.idx2,    &s.scal,       \
                          &s.c_iparent, &s.c_ichild, &s.c_nchild, &s.c_ibody, &s.c_nbody,   \
                          &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off, &s.seg_cnt,    \
-                         &s.d_lvl,    &s.seg_cnt2};                                        \
+                         &s.d_lvl,    &s.seg_cnt2, &s.body_leaf};                          \
     for (auto* a : ia) a->release();                                                       \
     s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
     s.c_info.release();                                                                    \

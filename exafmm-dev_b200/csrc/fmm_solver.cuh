@@ -118,6 +118,7 @@ struct SolverBase {
   int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
+  DevArr<int> body_leaf;  // the leaf cell of each body (tree order), written by P2M
   DevArr<int> seg_cnt;  // pairs per target while a list is grouped by target
   // the P2P list's grouping when it runs on the side stream beside M2L (whole solves)
   DevArr<int> seg_cnt2;

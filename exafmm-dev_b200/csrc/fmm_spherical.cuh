@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(32 * P2MCfg<T, P>::W)
     k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
           const int* __restrict__ nbody, vec4<T>* __restrict__ cX,
           const vec4<T>* __restrict__ bodies, T* __restrict__ M, int ncoef, int use_rmax,
-          T theta, int write_r) {
+          T theta, int write_r, int* __restrict__ body_leaf) {
   constexpr int NT = sph::NT(P), NC = 2 * NT, RS = NC | 1, KA = (NC + 31) / 32;
   constexpr int W = P2MCfg<T, P>::W;
   __shared__ T rows[W][32 * RS];
@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(32 * P2MCfg<T, P>::W)
     const int cnt = min(32, nb - base);
     __syncwarp();
     if (lane < cnt) {
+      body_leaf[b0 + base + lane] = c;
       const vec4<T> b = bodies[b0 + base + lane];
       const T dx = b.x - C.x, dy = b.y - C.y, dz = b.z - C.z;
       T yr[NT], yi[NT];
@@ -554,48 +555,39 @@ __global__ void __launch_bounds__(32 * SphCfg<T>::W)
   }
 }
 
-// ---------------------------------------------------------------- L2P
-// Half a warp per leaf (two leaves per warp), lane per body: most leaves hold fewer than
-// 32 bodies, so a whole warp per leaf would leave half its lanes idle.
+// L2P with one thread per body (tree order), its leaf from the map P2M wrote, the leaf's
+// local expansion read through L1 (the bodies of a warp share one to three leaves): every
+// lane busy whatever the leaf sizes; the arithmetic per body is that of k_l2p
 template <typename T, int P>
-__global__ void __launch_bounds__(32 * SphCfg<T>::W)
-    k_l2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
-          const int* __restrict__ nbody, const vec4<T>* __restrict__ cX,
-          const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
-          vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
-  constexpr int NT = sph::NT(P), NC = 2 * NT;
-  constexpr int W = SphCfg<T>::W;
-  __shared__ T sl[W][2][NC];
-  const int wl = threadIdx.x >> 5, lane = lane_id(), h = lane >> 4, hl = lane & 15;
-  const int w = 2 * (blockIdx.x * W + wl) + h;
-  const int c = w < nleaves ? leaves[w] : 0;
-  const int b0 = w < nleaves ? ibody[c] : 0, nb = w < nleaves ? nbody[c] : 0;
+__global__ void __launch_bounds__(128)
+    k_l2p_bodies(int n, const int* __restrict__ body_leaf, const vec4<T>* __restrict__ cX,
+                 const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
+                 vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = body_leaf[i];
   const vec4<T> C = cX[c];
-  if (w < nleaves)
-    for (int t = hl; t < NC; t += 16) sl[wl][h][t] = L[(size_t)c * ncoef + t];
-  __syncwarp();
-  for (int i = hl; i < nb; i += 16) {
-    const vec4<T> b = bodies[b0 + i];
-    T pot, gx, gy, gz;
-    sph::l2p_body<T, P>(b.x - C.x, b.y - C.y, b.z - C.z, sl[wl][h], pot, gx, gy, gz);
-    vec4<T> s = trg_s[b0 + i], e = trg_e[b0 + i];
-    Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
-    comp_add(a0, pot);
-    comp_add(a1, gx);
-    comp_add(a2, gy);
-    comp_add(a3, gz);
-    trg_s[b0 + i] = make_v4<T>(a0.s, a1.s, a2.s, a3.s);
-    trg_e[b0 + i] = make_v4<T>(a0.e, a1.e, a2.e, a3.e);
-  }
+  const vec4<T> b = bodies[i];
+  T pot, gx, gy, gz;
+  sph::l2p_body<T, P>(b.x - C.x, b.y - C.y, b.z - C.z, L + (size_t)c * ncoef, pot, gx, gy, gz);
+  vec4<T> s = trg_s[i], e = trg_e[i];
+  Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
+  comp_add(a0, pot);
+  comp_add(a1, gx);
+  comp_add(a2, gy);
+  comp_add(a3, gz);
+  trg_s[i] = make_v4<T>(a0.s, a1.s, a2.s, a3.s);
+  trg_e[i] = make_v4<T>(a0.e, a1.e, a2.e, a3.e);
 }
 
 // ---------------------------------------------------------------- dispatch
 template <typename T, int P> static void p2m_(Solver<T>& s) {
   constexpr int W = P2MCfg<T, P>::W;
   if (!s.nleaves) return;
+  s.body_leaf.ensure(std::max(s.n, 1));
   k_p2m<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.M.p, s.ncoef,
-      s.cfg.use_rmax, (T)s.cfg.theta, s.write_r);
+      s.cfg.use_rmax, (T)s.cfg.theta, s.write_r, s.body_leaf.p);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
@@ -635,11 +627,9 @@ template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
   }
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
-  constexpr int W = SphCfg<T>::W;
   if (!s.nleaves) return;
-  k_l2p<T, P><<<ceil_div(s.nleaves, 2 * W), 32 * W, 0, s.stream>>>(
-      s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef,
-      s.trg_s.p, s.trg_e.p);
+  k_l2p_bodies<T, P><<<ceil_div(s.n, 128), 128, 0, s.stream>>>(
+      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p);
   FMM_LAUNCH_CHECK();
 }
 

@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(32 * CartCfg<T, P>::W)
     k_cp2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
            const int* __restrict__ nbody, vec4<T>* __restrict__ cX,
            const vec4<T>* __restrict__ bodies, T* __restrict__ M, int ncoef, int use_rmax,
-           T theta) {
+           T theta, int* __restrict__ body_leaf) {
   constexpr int NT = cart::NT(P), RS = CartCfg<T, P>::RS, KA = (NT + 31) / 32;
   constexpr int W = CartCfg<T, P>::W;
   __shared__ T rows[W][32 * RS];
@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(32 * CartCfg<T, P>::W)
     const int cnt = min(32, nb - base);
     __syncwarp();
     if (lane < cnt) {
+      body_leaf[b0 + base + lane] = c;
       const vec4<T> b = bodies[b0 + base + lane];
       T C[NT];
       C[0] = b.w;
@@ -205,43 +206,37 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// L2P with one thread per body (tree order), its leaf from the map P2M wrote, the leaf's
+// local expansion read through L1 (the bodies of a warp share one to three leaves)
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
-    k_cl2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
-           const int* __restrict__ nbody, const vec4<T>* __restrict__ cX,
-           const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
-           vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
-  constexpr int NT = cart::NT(P), W = 4;
-  __shared__ T sl[W][NT];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int w = blockIdx.x * W + wl;
-  if (w >= nleaves) return;
-  const int c = leaves[w];
-  const int b0 = ibody[c], nb = nbody[c];
+    k_cl2p_bodies(int n, const int* __restrict__ body_leaf, const vec4<T>* __restrict__ cX,
+                  const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
+                  vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = body_leaf[i];
   const vec4<T> X = cX[c];
-  for (int t = lane; t < NT; t += 32) sl[wl][t] = L[(size_t)c * ncoef + t];
-  __syncwarp();
-  for (int i = lane; i < nb; i += 32) {
-    const vec4<T> b = bodies[b0 + i];
-    T pot, gx, gy, gz;
-    cart::l2p_body<T, P>(b.x - X.x, b.y - X.y, b.z - X.z, sl[wl], pot, gx, gy, gz);
-    vec4<T> s = trg_s[b0 + i], e = trg_e[b0 + i];
-    Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
-    comp_add(a0, pot);
-    comp_add(a1, gx);
-    comp_add(a2, gy);
-    comp_add(a3, gz);
-    trg_s[b0 + i] = make_v4<T>(a0.s, a1.s, a2.s, a3.s);
-    trg_e[b0 + i] = make_v4<T>(a0.e, a1.e, a2.e, a3.e);
-  }
+  const vec4<T> b = bodies[i];
+  T pot, gx, gy, gz;
+  cart::l2p_body<T, P>(b.x - X.x, b.y - X.y, b.z - X.z, L + (size_t)c * ncoef, pot, gx, gy, gz);
+  vec4<T> s = trg_s[i], e = trg_e[i];
+  Comp<T> a0 = {s.x, e.x}, a1 = {s.y, e.y}, a2 = {s.z, e.z}, a3 = {s.w, e.w};
+  comp_add(a0, pot);
+  comp_add(a1, gx);
+  comp_add(a2, gy);
+  comp_add(a3, gz);
+  trg_s[i] = make_v4<T>(a0.s, a1.s, a2.s, a3.s);
+  trg_e[i] = make_v4<T>(a0.e, a1.e, a2.e, a3.e);
 }
 
 template <typename T, int P> static void p2m_(Solver<T>& s) {
   constexpr int W = CartCfg<T, P>::W;
   if (!s.nleaves) return;
+  s.body_leaf.ensure(std::max(s.n, 1));
   k_cp2m<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.M.p, s.ncoef,
-      s.cfg.use_rmax, (T)s.cfg.theta);
+      s.cfg.use_rmax, (T)s.cfg.theta, s.body_leaf.p);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
@@ -264,9 +259,8 @@ template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   if (!s.nleaves) return;
-  k_cl2p<T, P><<<ceil_div(s.nleaves, 4), 128, 0, s.stream>>>(
-      s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef,
-      s.trg_s.p, s.trg_e.p);
+  k_cl2p_bodies<T, P><<<ceil_div(s.n, 128), 128, 0, s.stream>>>(
+      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p);
   FMM_LAUNCH_CHECK();
 }
 

@@ -395,7 +395,7 @@ __device__ __forceinline__ void warp_sort_range(const unsigned* __restrict__ key
 }
 
 // one warp per target with at most kSegWarpCap pairs
-__global__ void __launch_bounds__(32 * kSegWarps)
+__global__ void __launch_bounds__(32 * kSegWarps, 5)
     k_seg_sort_warp(int ncells, const int* __restrict__ off, const unsigned* __restrict__ keys,
                     int b, unsigned long long* __restrict__ out) {
   const int c = blockIdx.x * kSegWarps + (threadIdx.x >> 5);

@@ -11,14 +11,21 @@ use_rmax = use_ropt = 1, FP32 expansions with compensated potential/gradient sum
   outside its events.
 * e2e: the same solve through the host C ABI (fmm_b200_solve_host: pinned double x, q in,
   p, f out, host<->device copies inside the timed region).
-* roofline: the M2L kernel (the largest phase), FP32-pipe bound: algorithmic flops per cell
-  pair of the contraction in the source's azimuthal frame, 4 * sum_{j<P} (j+1)(P-j)^2 (two
-  real multiply-adds per term) + 6 (P(P+1)/2 - P) (rotating the source) + 8 (P(P+1)/2 - P)
-  + 2 P (rotating the outputs back) = 5,490 at P = 10, over its event-timed duration,
-  against the FP32 FMA peak measured on the same GPU by fmm_b200_fp32_peak.
+* roofline: the M2L kernel (the largest phase), FP32-pipe bound.  achieved = the algorithmic
+  flops of the reference's M2L loop, 8 sum_{j<P} (j+1)(P-j)^2 per cell pair (a complex
+  multiply-add = 8 flops; 9,680 at P = 10), times the run's M2L pairs, over the M2L phase's
+  event-timed duration; peak = the nominal FP32 rate 148 SMs x 128 lanes x 2 flops x the SM
+  clock sampled during the timed solves (the FMA throughput measured by fmm_b200_fp32_peak
+  is reported beside it).  The flops the kernel actually executes (the contraction in the
+  source's azimuthal frame: 4 sum (j+1)(P-j)^2 + 14 (P(P+1)/2 - P) + 2 P = 5,490 per pair
+  at P = 10) are reported as executed_tflops.
 * cpu_baseline: the reference exafmm-dev CPU FMM (oracle/_ref/perf, compiled from the
-  reference's sources) on a bounded sample of the same workload with all host threads.
-* --impl reference: that reference CPU FMM as the timed arm (rank 0 only).
+  reference's sources) on the same workload (N = 2^20) with all host threads, median of 3
+  runs, per phase.
+* --impl reference: that reference CPU FMM as the timed arm (rank 0 only), same workload.
+* cartesian (rank 0): BASELINE config 3, Cartesian P = 5, theta = 0.5, ncrit = 32, 4,194,304
+  bodies on the unit sphere surface, FP32: device time, phases, M2L / P2P work and roofline,
+  accuracy vs FP64 direct, and the reference CPU build on the same config.
 * multi-GPU (torchrun): replicas only; every rank solves its own instance, no collective
   on the data path (a barrier and a max-reduction of the timings only).
 * batched (rank 0): 256 independent solves of uneven N in one batched call (a forest of
@@ -45,16 +52,33 @@ WORKLOAD = dict(dist="plummer", n=1 << 20, basis="spherical", P=10, theta=0.35, 
                 nspawn=1000, use_rmax=1, use_ropt=1)
 WORKLOAD_NAME = "plummer_N1048576_spherical_P10_theta0.35_ncrit64_fp32"
 REF_CONFIG = "sph_p10_f32k_mass"   # reference build: float + KAHAN + MASS (q = 1/N)
-REF_SAMPLE_N = 1 << 18            # bodies per reference step (bounded CPU sample)
+REF_N = 1 << 20                   # the reference arm runs the headline workload itself
+CART = dict(dist="sphere", n=1 << 22, basis="cartesian", P=5, theta=0.5, ncrit=32, nspawn=1000,
+            use_rmax=1, use_ropt=0)
+CART_NAME = "sphere_N4194304_cartesian_P5_theta0.5_ncrit32_fp32"
+CART_REF_CONFIG = "cart_p5_f32"
+SMS, FP32_LANES = 148, 128         # B200: SMs, FP32 lanes per SM
 
 
 def m2l_flops_per_pair(P, basis="spherical"):
+    """Algorithmic M2L flops per cell pair: spherical 8 sum_{j<P} (j+1)(P-j)^2 (the reference
+    loop, LaplaceSphericalCPU.cxx:156-190, one complex multiply-add = 8 flops); Cartesian 2
+    per multiply-add of the truncated tensor contraction (420 at P = 5)."""
     if basis == "spherical":
-        rot = P * (P + 1) // 2 - P
-        return 4 * sum((j + 1) * (P - j) ** 2 for j in range(P)) + 6 * rot + 8 * rot + 2 * P
-    # Cartesian: 2 flops per multiply-add of the truncated tensor contraction
+        return 8 * sum((j + 1) * (P - j) ** 2 for j in range(P))
     nt = lambda p: p * (p + 1) * (p + 2) // 6
     return 2 * sum(((o + 1) * (o + 2) // 2) * nt(P - o) for o in range(P))
+
+
+def m2l_executed_flops_per_pair(P):
+    """Flops the spherical M2L kernel executes per pair: the contraction in the source's
+    azimuthal frame (two real multiply-adds per term) plus the source and output rotations."""
+    rot = P * (P + 1) // 2 - P
+    return 4 * sum((j + 1) * (P - j) ** 2 for j in range(P)) + 14 * rot + 2 * P
+
+
+def nominal_fp32_tflops(sm_mhz):
+    return SMS * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
 
 
 def dist_env():
@@ -120,14 +144,26 @@ def reference_lib():
     return oracle, oracle.Reference(REF_CONFIG, "perf")
 
 
-def run_reference_sample(ref, datasets, n, threads, seed=43):
-    x, q = datasets.make(WORKLOAD["dist"], n, seed=seed, precision="f32")
+def run_reference(ref, x, q, wl, threads):
+    """One reference CPU solve of workload wl (same parameters as the GPU arm): wall seconds
+    and the reference's own per-phase times."""
     t0 = time.perf_counter()
-    run = ref.run(x, q, ncrit=WORKLOAD["ncrit"], nspawn=WORKLOAD["nspawn"],
-                  theta=WORKLOAD["theta"], use_rmax=1, use_ropt=1, record=False,
-                  threads=threads)
+    run = ref.run(x, q, ncrit=wl["ncrit"], nspawn=wl["nspawn"], theta=wl["theta"],
+                  use_rmax=wl["use_rmax"], use_ropt=wl["use_ropt"], record=False, threads=threads)
     wall = time.perf_counter() - t0
     return wall, run.times()
+
+
+def reference_median(ref, x, q, wl, threads, runs=3):
+    """Median of `runs` reference solves: wall seconds and per-phase seconds (each phase's
+    own median)."""
+    walls, phases = [], []
+    for _ in range(runs):
+        w, t = run_reference(ref, x, q, wl, threads)
+        walls.append(w)
+        phases.append(t)
+    med = {k: float(np.median([t[k] for t in phases])) for k in phases[0]}
+    return float(np.median(walls)), med
 
 
 # use_ropt = 0 for the mixed workloads: the cube solves carry zero net charge, for which the
@@ -135,8 +171,14 @@ def run_reference_sample(ref, datasets, n, threads, seed=43):
 # acceptance test, turning those solves into direct sums (the reference does the same)
 BATCH = dict(solves=256, n_min=1000, n_max=200000, P=8, theta=0.4, ncrit=64, nspawn=1000,
              use_ropt=0)
-SERVE = dict(requests=48, n_min=1000, n_max=1000000, orders=(6, 8, 10), theta=0.4, ncrit=64,
-             use_ropt=0, workers=3, max_batch=64, hbm_budget_gb=60.0, load=(0.3, 0.6, 0.9))
+# the same batch at the opening angle that holds every solve to rel-L2 <= 1e-4
+BATCH_THETA_1E4 = 0.3
+# serving: the opening angle per order that holds every request to rel-L2 <= 1e-4 of potential
+# and gradient (measured on zero-net-charge cubes and Plummer spheres of 1e3..1e6 bodies with
+# the reference's FP32 + Kahan build: worst 4.1e-5 at P = 6, 2.6e-5 at P = 8, 2.1e-5 at P = 10)
+SERVE = dict(requests=48, n_min=1000, n_max=1000000, orders=(6, 8, 10),
+             theta={6: 0.22, 8: 0.30, 10: 0.35}, ncrit=64, use_ropt=0, workers=3, max_batch=64,
+             hbm_budget_gb=60.0, load=(0.3, 0.6, 0.9), passes=3, acc_min_n=10000)
 
 
 def log_uniform_sizes(rng, count, lo, hi):
@@ -152,7 +194,9 @@ def rel_err(got, ref):
 def bench_batched(fmm, datasets, torch, dev, stream, flush, device, steps):
     """256 independent solves (N log-uniform in [1e3, 2e5], cube / Plummer / sphere surface
     by i mod 3, spherical P = 8, theta = 0.4, FP32 + compensation) in one batched call
-    (a forest of independent trees) against the same solves one call each."""
+    (a forest of independent trees) against the same solves one call each; accuracy of every
+    solve against an FP64 direct sum; the same batch again at theta = 0.3, the angle at which
+    every solve meets rel-L2 <= 1e-4."""
     rng = np.random.default_rng(44)
     sizes = log_uniform_sizes(rng, BATCH["solves"], BATCH["n_min"], BATCH["n_max"])
     dists = ("cube", "plummer", "sphere")
@@ -167,10 +211,10 @@ def bench_batched(fmm, datasets, torch, dev, stream, flush, device, steps):
     host = np.concatenate([np.concatenate([x, q[:, None]], axis=1) for x, q in zip(xs, qs)])
     bodies = torch.tensor(host, dtype=torch.float32, device=dev)
     out = torch.empty_like(bodies)
-    kw = dict(basis="spherical", P=BATCH["P"], theta=BATCH["theta"], ncrit=BATCH["ncrit"],
-              nspawn=BATCH["nspawn"], use_rmax=1, use_ropt=BATCH["use_ropt"])
-    s = fmm.Solver(precision="f32", device=device, **kw)
-    s.set_stream(stream.cuda_stream)
+    # FP64 direct sums of 256 stride-sampled targets of every solve (the accuracy reference)
+    samples = [datasets.sample_targets(int(counts[i]), 256) for i in range(len(counts))]
+    direct = [fmm.direct(xs[i][samples[i]], xs[i], qs[i], device=device)
+              for i in range(len(counts))]
 
     def timed(fn):
         with torch.cuda.stream(stream):
@@ -182,49 +226,69 @@ def bench_batched(fmm, datasets, torch, dev, stream, flush, device, steps):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    batch = lambda: s.solve_batch_device(counts, bodies.data_ptr(), out.data_ptr())
-    for _ in range(3):
-        timed(batch)
-    ms = [timed(batch) for _ in range(max(3, steps // 2))]
-    phases = s.timings()
-    nm2l, np2p, body_pairs = s.list_counts()
-    res = out.cpu().numpy().astype(np.float64)
+    def accuracy():
+        res = out.cpu().numpy().astype(np.float64)
+        errs = [rel_err(res[offs[i]:offs[i + 1]][samples[i]], direct[i])
+                for i in range(len(counts))]
+        pot = [e[0] for e in errs]
+        acc = [e[1] for e in errs]
+        worst = int(np.argmax(np.maximum(pot, acc)))
+        return {"max_rel_l2_pot": max(pot), "max_rel_l2_acc": max(acc),
+                "median_rel_l2_acc": float(np.median(acc)),
+                "solves_over_1e-4": int(sum(max(a, b) > 1e-4 for a, b in errs)),
+                "worst_solve": {"index": worst, "n": int(counts[worst]),
+                                "dist": dists[worst % 3]},
+                "sample": "256 stride-sampled targets of every one of the %d solves, FP64 "
+                          "direct sum on the GPU" % len(counts)}
 
-    def one_by_one():
-        for i in range(len(counts)):
-            s.solve_device(int(counts[i]), bodies.data_ptr() + 16 * int(offs[i]),
-                           out.data_ptr() + 16 * int(offs[i]))
+    def run_batch(theta, one_by_one_too):
+        kw = dict(basis="spherical", P=BATCH["P"], theta=theta, ncrit=BATCH["ncrit"],
+                  nspawn=BATCH["nspawn"], use_rmax=1, use_ropt=BATCH["use_ropt"])
+        s = fmm.Solver(precision="f32", device=device, **kw)
+        s.set_stream(stream.cuda_stream)
+        batch = lambda: s.solve_batch_device(counts, bodies.data_ptr(), out.data_ptr())
+        for _ in range(3):
+            timed(batch)
+        ms = [timed(batch) for _ in range(max(3, steps // 2))]
+        r = {"theta": theta, "value": total / (float(np.median(ms)) * 1e-3),
+             "unit": "particles/s",
+             "ms_per_batch": {"p50": float(np.median(ms)), "p99": float(np.percentile(ms, 99))},
+             "phases_ms": s.timings()}
+        nm2l, np2p, body_pairs = s.list_counts()
+        r["work"] = {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs}
+        r["accuracy"] = accuracy()
+        if one_by_one_too:
+            def one_by_one():
+                for i in range(len(counts)):
+                    s.solve_device(int(counts[i]), bodies.data_ptr() + 16 * int(offs[i]),
+                                   out.data_ptr() + 16 * int(offs[i]))
+            timed(one_by_one)
+            seq_ms = [timed(one_by_one) for _ in range(2)]
+            r["one_call_per_solve"] = {"ms": float(np.median(seq_ms)),
+                                       "value": total / (float(np.median(seq_ms)) * 1e-3)}
+            r["speedup_vs_one_call_per_solve"] = float(np.median(seq_ms)) / float(np.median(ms))
+        del s
+        return r
 
-    timed(one_by_one)
-    seq_ms = [timed(one_by_one) for _ in range(2)]
-    errs = []
-    for i in range(6):  # two solves of each distribution
-        idx = datasets.sample_targets(int(counts[i]), 256)
-        d = fmm.direct(xs[i][idx], xs[i], qs[i], device=device)
-        errs.append(rel_err(res[offs[i]:offs[i + 1]][idx], d))
-    del bodies, out, s
-    return {
+    main = run_batch(BATCH["theta"], True)
+    at_bound = run_batch(BATCH_THETA_1E4, False)
+    del bodies, out
+    main.update({
         "workload": "batched: %d solves, N log-uniform [%d, %d] (seed 44), cube/plummer/sphere "
                     "by i mod 3, spherical P=%d theta=%.2f ncrit=%d use_rmax=1 use_ropt=%d, fp32 + "
                     "compensation" % (BATCH["solves"], BATCH["n_min"], BATCH["n_max"], BATCH["P"],
                                       BATCH["theta"], BATCH["ncrit"], BATCH["use_ropt"]),
-        "bodies": total, "value": total / (float(np.median(ms)) * 1e-3), "unit": "particles/s",
-        "ms_per_batch": {"p50": float(np.median(ms)), "p99": float(np.percentile(ms, 99))},
-        "one_call_per_solve": {"ms": float(np.median(seq_ms)),
-                               "value": total / (float(np.median(seq_ms)) * 1e-3)},
-        "speedup_vs_one_call_per_solve": float(np.median(seq_ms)) / float(np.median(ms)),
-        "phases_ms": phases,
-        "work": {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs},
-        "accuracy": {"max_rel_l2_pot": max(e[0] for e in errs),
-                     "max_rel_l2_acc": max(e[1] for e in errs),
-                     "sample": "256 targets of each of solves 0-5, FP64 direct sum on the GPU"},
-        "l2": "256 MB flush before each timed batch"}
+        "bodies": total, "at_theta_for_1e-4": at_bound,
+        "l2": "256 MB flush before each timed batch"})
+    return main
 
 
 def bench_serving(fmm, datasets, device):
     """Continuous batching: Poisson arrivals of solves with N log-uniform in [1e3, 1e6],
-    P uniform over {6, 8, 10}, cube or Plummer bodies (FP32 + compensation), submitted
-    through the host C ABI at three loads (fractions of the capacity measured by a burst)."""
+    P uniform over {6, 8, 10} (each order at the opening angle that holds it to rel-L2 <=
+    1e-4), cube or Plummer bodies (FP32 + compensation), submitted through the host C ABI:
+    bursts (every request at t = 0) for the capacity, then three loads (fractions of it);
+    accuracy of every request of at least 1e4 bodies against an FP64 direct sum."""
     import threading as th
     rng = np.random.default_rng(45)
     R = SERVE["requests"]
@@ -236,10 +300,12 @@ def bench_serving(fmm, datasets, device):
                              precision="f32")
         reqs.append((x, q, int(orders[i])))
     total = int(sizes.sum())
-    srv = fmm.Server(theta=SERVE["theta"], ncrit=SERVE["ncrit"], use_ropt=SERVE["use_ropt"],
+    srv = fmm.Server(theta=0.4, ncrit=SERVE["ncrit"], use_ropt=SERVE["use_ropt"],
                      workers=SERVE["workers"],
                      max_batch=SERVE["max_batch"], hbm_budget_gb=SERVE["hbm_budget_gb"],
                      device=device)
+    for P, theta in SERVE["theta"].items():
+        srv.set_theta(P, theta)
 
     def run(gaps):
         ids, t0 = [None] * R, time.perf_counter()
@@ -265,46 +331,60 @@ def bench_serving(fmm, datasets, device):
         wall = time.perf_counter() - t0
         return outs, np.array(lat), np.array(que), wall
 
+    def row(load, lam, lat, que, wall):
+        return {"load": load, "lambda_rps": lam, "p50_ms": 1e3 * float(np.median(lat)),
+                "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "queue_p50_ms": 1e3 * float(np.median(que)), "particles_per_s": total / wall}
+
     b0 = srv.stats()["batches"]
     run(np.zeros(R))  # warm-up: handles per order, pinned staging, device buffers grown
     run(np.zeros(R))  # (the batches of a pass differ from run to run; a second pass
     #                   grows the buffers that the first batches did not reach)
-    outs, lat, que, wall = run(np.zeros(R))  # burst: every request at t = 0
-    capacity = R / wall
-    sweep = [{"load": "burst", "lambda_rps": None, "p50_ms": 1e3 * float(np.median(lat)),
-              "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-              "queue_p50_ms": 1e3 * float(np.median(que)), "particles_per_s": total / wall}]
+    bursts, caps, outs = [], [], None
+    for _ in range(SERVE["passes"]):  # bursts: every request at t = 0
+        outs, lat, que, wall = run(np.zeros(R))
+        caps.append(R / wall)
+        bursts.append(row("burst", None, lat, que, wall))
+    capacity = float(np.median(caps))
+    sweep = list(bursts)
     for f in SERVE["load"]:
         lam = f * capacity
         gaps = rng.exponential(1.0 / lam, R)
         gaps[0] = 0.0
         _, lat, que, wall = run(gaps)
-        sweep.append({"load": f, "lambda_rps": lam, "p50_ms": 1e3 * float(np.median(lat)),
-                      "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                      "queue_p50_ms": 1e3 * float(np.median(que)),
-                      "particles_per_s": total / wall})
+        sweep.append(row(f, lam, lat, que, wall))
     st = srv.stats()
     prof = srv.profile()
     srv.close()
     errs = {}
     for i in range(R):
-        P = reqs[i][2]
-        if P in errs or sizes[i] < 20000:
+        if sizes[i] < SERVE["acc_min_n"]:
             continue
-        x, q = reqs[i][0], reqs[i][1]
+        x, q, P = reqs[i]
         idx = datasets.sample_targets(len(q), 256)
-        errs[P] = rel_err(outs[i][idx], fmm.direct(x[idx], x, q, device=device))
+        errs.setdefault(P, []).append(rel_err(outs[i][idx], fmm.direct(x[idx], x, q,
+                                                                        device=device)))
+    accuracy = {str(P): {"theta": SERVE["theta"][P], "requests": len(e),
+                         "max_rel_l2_pot": max(v[0] for v in e),
+                         "max_rel_l2_acc": max(v[1] for v in e)} for P, e in sorted(errs.items())}
     return {
         "workload": "serving: %d requests, N log-uniform [%d, %d] (seed 45), P in %s, "
-                    "cube/plummer, theta=%.2f ncrit=%d use_rmax=1 use_ropt=%d, fp32 + compensation; "
-                    "%d workers, max batch %d, HBM budget %.0f GB; host double buffers through "
-                    "the C ABI" % (R, SERVE["n_min"], SERVE["n_max"], list(SERVE["orders"]),
-                                   SERVE["theta"], SERVE["ncrit"], SERVE["use_ropt"],
-                                   SERVE["workers"], SERVE["max_batch"], SERVE["hbm_budget_gb"]),
-        "bodies_per_pass": total, "capacity_rps": capacity, "sweep": sweep,
+                    "cube/plummer, theta per order %s, ncrit=%d use_rmax=1 use_ropt=%d, fp32 + "
+                    "compensation; %d workers, max batch %d, HBM budget %.0f GB; host double "
+                    "buffers through the C ABI" % (
+                        R, SERVE["n_min"], SERVE["n_max"], list(SERVE["orders"]),
+                        json.dumps({str(k): v for k, v in SERVE["theta"].items()}),
+                        SERVE["ncrit"], SERVE["use_ropt"], SERVE["workers"],
+                        SERVE["max_batch"], SERVE["hbm_budget_gb"]),
+        "bodies_per_pass": total, "capacity_rps": capacity,
+        "capacity_rps_per_burst": caps,
+        "capacity_spread": (max(caps) - min(caps)) / capacity,
+        "sweep": sweep,
         "batches": st["batches"] - b0,
         "worker_seconds_all_passes": prof,
-        "accuracy": {str(P): {"rel_l2_pot": e[0], "rel_l2_acc": e[1]} for P, e in errs.items()},
+        "accuracy": accuracy,
+        "accuracy_sample": "256 stride-sampled targets of every request of >= %d bodies (last "
+                           "burst), FP64 direct sum on the GPU" % SERVE["acc_min_n"],
         "latency": "submit to result ready, host clock; Poisson gaps at load x capacity"}
 
 
@@ -319,7 +399,8 @@ def cpu_model():
 
 
 def bench_reference(args, datasets):
-    """--impl reference: the reference CPU FMM, bounded sample per step, rank 0 only."""
+    """--impl reference: the reference CPU FMM on the headline workload itself (N = 2^20,
+    same bodies, parameters and float + Kahan + MASS arithmetic), rank 0 only."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
@@ -331,28 +412,93 @@ def bench_reference(args, datasets):
         return
     threads = os.cpu_count() or 1
     n = args.ref_n
+    x, q = datasets.make(WORKLOAD["dist"], n, seed=43, precision="f32")
     for _ in range(args.warmup):
-        run_reference_sample(ref, datasets, n, threads)
-    walls = []
+        run_reference(ref, x, q, WORKLOAD, threads)
+    walls, phases = [], []
     for _ in range(args.steps):
-        w, _t = run_reference_sample(ref, datasets, n, threads)
+        w, t = run_reference(ref, x, q, WORKLOAD, threads)
         walls.append(w)
+        phases.append(t)
     total = sum(walls)
     value = n * args.steps / total
-    sample = "Plummer N=%d (same distribution and parameters, %s build, %d threads, %s)" % (
+    sample = "Plummer N=%d, the GPU arm's bodies and parameters, %s build, %d threads, %s" % (
         n, REF_CONFIG, threads, cpu_model())
     print(json.dumps({
         "metric": METRIC, "impl": "reference", "value": value, "unit": "particles/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer, q = 1/N)",
-        "config": {"workload": WORKLOAD_NAME, "sample_n_bodies": n},
+        "config": {"workload": WORKLOAD_NAME, "n_bodies": n},
         "latency_ms": {"p50": 1e3 * float(np.median(walls)),
                        "p99": 1e3 * float(np.percentile(walls, 99))},
+        "phases_ms_median": {k: 1e3 * float(np.median([t[k] for t in phases]))
+                             for k in phases[0]},
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))
+
+
+def bench_cartesian(fmm, datasets, torch, dev, stream, flush, device, steps, clk_mhz,
+                    cpu_baseline):
+    """Cartesian P = 5, theta = 0.5, ncrit = 32, N = 4,194,304 bodies on
+    the unit sphere surface (charges uniform in [0, 1]), FP32 expansions: device time and
+    phases, work and roofline of M2L and P2P, accuracy against an FP64 direct sum on 1024
+    targets, and the reference CPU build (cart_p5_f32) on the same bodies."""
+    n = CART["n"]
+    x, q = datasets.make(CART["dist"], n, seed=46, precision="f32")
+    kw = {k: CART[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax", "use_ropt")}
+    s = fmm.Solver(precision="f32", device=device, **kw)
+    s.set_stream(stream.cuda_stream)
+    bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1), dtype=torch.float32, device=dev)
+    out = torch.empty_like(bodies)
+    ms, phase_sum = [], None
+    for it in range(3 + max(3, steps // 2)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.solve_device(n, bodies.data_ptr(), out.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= 3:
+            ms.append(e0.elapsed_time(e1))
+            t = s.timings()
+            phase_sum = t if phase_sum is None else {k: phase_sum[k] + t[k] for k in t}
+    phases = {k: v / len(ms) for k, v in phase_sum.items()}
+    nm2l, np2p, body_pairs = s.list_counts()
+    idx = datasets.sample_targets(n, 1024)
+    trg = out.cpu().numpy().astype(np.float64)
+    err = rel_err(trg[idx], fmm.direct(x[idx], x, q, device=device))
+    del s, bodies, out
+    peak = nominal_fp32_tflops(clk_mhz)
+    m2l_tf = nm2l * m2l_flops_per_pair(CART["P"], "cartesian") / (phases["m2l"] * 1e-3) / 1e12
+    p2p_tf = 20.0 * body_pairs / (phases["p2p"] * 1e-3) / 1e12
+    res = {"workload": CART_NAME, "n_bodies": n, "steps": len(ms), "warmup": 3,
+           "value": n / (float(np.median(ms)) * 1e-3), "unit": "particles/s",
+           "ms_per_step": float(np.median(ms)), "phases_ms": phases,
+           "work": {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs},
+           "roofline": {"m2l_tflops": m2l_tf, "m2l_frac": m2l_tf / peak,
+                        "m2l_flops_per_pair": m2l_flops_per_pair(CART["P"], "cartesian"),
+                        "p2p_tflops": p2p_tf, "p2p_frac": p2p_tf / peak, "peak": peak,
+                        "peak_source": "nominal FP32 at the sampled SM clock"},
+           "accuracy": {"rel_l2_pot": err[0], "rel_l2_acc": err[1], "targets": 1024,
+                        "reference": "FP64 direct sum on the GPU"},
+           "l2": "256 MB flush before each timed solve"}
+    if cpu_baseline:
+        oracle, _ = reference_lib()
+        if oracle.have_reference(CART_REF_CONFIG, "perf"):
+            ref = oracle.Reference(CART_REF_CONFIG, "perf")
+            threads = os.cpu_count() or 1
+            wall, ph = reference_median(ref, x, q, CART, threads)
+            res["reference_cpu"] = {
+                "value": n / wall, "unit": "particles/s", "cores": threads,
+                "wall_s_median_of_3": wall, "phases_s_median": ph,
+                "kind": "reference", "build": CART_REF_CONFIG + " (float, OpenMP, -O3)",
+                "cpu": cpu_model()}
+            res["speedup_vs_reference_cpu"] = res["value"] / res["reference_cpu"]["value"]
+    return res
 
 
 def main():
@@ -362,11 +508,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
-    ap.add_argument("--ref-n", type=int, default=REF_SAMPLE_N)
+    ap.add_argument("--ref-n", type=int, default=REF_N)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop line")
+    ap.add_argument("--no-cart", action="store_true",
+                    help="skip the Cartesian P = 5, N = 4,194,304 line")
     ap.add_argument("--profile", action="store_true",
                     help="warm-ups, then one solve between cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off), then exit")
@@ -499,7 +647,7 @@ def main():
             ms64.append(e0.elapsed_time(e1))
         t64 = o64.cpu().numpy()
         fp64 = {"value": n / (float(np.mean(ms64)) * 1e-3), "unit": "particles/s",
-                "ms_per_step": float(np.mean(ms64)),
+                "ms_per_step": float(np.mean(ms64)), "phases_ms": s64.timings(),
                 "err_pot": float(np.sqrt(((t64[idx, 0] - dref[:, 0]) ** 2).sum() / (dref[:, 0] ** 2).sum())),
                 "err_acc": float(np.sqrt(((t64[idx, 1:] - dref[:, 1:]) ** 2).sum() / (dref[:, 1:] ** 2).sum())),
                 "fp32_speedup": (n / (total_ms / args.steps * 1e-3)) / (n / (float(np.mean(ms64)) * 1e-3))}
@@ -520,10 +668,17 @@ def main():
     batched = None if args.no_batch else bench_batched(fmm, datasets, torch, dev, stream, flush,
                                                        local, args.steps)
     serving = None if args.no_serve else bench_serving(fmm, datasets, local)
+    clk_mhz = clk["sm_mhz"] or 1965.0
+    cart = None if args.no_cart else bench_cartesian(fmm, datasets, torch, dev, stream, flush,
+                                                     local, args.steps, clk_mhz,
+                                                     not args.no_cpu_baseline)
 
-    peak = fmm.fp32_peak_tflops(local)
-    m2l_flops = nm2l * m2l_flops_per_pair(WORKLOAD["P"])
-    m2l_tflops = m2l_flops / (phases["m2l"] * 1e-3) / 1e12
+    # roofline of M2L (the largest phase): algorithmic flops per pair of the reference's loop
+    # over the phase's event time, against the nominal FP32 rate at the sampled SM clock
+    probe = fmm.fp32_peak_tflops(local)
+    peak = nominal_fp32_tflops(clk_mhz)
+    m2l_tflops = nm2l * m2l_flops_per_pair(WORKLOAD["P"]) / (phases["m2l"] * 1e-3) / 1e12
+    m2l_exec = nm2l * m2l_executed_flops_per_pair(WORKLOAD["P"]) / (phases["m2l"] * 1e-3) / 1e12
     p2p_tflops = 20.0 * body_pairs / (phases["p2p"] * 1e-3) / 1e12
     traffic = None
     prof = os.path.join(ROOT, "profiles", "m2l_traffic.json")
@@ -538,11 +693,15 @@ def main():
         oracle, ref = reference_lib()
         threads = os.cpu_count() or 1
         if ref is not None:
-            walls = [run_reference_sample(ref, datasets, args.ref_n, threads)[0] for _ in range(2)]
-            cpu = {"value": args.ref_n / min(walls), "unit": "particles/s", "cores": threads,
+            xr, qr = (x, q) if args.ref_n == n else datasets.make(
+                WORKLOAD["dist"], args.ref_n, seed=43, precision="f32")
+            wall, ph = reference_median(ref, xr, qr, WORKLOAD, threads)
+            cpu = {"value": args.ref_n / wall, "unit": "particles/s", "cores": threads,
                    "kind": "reference",
-                   "sample": "Plummer N=%d, same parameters, reference %s build, best of 2, %s" % (
-                       args.ref_n, REF_CONFIG, cpu_model())}
+                   "sample": "the headline workload itself (Plummer N=%d, same bodies and "
+                             "parameters), reference %s build, median of 3, %s" % (
+                                 args.ref_n, REF_CONFIG, cpu_model()),
+                   "phases_s_median": ph}
 
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
@@ -558,18 +717,28 @@ def main():
                      "reference": "FP64 direct sum on the GPU"},
         "phases_ms": phases,
         "work": {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs,
-                 "p2p_tflops": p2p_tflops, "p2p_frac_of_fp32_peak": p2p_tflops / peak},
+                 "p2p_tflops": p2p_tflops, "p2p_frac_of_fp32_peak": p2p_tflops / peak,
+                 "p2p_flops_per_pair": 20,
+                 "m2l_flops_per_pair": m2l_flops_per_pair(WORKLOAD["P"]),
+                 "m2l_executed_flops_per_pair": m2l_executed_flops_per_pair(WORKLOAD["P"])},
         "fp64_gpu": fp64,
         "e2e": {"value": e2e_value, "unit": "particles/s", "h2d_bytes_per_step": 32 * n,
                 "d2h_bytes_per_step": 32 * n, "ms_per_step": e2e_total / len(e2e_ms)},
         "roofline": {"kernel": "M2L (k_m2l_reg<float,10>)", "bound": "fp32",
                      "achieved": m2l_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": m2l_tflops / peak, "traffic": traffic,
-                     "peak_source": "fmm_b200_fp32_peak: FMA probe measured on this GPU in this run"},
+                     "flops_per_pair": m2l_flops_per_pair(WORKLOAD["P"]),
+                     "executed_tflops": m2l_exec, "probe_tflops": probe,
+                     "frac_of_probe": m2l_tflops / probe,
+                     "peak_source": "nominal FP32: 148 SMs x 128 lanes x 2 flops x %.0f MHz "
+                                    "(SM clock sampled during the timed solves); "
+                                    "MEASURED_PEAKS.json has no FP32 figure; probe_tflops = "
+                                    "FMA throughput measured on this GPU in this run" % clk_mhz},
         "cpu_baseline": cpu,
         "autotune_ncrit": autotune,
         "batched": batched,
         "serving": serving,
+        "cartesian": cart,
         "clocks": clk,
         "gpu_launches": int(launches),
     }

@@ -83,6 +83,7 @@ SIGNATURES = {
     "fmm_b200_get_timings": (_i, [_vp, _vp]),
     "fmm_b200_server_create": (_i, [_vp, _d, _i, _i, _vp]),
     "fmm_b200_server_submit": (_i, [_vp, _i, _vp, _vp, _i, _vp]),
+    "fmm_b200_server_set_theta": (_i, [_vp, _i, _d]),
     "fmm_b200_server_poll": (_i, [_vp, _ll, _vp]),
     "fmm_b200_server_wait": (_i, [_vp, _ll, _vp, _vp, _vp, _vp]),
     "fmm_b200_server_stats": (_i, [_vp, _vp, _vp, _vp, _vp]),
@@ -135,12 +136,22 @@ def direct(xt, xs, qs, eps2=0.0, device=0):
     out = np.zeros((len(xt), 4))
     rc = lib.fmm_b200_direct(device, len(xt), _p(xt), len(xs), _p(xs), _p(qs), eps2, _p(out))
     if rc != FMM_OK:
-        raise FmmError(rc, "direct sum failed")
+        raise FmmError(rc, "direct sum failed: " + lib.fmm_b200_last_error(None).decode())
     return out
 
 
-DIRECT_NOALLOC_MAX_TARGETS = 32768
-DIRECT_NOALLOC_MAX_SOURCES = 65536
+def _header_define(name, header=os.path.join(HERE, "..", "include", "exafmm_b200.h")):
+    """Integer value of a #define in the C header (the one place the C limits are set)."""
+    with open(header) as fh:
+        for line in fh:
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "#define" and parts[1] == name:
+                return int(parts[2])
+    raise FmmError(FMM_ERR_INVALID, "%s is not defined in %s" % (name, header))
+
+
+DIRECT_NOALLOC_MAX_TARGETS = _header_define("FMM_DIRECT_NOALLOC_MAX_TARGETS")
+DIRECT_NOALLOC_MAX_SOURCES = _header_define("FMM_DIRECT_NOALLOC_MAX_SOURCES")
 
 
 def direct_noalloc(xt, xs, qs, eps2=0.0, device=0):
@@ -422,6 +433,12 @@ class Server:
         if rc != FMM_OK:
             raise FmmError(rc, self.lib.fmm_b200_last_error(None).decode())
         self._n = {}
+
+    def set_theta(self, P, theta):
+        """Opening angle of the requests of order P submitted from now on."""
+        rc = self.lib.fmm_b200_server_set_theta(self.h, P, theta)
+        if rc != FMM_OK:
+            raise FmmError(rc, "set_theta(%r, %r) rejected" % (P, theta))
 
     def submit(self, x, q, P):
         x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)

@@ -1,8 +1,10 @@
 // Serving loop over the batched solver: continuous batching of independent FMM solves.
 //
-// Requests (bodies + expansion order) are copied in at submit and queued.  A scheduler
-// thread forms batches from whatever is pending whenever a worker is free: the oldest
-// request decides the order P, later requests of the same P join in arrival order while the
+// Requests (bodies + expansion order) are copied in at submit and queued; each takes the
+// opening angle set for its order (fmm_b200_server_set_theta; else the configuration's), so
+// that every order can be held to the same accuracy.  A scheduler thread forms batches from
+// whatever is pending whenever a worker is free: the oldest request decides the order P (and
+// angle), later requests of the same P and angle join in arrival order while the
 // batch fits the free part of the device-memory budget and the batch-size limit.  Each
 // worker owns a CUDA stream and one solver handle per order, so batches on different
 // workers overlap on the GPU; requests that arrive while batches run are admitted into the
@@ -33,6 +35,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   long long id = 0;
   int n = 0, P = 0;
+  double theta = 0;  // opening angle of the request's order when it was submitted
   std::vector<double> x, q, p, f;
   size_t bytes = 0;
   int status = FMM_OK;
@@ -43,7 +46,7 @@ struct Request {
 struct Worker {
   int index = 0;
   cudaStream_t stream = nullptr;
-  std::map<int, fmm_b200_solver*> handles;  // per expansion order
+  std::map<std::pair<int, double>, fmm_b200_solver*> handles;  // per (order, theta)
   std::vector<std::shared_ptr<Request>> batch;
   bool busy = false;
   std::thread thread;
@@ -71,6 +74,7 @@ struct fmm_b200_server {
   // worker seconds spent staging inputs, in the batched solve, and copying results out
   double t_stage = 0, t_solve = 0, t_unstage = 0;
   std::string err;
+  std::map<int, double> theta_of;  // per-order opening angle (fmm_b200_server_set_theta)
 };
 
 namespace {
@@ -131,11 +135,13 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
       batch.swap(W->batch);
     }
     const int P = batch.front()->P;
+    const double theta = batch.front()->theta;
     int rc = FMM_OK;
-    fmm_b200_solver*& h = W->handles[P];
+    fmm_b200_solver*& h = W->handles[{P, theta}];
     if (!h) {
       fmm_b200_config c = S->cfg;
       c.P = P;
+      c.theta = theta;
       rc = fmm_b200_create(&c, &h);
       if (rc == FMM_OK) rc = fmm_b200_set_stream(h, W->stream);
       if (rc != FMM_OK) h = nullptr;
@@ -229,11 +235,13 @@ void scheduler_loop(fmm_b200_server* S) {
       return free_w && S->in_flight + S->pending.front()->bytes <= S->budget;
     });
     if (S->stop) break;
-    // batch: the oldest request's order, later ones of the same order in arrival order
+    // batch: the oldest request's order (and opening angle), later ones of the same order
+    // and angle in arrival order
     const int P = S->pending.front()->P;
+    const double theta = S->pending.front()->theta;
     std::vector<std::shared_ptr<Request>> batch;
     for (auto it = S->pending.begin(); it != S->pending.end() && (int)batch.size() < S->max_batch;) {
-      if ((*it)->P == P && S->in_flight + (*it)->bytes <= S->budget) {
+      if ((*it)->P == P && (*it)->theta == theta && S->in_flight + (*it)->bytes <= S->budget) {
         S->in_flight += (*it)->bytes;
         batch.push_back(*it);
         it = S->pending.erase(it);
@@ -285,6 +293,11 @@ int fmm_b200_server_submit(fmm_b200_server* S, int n, const double* x, const dou
   int buf[64];
   const int nord = fmm_b200_supported_orders(S->cfg.basis, buf, 64);
   if (std::find(buf, buf + std::min(nord, 64), P) == buf + std::min(nord, 64)) return FMM_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto th = S->theta_of.find(P);
+    r->theta = th == S->theta_of.end() ? S->cfg.theta : th->second;
+  }
   r->x.resize(3 * (size_t)n);
   r->q.resize(n);
   copy_jobs({{r->x.data(), x, sizeof(double) * 3 * n}, {r->q.data(), q, sizeof(double) * n}});
@@ -298,6 +311,16 @@ int fmm_b200_server_submit(fmm_b200_server* S, int n, const double* x, const dou
     *id = r->id;
   }
   S->cv.notify_all();
+  return FMM_OK;
+}
+
+int fmm_b200_server_set_theta(fmm_b200_server* S, int P, double theta) {
+  if (!S || !(theta > 0) || !(theta < 1)) return FMM_ERR_INVALID;
+  int buf[64];
+  const int nord = std::min(fmm_b200_supported_orders(S->cfg.basis, buf, 64), 64);
+  if (std::find(buf, buf + nord, P) == buf + nord) return FMM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->theta_of[P] = theta;
   return FMM_OK;
 }
 

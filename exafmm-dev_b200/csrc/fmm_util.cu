@@ -97,17 +97,25 @@ static __device__ __align__(256) double g_direct_scratch[kNoAllocDoubles];
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_base[kNoAllocMaxDevices] = {};
+cudaStream_t g_noalloc_stream[kNoAllocMaxDevices] = {};
 
-// device address of the array on `device` (which must be current), looked up once per
-// device: host code only sees a host-side stand-in under the array's name
-double* noalloc_scratch(int device) {
+// Set-up of one device (which must be current), done once: the device address of the array
+// (host code only sees a host-side stand-in under the array's name) and the call's own
+// non-blocking stream (creating a stream allocates no device memory), so that the call
+// neither waits for nor holds up the caller's other streams, the legacy default stream's
+// implicit synchronisation included.
+void noalloc_setup(int device, double** base, cudaStream_t* stream) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (!g_noalloc_base[device]) {
     void* p = nullptr;
     FMM_CUDA(cudaGetSymbolAddress(&p, g_direct_scratch));
+    cudaStream_t st = nullptr;
+    FMM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    g_noalloc_stream[device] = st;
     g_noalloc_base[device] = static_cast<double*>(p);
   }
-  return g_noalloc_base[device];
+  *base = g_noalloc_base[device];
+  *stream = g_noalloc_stream[device];
 }
 
 }  // namespace
@@ -118,6 +126,7 @@ long long fmm_b200_kernel_launches(void) { return g_launches.load(); }
 
 int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const double* xs,
                             const double* qs, double eps2, double* out) {
+  fmmb200::set_call_error("");
   if (nt < 0 || ns < 0 || (nt > 0 && (!xt || !out)) || (ns > 0 && (!xs || !qs)) ||
       device < 0 || device >= kNoAllocMaxDevices) {
     fmmb200::set_call_error("fmm_b200_direct_noalloc: invalid argument");
@@ -135,17 +144,20 @@ int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const 
   if (nt == 0) return FMM_OK;
   try {
     FMM_CUDA(cudaSetDevice(device));
-    double* base = noalloc_scratch(device);
+    double* base = nullptr;
+    cudaStream_t st = nullptr;
+    noalloc_setup(device, &base, &st);
     double *dxt = base, *dxs = base + 3 * (size_t)nt, *dqs = dxs + 3 * (size_t)ns,
            *dout = dqs + ns;
-    FMM_CUDA(cudaMemcpy(dxt, xt, 24 * (size_t)nt, cudaMemcpyHostToDevice));
+    FMM_CUDA(cudaMemcpyAsync(dxt, xt, 24 * (size_t)nt, cudaMemcpyHostToDevice, st));
     if (ns) {
-      FMM_CUDA(cudaMemcpy(dxs, xs, 24 * (size_t)ns, cudaMemcpyHostToDevice));
-      FMM_CUDA(cudaMemcpy(dqs, qs, 8 * (size_t)ns, cudaMemcpyHostToDevice));
+      FMM_CUDA(cudaMemcpyAsync(dxs, xs, 24 * (size_t)ns, cudaMemcpyHostToDevice, st));
+      FMM_CUDA(cudaMemcpyAsync(dqs, qs, 8 * (size_t)ns, cudaMemcpyHostToDevice, st));
     }
-    k_direct<<<ceil_div(nt, kDirTile), kDirTile>>>(nt, dxt, ns, dxs, dqs, eps2, dout);
+    k_direct<<<ceil_div(nt, kDirTile), kDirTile, 0, st>>>(nt, dxt, ns, dxs, dqs, eps2, dout);
     FMM_LAUNCH_CHECK();
-    FMM_CUDA(cudaMemcpy(out, dout, 32 * (size_t)nt, cudaMemcpyDeviceToHost));
+    FMM_CUDA(cudaMemcpyAsync(out, dout, 32 * (size_t)nt, cudaMemcpyDeviceToHost, st));
+    FMM_CUDA(cudaStreamSynchronize(st));
   } catch (const FmmError& e) {
     fmmb200::set_call_error(e.what());
     return e.code;
@@ -155,8 +167,11 @@ int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const 
 
 int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
                     const double* qs, double eps2, double* out) {
-  if (nt < 0 || ns < 0 || (nt > 0 && (!xt || !out)) || (ns > 0 && (!xs || !qs)))
+  fmmb200::set_call_error("");
+  if (nt < 0 || ns < 0 || (nt > 0 && (!xt || !out)) || (ns > 0 && (!xs || !qs))) {
+    fmmb200::set_call_error("fmm_b200_direct: invalid argument");
     return FMM_ERR_INVALID;
+  }
   if (nt == 0) return FMM_OK;
   try {
     FMM_CUDA(cudaSetDevice(device));
@@ -174,6 +189,7 @@ int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* 
     FMM_CUDA(cudaMemcpy(out, dout, 32 * (size_t)nt, cudaMemcpyDeviceToHost));
     b.release();
   } catch (const FmmError& e) {
+    fmmb200::set_call_error(e.what());
     return e.code;
   }
   return FMM_OK;

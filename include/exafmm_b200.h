@@ -203,6 +203,12 @@ int fmm_b200_server_create(const fmm_b200_config* cfg, double hbm_budget_bytes, 
                            int max_batch, fmm_b200_server** out);
 int fmm_b200_server_submit(fmm_b200_server* srv, int n, const double* x, const double* q,
                            int P, long long* request_id);
+/* Opening angle for the requests of order P submitted from now on (0 < theta < 1; else the
+ * configuration's theta): a lower order needs a smaller angle for the same accuracy, e.g.
+ * rel-L2 <= 1e-4 of potential and gradient on zero-net-charge cubes of 1e3..1e6 bodies
+ * needs theta <= 0.22 at P = 6, 0.30 at P = 8, 0.35 at P = 10 with a margin of two.  Only
+ * requests of equal order and angle share a batch. */
+int fmm_b200_server_set_theta(fmm_b200_server* srv, int P, double theta);
 int fmm_b200_server_poll(fmm_b200_server* srv, long long request_id, int* done);
 int fmm_b200_server_wait(fmm_b200_server* srv, long long request_id, double* p, double* f,
                          double* latency_s, double* queue_s);
@@ -218,7 +224,7 @@ int fmm_b200_server_destroy(fmm_b200_server* srv);
 /* FP64 direct sum on the GPU: Traversal::direct + normalize (include/traversal.h:304-337)
  * with double accumulation.  Targets xt (3 nt), sources xs (3 ns) with charges qs; out
  * receives 4 nt values (phi, grad phi) per unit target charge; pairs with r^2 + eps2 == 0
- * are skipped.  Synchronous. */
+ * are skipped.  Synchronous; a failure's message is in fmm_b200_last_error(NULL). */
 int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* xs,
                     const double* qs, double eps2, double* out);
 /* fmm_b200_direct without any device allocation: same arguments, kernel and (bitwise)
@@ -230,7 +236,8 @@ int fmm_b200_direct(int device, int nt, const double* xt, int ns, const double* 
  * other streams of theirs are busy.  No counterpart in the reference.
  * Limits: nt <= FMM_DIRECT_NOALLOC_MAX_TARGETS and ns <= FMM_DIRECT_NOALLOC_MAX_SOURCES;
  * larger sizes return FMM_ERR_INVALID, with the limits in fmm_b200_last_error(NULL), before
- * the device is touched.  The first call on each device does the set-up: it looks up the
+ * the device is touched.  Every call clears that message first, so it describes this call's
+ * failure or is empty after a success.  The first call on each device does the set-up: it looks up the
  * array's address (cudaGetSymbolAddress, with that device current), which may load the
  * library's device code; make that first call before any stream capture begins on the
  * device.  Nothing in the array has to start at zero: a call copies in every input it reads

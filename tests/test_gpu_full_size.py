@@ -63,8 +63,10 @@ def test_plain_fmm_cube_16k_fp64(datasets):
 
 def test_batched_256_solves(datasets):
     """256 solves, N log-uniform in [1e3, 2e5], cube / Plummer / sphere by i mod 3,
-    spherical P = 8, theta = 0.4: every solve of the batch bitwise as alone (checked on a
-    sample of them) and within the method's error of FP64 direct."""
+    spherical P = 8: every solve of the batch bitwise as alone (checked on a sample of them)
+    and every solve within the method's error of FP64 direct.  At the configuration's
+    theta = 0.4 the zero-net-charge cubes reach ~2.3e-4 (the reference's FP64 build measures
+    the same on them), so the bound there is 5e-4; at theta = 0.3 every solve meets 1e-4."""
     rng = np.random.default_rng(44)
     sizes = np.rint(np.exp(rng.uniform(np.log(1e3), np.log(2e5), 256))).astype(int)
     dists = ("cube", "plummer", "sphere")
@@ -73,10 +75,38 @@ def test_batched_256_solves(datasets):
         x, q = datasets.make(dists[i % 3], int(n), seed=1000 + i, precision="f32")
         xs.append(x)
         qs.append(q)
-    kw = dict(P=8, theta=0.4, ncrit=64, use_ropt=0)
-    batch = fmm.Solver(**kw).solve_batch(xs, qs)
-    alone = fmm.Solver(**kw)
-    for i in (0, 1, 2, 100, 255):
-        assert np.array_equal(batch[i], alone.solve(xs[i], qs[i])), i
-        pot, acc = direct_error(datasets, xs[i], qs[i], batch[i], 128)
-        assert pot < 1e-3 and acc < 1e-2, (i, pot, acc)
+    idx = [datasets.sample_targets(len(q), 128) for q in qs]
+    ref = [fmm.direct(x[k], x, q) for x, q, k in zip(xs, qs, idx)]
+    for theta, bound in ((0.4, 5e-4), (0.3, 1e-4)):
+        kw = dict(P=8, theta=theta, ncrit=64, use_ropt=0)
+        batch = fmm.Solver(**kw).solve_batch(xs, qs)
+        if theta == 0.4:
+            alone = fmm.Solver(**kw)
+            for i in (0, 1, 2, 100, 255):
+                assert np.array_equal(batch[i], alone.solve(xs[i], qs[i])), i
+        for i in range(len(xs)):
+            pot, acc = rel_l2(batch[i][idx[i]], ref[i])
+            assert pot < bound and acc < bound, (theta, i, dists[i % 3], len(qs[i]), pot, acc)
+
+
+def test_serving_mixed_orders_meet_1e4(datasets):
+    """Serving: requests of 2e4, 2e5 and 1e6 bodies at P = 6, 8 and 10,
+    cube and Plummer, through the continuous-batching server with the opening angle per
+    order (P = 6: 0.22, P = 8: 0.30, P = 10: 0.35): every request within rel-L2 1e-4 of
+    potential and gradient against FP64 direct."""
+    thetas = {6: 0.22, 8: 0.30, 10: 0.35}
+    srv = fmm.Server(theta=0.4, ncrit=64, use_ropt=0, hbm_budget_gb=40.0, workers=2,
+                     max_batch=8)
+    for P, t in thetas.items():
+        srv.set_theta(P, t)
+    reqs, k = [], 0
+    for n in (20000, 200000, 1000000):
+        for P in (6, 8, 10):
+            x, q = datasets.make(("cube", "plummer")[k % 2], n, seed=300 + k, precision="f32")
+            reqs.append((x, q, P, srv.submit(x, q, P)))
+            k += 1
+    for x, q, P, rid in reqs:
+        out, _, _ = srv.wait(rid)
+        pot, acc = direct_error(datasets, x, q, out, 256)
+        assert pot < 1e-4 and acc < 1e-4, (P, len(q), pot, acc)
+    srv.close()

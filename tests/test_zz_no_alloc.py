@@ -12,6 +12,8 @@ import importlib
 import numpy as np
 import pytest
 
+from oracle import Oracle, rel_l2
+
 fmm = importlib.import_module("exafmm-dev_b200")
 
 
@@ -53,3 +55,36 @@ def test_sizes_beyond_the_limits_are_rejected():
             fmm.direct_noalloc(np.zeros((mt, 3)), np.zeros((ms, 3)), np.ones(ms))
         assert e.value.code == fmm.FMM_ERR_INVALID
         assert "limits of %d targets / %d sources" % (nt, ns) in str(e.value)
+
+
+@pytest.mark.gpu
+def test_matches_the_oracle_direct_sum(datasets):
+    """Both GPU direct sums against the oracle's FP64 sum: softened, unsoftened, and targets
+    that coincide with sources (skipped pairs); rounding differences only (FMA contraction)."""
+    xs, qs = datasets.make("plummer", 20000, seed=9, precision="f64")
+    rng = np.random.default_rng(10)
+    xt = np.concatenate([xs[:1000], rng.uniform(-1, 1, (1000, 3))])
+    o64 = Oracle("f64")
+    for eps2 in (0.0, 1e-3):
+        want = o64.direct(xt, xs, qs, eps2=eps2)
+        for got in (fmm.direct_noalloc(xt, xs, qs, eps2=eps2), fmm.direct(xt, xs, qs, eps2=eps2)):
+            pot, acc = rel_l2(got, want)
+            assert pot < 1e-13 and acc < 1e-13, (eps2, pot, acc)
+
+
+@pytest.mark.gpu
+def test_a_success_clears_the_last_error(datasets):
+    lib = fmm.load_library()
+    nt = fmm.DIRECT_NOALLOC_MAX_TARGETS
+    with pytest.raises(fmm.FmmError):
+        fmm.direct_noalloc(np.zeros((nt + 1, 3)), np.zeros((4, 3)), np.ones(4))
+    assert b"limits" in lib.fmm_b200_last_error(None)
+    xs, qs = datasets.make("cube", 100, seed=4, precision="f64")
+    fmm.direct_noalloc(xs[:10], xs, qs)
+    assert lib.fmm_b200_last_error(None) == b""
+
+
+def test_limits_come_from_the_header():
+    hdr = open(__file__.replace("tests/test_zz_no_alloc.py", "include/exafmm_b200.h")).read()
+    assert "#define FMM_DIRECT_NOALLOC_MAX_TARGETS %d" % fmm.DIRECT_NOALLOC_MAX_TARGETS in hdr
+    assert "#define FMM_DIRECT_NOALLOC_MAX_SOURCES %d" % fmm.DIRECT_NOALLOC_MAX_SOURCES in hdr

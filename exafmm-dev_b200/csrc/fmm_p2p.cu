@@ -5,15 +5,16 @@
 // small leaf still keeps the warp busy: each group holds one target body and its G lanes
 // take every G-th source; a leaf of 33..64 bodies gives each lane two targets that share
 // every staged source.  Sources stream through shared memory 32 bodies at a time (one
-// coalesced 16-byte load per lane); in FP32 a chunk of 32 runs on across source leaves, and
-// the staged sources are taken two at a time with the packed two-wide instructions of
-// sm_100 (half the issue slots of the scalar pair arithmetic).  The inner loop is FMA + one
-// rsqrt per pair (no r^2 == 0 test away from the target leaf itself), and each chunk's (FP64:
-// each source leaf's) plain partial sum is folded into a compensated (TwoSum) accumulator,
-// so the accumulation error does not grow with the length of the list.  Pairs with r^2 == 0 are skipped, as the reference does (:149); the
-// result is per unit target charge (the reference multiplies by q_i in P2P and divides
-// again in L2P / normalize).
+// coalesced load per lane), a chunk of 32 running on across source leaves; in FP32 the
+// staged sources are taken two at a time with the packed two-wide instructions of sm_100
+// (half the issue slots of the scalar pair arithmetic).  The inner loop is FMA + one rsqrt
+// per pair (no r^2 == 0 test away from the target leaf itself).  FP32 folds each chunk's
+// plain partial sum into a compensated (TwoSum) accumulator, so the accumulation error does
+// not grow with the length of the list; FP64 sums plainly.  Pairs with r^2 == 0 are
+// skipped, as the reference does (:149); the result is per unit target charge (the
+// reference multiplies by q_i in P2P and divides again in L2P / normalize).
 #include <algorithm>
+#include <type_traits>
 
 #include "fmm_solver.cuh"
 
@@ -96,175 +97,67 @@ __device__ __forceinline__ void row_pairs(const float4* row, int sub, int G, int
   }
 }
 
-// all bodies of one source leaf (first body j0, nj bodies) on the lane's TPL targets, its
-// sums started from zero; sources are staged through the warp's shared row 32 at a time
-template <typename T, int TPL, bool EXACT, bool SHIFT = false>
-__device__ __forceinline__ void source_leaf(int lane, int wl, vec4<T> (*sh)[32], int sub, int G,
-                                            int j0, int nj, const vec4<T>* __restrict__ bodies,
-                                            T eps2, const vec4<T>* xi, T* pot, T* ax, T* ay,
-                                            T* az, T px = 0, T py = 0, T pz = 0) {
+// FP64 rows: one source per entry (x, y, z, q); the pairs of a staged row (cnt sources) on
+// the lane's TPL targets, added to the plain sums
+template <int TPL, bool EXACT, bool SHIFT>
+__device__ __forceinline__ void row_pairs(const vec4<double>* row, int sub, int G, int cnt,
+                                          const vec4<double>* xi, double eps2, double px,
+                                          double py, double pz, double* sp, double* sx,
+                                          double* sy, double* sz) {
+#pragma unroll (4 / TPL)
+  for (int k = sub; k < cnt; k += G) {
+    const vec4<double> sj = row[k];
 #pragma unroll
-  for (int u = 0; u < TPL; u++) pot[u] = ax[u] = ay[u] = az[u] = 0;
-  for (int jb = 0; jb < nj; jb += 32) {
-    const int cnt = min(32, nj - jb);
-    __syncwarp();
-    if (lane < cnt) sh[wl][lane] = bodies[j0 + jb + lane];
-    __syncwarp();
-#pragma unroll 4
-    for (int k = sub; k < cnt; k += G) {
-      const vec4<T> sj = sh[wl][k];
-#pragma unroll
-      for (int u = 0; u < TPL; u++)
-        p2p_accum<T, EXACT, SHIFT>(sj, xi[u], eps2, pot[u], ax[u], ay[u], az[u], px, py, pz);
-    }
+    for (int u = 0; u < TPL; u++)
+      p2p_accum<double, EXACT, SHIFT>(sj, xi[u], eps2, sp[u], sx[u], sy[u], sz[u], px, py, pz);
   }
 }
 
-// TPL targets per lane (1 or 2): a lane holds targets ti and ti + 32 / G and reuses every
-// staged source for both.
+// Target leaf, either precision: the bodies of its source leaves, taken in list order, are
+// staged 32 at a time whatever the leaves' sizes (a chunk runs on into the next source leaf,
+// and ends early only where the periodic image changes or after 32 source leaves), so that
+// the rows are full and the per-chunk work (staging, the finite test, the compensated fold)
+// is shared by all of its source leaves.  The source leaves' descriptors (first body,
+// count, image) are read 32 at a time, one per lane; a lane finds the leaf of its chunk
+// position by a scan of the counts and a binary search over the lanes.  A chunk that holds
+// bodies of the target leaf itself is summed in the exact form; any other chunk in the fast
+// form, and again in the exact form (from the same row) if a sum is not finite, so the
+// results are those of the exact form throughout.  FP32 takes the staged sources two at a
+// time with the packed f32x2 instructions; FP64 one at a time.
 template <typename T, bool COMP, int TPL>
-__device__ __forceinline__ void p2p_leaf(int lane, int wl, vec4<T> (*sh)[32], int b0, int nb,
-                                         int base, int G, int s0, int s1,
-                                         const unsigned long long* __restrict__ pairs,
-                                         const int* __restrict__ ibody,
-                                         const int* __restrict__ nbody,
-                                         const vec4<T>* __restrict__ bodies, T eps2, T cycle,
-                                         vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+__device__ __forceinline__ void p2p_leaf_chunked(int lane, void* rowmem, int b0, int nb,
+                                                 int base, int G, int s0, int s1,
+                                                 const unsigned long long* __restrict__ pairs,
+                                                 const int* __restrict__ ibody,
+                                                 const int* __restrict__ nbody,
+                                                 const vec4<T>* __restrict__ bodies, T eps2,
+                                                 T cycle, vec4<T>* __restrict__ trg_s,
+                                                 vec4<T>* __restrict__ trg_e) {
+  constexpr bool F32 = sizeof(T) == 4;
+  // per-lane pair sums: float2 (two halves of the packed form) or T
+  using Acc = typename std::conditional<F32, float2, T>::type;
+  const unsigned full = 0xffffffffu;
   const int tpp = 32 / G;
   const int sub = lane % G;
   int ti[TPL];
   bool act[TPL];
   vec4<T> xi[TPL];
+  float2 nx[TPL], ny[TPL], nz[TPL];  // FP32: negated target coordinates in both halves
   Comp<T> acc[TPL][4];
 #pragma unroll
   for (int u = 0; u < TPL; u++) {
     ti[u] = base + u * tpp + lane / G;
     act[u] = ti[u] < nb;
     xi[u] = act[u] ? bodies[b0 + ti[u]] : make_v4<T>(0, 0, 0, 0);
+    if constexpr (F32) {
+      nx[u] = make_float2(-xi[u].x, -xi[u].x);
+      ny[u] = make_float2(-xi[u].y, -xi[u].y);
+      nz[u] = make_float2(-xi[u].z, -xi[u].z);
+    }
 #pragma unroll
     for (int d = 0; d < 4; d++) acc[u][d] = Comp<T>{0, 0};
   }
-  // source leaf s: (first body, count, periodic image), the next one prefetched
-  const unsigned src0 = s0 < s1 ? (unsigned)pairs[s0] : 0u;
-  int j0 = s0 < s1 ? ibody[pair_cell(src0)] : 0, nj = s0 < s1 ? nbody[pair_cell(src0)] : 0;
-  int img = pair_img(src0);
-  for (int s = s0; s < s1; s++) {
-    int j0n = 0, njn = 0, imgn = 0;
-    if (s + 1 < s1) {
-      const unsigned srcn = (unsigned)pairs[s + 1];
-      j0n = ibody[pair_cell(srcn)];
-      njn = nbody[pair_cell(srcn)];
-      imgn = pair_img(srcn);
-    }
-    T pot[TPL], ax[TPL], ay[TPL], az[TPL];
-    // Bodies at one position share every octant and so one leaf: only the target leaf
-    // itself can hold a pair at r^2 == 0.  Other source leaves take the fast pair form;
-    // if a pair underflowed to r^2 == 0 or below the normal range there, its sum is not
-    // finite and the leaf is summed again in the exact form, so results are always those
-    // of the exact form.
-    if (img != 0) {
-      // a periodic image of a source leaf (r^2 == 0 would take bodies exactly one period
-      // apart): fast form, exact re-sum if not finite
-      T px, py, pz;
-      img_shift<T>(img, cycle, px, py, pz);
-      source_leaf<T, TPL, false, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax,
-                                       ay, az, px, py, pz);
-      bool bad = false;
-#pragma unroll
-      for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(pot[u]);
-      if (__any_sync(0xffffffffu, bad))
-        source_leaf<T, TPL, true, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax,
-                                        ay, az, px, py, pz);
-    } else if (j0 != b0) {
-      source_leaf<T, TPL, false>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
-      bool bad = false;
-#pragma unroll
-      for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(pot[u]);
-      if (__any_sync(0xffffffffu, bad))
-        source_leaf<T, TPL, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
-    } else {
-      source_leaf<T, TPL, true>(lane, wl, sh, sub, G, j0, nj, bodies, eps2, xi, pot, ax, ay, az);
-    }
-#pragma unroll
-    for (int u = 0; u < TPL; u++) {
-      if (COMP) {
-        comp_add(acc[u][0], pot[u]);
-        comp_add(acc[u][1], ax[u]);
-        comp_add(acc[u][2], ay[u]);
-        comp_add(acc[u][3], az[u]);
-      } else {
-        acc[u][0].s += pot[u];
-        acc[u][1].s += ax[u];
-        acc[u][2].s += ay[u];
-        acc[u][3].s += az[u];
-      }
-    }
-    j0 = j0n;
-    nj = njn;
-    img = imgn;
-  }
-  for (int o = 1; o < G; o <<= 1) {
-#pragma unroll
-    for (int u = 0; u < TPL; u++)
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        Comp<T> r;
-        r.s = __shfl_xor_sync(0xffffffffu, acc[u][d].s, o);
-        r.e = __shfl_xor_sync(0xffffffffu, acc[u][d].e, o);
-        if (COMP) comp_merge(acc[u][d], r);
-        else acc[u][d].s += r.s;
-      }
-  }
-  if (sub == 0) {
-#pragma unroll
-    for (int u = 0; u < TPL; u++)
-      if (act[u]) {
-        trg_s[b0 + ti[u]] = make_v4<T>(acc[u][0].s, acc[u][1].s, acc[u][2].s, acc[u][3].s);
-        trg_e[b0 + ti[u]] = make_v4<T>(acc[u][0].e, acc[u][1].e, acc[u][2].e, acc[u][3].e);
-      }
-  }
-}
-
-// FP32 target leaf: the bodies of its source leaves, taken in list order, are staged 32 at
-// a time whatever the leaves' sizes (a chunk runs on into the next source leaf, and ends
-// early only where the periodic image changes or after 32 source leaves), so that the rows
-// are full and the per-chunk work (staging, the finite test, the compensated fold) is
-// shared by all of its source leaves.  The source leaves' descriptors (first body, count,
-// image) are read 32 at a time, one per lane; a lane finds the leaf of its chunk position
-// by a scan of the counts and a binary search over the lanes.  A chunk that holds bodies of
-// the target leaf itself is summed in the exact form; any other chunk in the fast form,
-// and again in the exact form (from the same row) if a sum is not finite, so the results
-// are those of the exact form throughout.
-template <bool COMP, int TPL>
-__device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int nb, int base,
-                                             int G, int s0, int s1,
-                                             const unsigned long long* __restrict__ pairs,
-                                             const int* __restrict__ ibody,
-                                             const int* __restrict__ nbody,
-                                             const vec4<float>* __restrict__ bodies, float eps2,
-                                             float cycle, vec4<float>* __restrict__ trg_s,
-                                             vec4<float>* __restrict__ trg_e) {
-  const unsigned full = 0xffffffffu;
-  const int tpp = 32 / G;
-  const int sub = lane % G;
-  int ti[TPL];
-  bool act[TPL];
-  float2 nx[TPL], ny[TPL], nz[TPL];
-  Comp<float> acc[TPL][4];
-#pragma unroll
-  for (int u = 0; u < TPL; u++) {
-    ti[u] = base + u * tpp + lane / G;
-    act[u] = ti[u] < nb;
-    const vec4<float> x = act[u] ? bodies[b0 + ti[u]] : make_v4<float>(0, 0, 0, 0);
-    nx[u] = make_float2(-x.x, -x.x);
-    ny[u] = make_float2(-x.y, -x.y);
-    nz[u] = make_float2(-x.z, -x.z);
-#pragma unroll
-    for (int d = 0; d < 4; d++) acc[u][d] = Comp<float>{0, 0};
-  }
-  const float2 e2 = make_float2(eps2, eps2);
-  float4* A = row;
-  float4* B = row + 16;
+  const float2 e2 = make_float2((float)eps2, (float)eps2);
   for (int sb = s0; sb < s1; sb += 32) {
     // lane k: source leaf sb + k (image -1 past the end of the list)
     int dj0 = 0, dnj = 0, dimg = -1;
@@ -307,11 +200,32 @@ __device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int 
       const int ex = __shfl_sync(full, incl - avail, f);
       const int jf = __shfl_sync(full, dj0 + (lane == k ? o : 0), f);
       const int bj = jf + lane - ex;
-      const vec4<float> b =
-          lane < cnt ? bodies[bj] : make_v4<float>(1e30f, 1e30f, 1e30f, 0.f);
+      const vec4<T> b = lane < cnt ? bodies[bj] : make_v4<T>(T(1e30), T(1e30), T(1e30), T(0));
       const bool self = __any_sync(full, lane < cnt && img == 0 && bj >= b0 && bj < b0 + nb);
+      T px = 0, py = 0, pz = 0;
+      if (img != 0) img_shift<T>(img, cycle, px, py, pz);
+      Acc sp[TPL], sx[TPL], sy[TPL], sz[TPL];
+      auto zero = [&]() {
+#pragma unroll
+        for (int u = 0; u < TPL; u++) {
+          if constexpr (F32) sp[u] = sx[u] = sy[u] = sz[u] = make_float2(0.f, 0.f);
+          else sp[u] = sx[u] = sy[u] = sz[u] = T(0);
+        }
+      };
+      auto finite = [&]() {
+        bool bad = false;
+#pragma unroll
+        for (int u = 0; u < TPL; u++) {
+          if constexpr (F32) bad |= act[u] && !isfinite(sp[u].x + sp[u].y);
+          else bad |= act[u] && !isfinite(sp[u]);
+        }
+        return !__any_sync(full, bad);
+      };
       __syncwarp();
-      {
+      if constexpr (F32) {
+        // A[i] = (x, x', y, y'), B[i] = (z, z', q, q') for the sources 2i and 2i + 1
+        float4* A = static_cast<float4*>(rowmem);
+        float4* B = A + 16;
         float* a = reinterpret_cast<float*>(&A[lane >> 1]);
         float* c = reinterpret_cast<float*>(&B[lane >> 1]);
         const int h = lane & 1;
@@ -319,52 +233,55 @@ __device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int 
         a[2 + h] = b.y;
         c[h] = b.z;
         c[2 + h] = b.w;
+      } else {
+        static_cast<vec4<T>*>(rowmem)[lane] = b;
       }
       __syncwarp();
-      const int np = (cnt + 1) >> 1;
-      float2 sp[TPL], sx[TPL], sy[TPL], sz[TPL];
-      auto zero = [&]() {
-#pragma unroll
-        for (int u = 0; u < TPL; u++) sp[u] = sx[u] = sy[u] = sz[u] = make_float2(0.f, 0.f);
+      // evaluate the row in the fast or the exact pair form (with or without the shift)
+      auto pairs_of = [&](auto exact, auto shift) {
+        constexpr bool EX = decltype(exact)::value, SH = decltype(shift)::value;
+        if constexpr (F32) {
+          const float2 p2x = make_float2(px, px), p2y = make_float2(py, py),
+                       p2z = make_float2(pz, pz);
+          row_pairs<TPL, EX, SH>(static_cast<const float4*>(rowmem), sub, G, (cnt + 1) >> 1,
+                                 nx, ny, nz, e2, p2x, p2y, p2z, sp, sx, sy, sz);
+        } else {
+          row_pairs<TPL, EX, SH>(static_cast<const vec4<T>*>(rowmem), sub, G, cnt, xi, eps2,
+                                 px, py, pz, sp, sx, sy, sz);
+        }
       };
-      auto finite = [&]() {
-        bool bad = false;
-#pragma unroll
-        for (int u = 0; u < TPL; u++) bad |= act[u] && !isfinite(sp[u].x + sp[u].y);
-        return !__any_sync(full, bad);
-      };
+      using TT = std::true_type;
+      using FF = std::false_type;
       zero();
       if (img != 0) {
-        float px, py, pz;
-        img_shift<float>(img, cycle, px, py, pz);
-        const float2 p2x = make_float2(px, px), p2y = make_float2(py, py),
-                     p2z = make_float2(pz, pz);
-        row_pairs<TPL, false, true>(row, sub, G, np, nx, ny, nz, e2, p2x, p2y, p2z, sp, sx, sy,
-                                    sz);
+        pairs_of(FF(), TT());
         if (!finite()) {
           zero();
-          row_pairs<TPL, true, true>(row, sub, G, np, nx, ny, nz, e2, p2x, p2y, p2z, sp, sx, sy,
-                                     sz);
+          pairs_of(TT(), TT());
         }
+      } else if (self) {
+        pairs_of(TT(), FF());
       } else {
-        const float2 z2 = make_float2(0.f, 0.f);
-        if (self) {
-          row_pairs<TPL, true, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx, sy,
-                                      sz);
-        } else {
-          row_pairs<TPL, false, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx, sy,
-                                       sz);
-          if (!finite()) {
-            zero();
-            row_pairs<TPL, true, false>(row, sub, G, np, nx, ny, nz, e2, z2, z2, z2, sp, sx,
-                                        sy, sz);
-          }
+        pairs_of(FF(), FF());
+        if (!finite()) {
+          zero();
+          pairs_of(TT(), FF());
         }
       }
 #pragma unroll
       for (int u = 0; u < TPL; u++) {
-        const float pot = sp[u].x + sp[u].y, ax = sx[u].x + sx[u].y, ay = sy[u].x + sy[u].y,
-                    az = sz[u].x + sz[u].y;
+        T pot, ax, ay, az;
+        if constexpr (F32) {
+          pot = sp[u].x + sp[u].y;
+          ax = sx[u].x + sx[u].y;
+          ay = sy[u].x + sy[u].y;
+          az = sz[u].x + sz[u].y;
+        } else {
+          pot = sp[u];
+          ax = sx[u];
+          ay = sy[u];
+          az = sz[u];
+        }
         if (COMP) {
           comp_add(acc[u][0], pot);
           comp_add(acc[u][1], ax);
@@ -394,7 +311,7 @@ __device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int 
     for (int u = 0; u < TPL; u++)
 #pragma unroll
       for (int d = 0; d < 4; d++) {
-        Comp<float> r;
+        Comp<T> r;
         r.s = __shfl_xor_sync(full, acc[u][d].s, o);
         r.e = __shfl_xor_sync(full, acc[u][d].e, o);
         if (COMP) comp_merge(acc[u][d], r);
@@ -405,10 +322,8 @@ __device__ __forceinline__ void p2p_leaf_f32(int lane, float4* row, int b0, int 
 #pragma unroll
     for (int u = 0; u < TPL; u++)
       if (act[u]) {
-        trg_s[b0 + ti[u]] =
-            make_v4<float>(acc[u][0].s, acc[u][1].s, acc[u][2].s, acc[u][3].s);
-        trg_e[b0 + ti[u]] =
-            make_v4<float>(acc[u][0].e, acc[u][1].e, acc[u][2].e, acc[u][3].e);
+        trg_s[b0 + ti[u]] = make_v4<T>(acc[u][0].s, acc[u][1].s, acc[u][2].s, acc[u][3].s);
+        trg_e[b0 + ti[u]] = make_v4<T>(acc[u][0].e, acc[u][1].e, acc[u][2].e, acc[u][3].e);
       }
   }
 }
@@ -429,26 +344,14 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
   const int b0 = ibody[c], nb = nbody[c];
   const int G = nb <= 8 ? 4 : (nb <= 16 ? 2 : 1);
   const int s0 = off[c], s1 = off[c + 1];
-  if constexpr (sizeof(T) == 4) {
-    float4* row = reinterpret_cast<float4*>(smem[wl]);
-    if (nb <= 32) {
-      p2p_leaf_f32<COMP, 1>(lane, row, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
-                            cycle, trg_s, trg_e);
-    } else {
-      for (int base = 0; base < nb; base += 64)
-        p2p_leaf_f32<COMP, 2>(lane, row, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
-                              eps2, cycle, trg_s, trg_e);
-    }
+  void* row = smem[wl];
+  if (nb <= 32) {
+    p2p_leaf_chunked<T, COMP, 1>(lane, row, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies,
+                                 eps2, cycle, trg_s, trg_e);
   } else {
-    vec4<T>(*sh)[32] = reinterpret_cast<vec4<T>(*)[32]>(&smem[0][0]);
-    if (nb <= 32) {
-      p2p_leaf<T, COMP, 1>(lane, wl, sh, b0, nb, 0, G, s0, s1, pairs, ibody, nbody, bodies, eps2,
-                           cycle, trg_s, trg_e);
-    } else {
-      for (int base = 0; base < nb; base += 64)
-        p2p_leaf<T, COMP, 2>(lane, wl, sh, b0, nb, base, 1, s0, s1, pairs, ibody, nbody, bodies,
-                             eps2, cycle, trg_s, trg_e);
-    }
+    for (int base = 0; base < nb; base += 64)
+      p2p_leaf_chunked<T, COMP, 2>(lane, row, b0, nb, base, 1, s0, s1, pairs, ibody, nbody,
+                                   bodies, eps2, cycle, trg_s, trg_e);
   }
 }
 

@@ -1,15 +1,16 @@
 // Spherical-basis expansion kernels (P2M, M2M, M2L, L2L, L2P) for compile-time P.
 //
-// Warp mappings:
+// Mappings (the same kernels in FP32 and FP64; register and thread budgets per precision):
 //   P2M  warp per leaf, lane per body; each lane's q conj(Y) row goes to shared memory and
 //        the warp sums columns in body order, so M[0] is the reference's sequential sum.
-//   M2M  warp per parent, lane per output coefficient, children in order (reference order
-//        of Ci->M += ..., include/up_down_pass.h:79-80 / LaplaceSphericalCPU.cxx:143).
-//   M2L  FP32: warp per target cell, lane per source cell, harmonics and the local
-//        expansion held in registers, one warp reduction per target.  FP64: warp per
-//        target, lanes over output coefficients (harmonics in shared memory).
-//   L2L  warp per cell, lane per output coefficient.
-//   L2P  warp per leaf, lane per body, harmonics generated and consumed on the fly.
+//   M2M  8 lanes per parent, one child each, compile-time indices; children summed in a
+//        fixed order and the monopole in the reference's child order
+//        (include/up_down_pass.h:79-80 / LaplaceSphericalCPU.cxx:143).
+//   M2L  warp per target cell, lane per source cell, each pair contracted in the source's
+//        azimuthal frame with the harmonics and the local expansion held in registers,
+//        passes over the output degrees, one warp reduction per target.
+//   L2L  thread per cell, the parent's local staged in the thread's row of shared memory.
+//   L2P  thread per body, harmonics generated and consumed on the fly.
 // setRmax / R /= theta (include/up_down_pass.h:51-67, :81-82) are fused into P2M and M2M.
 #pragma once
 #include <algorithm>
@@ -19,9 +20,6 @@
 
 namespace fmmb200 {
 
-template <typename T> struct SphCfg {
-  static constexpr int W = sizeof(T) == 4 ? 4 : 2;  // warps per block
-};
 // P2M keeps one row of 2 NT (+1 pad) values per lane in shared memory: as many warps per
 // block as fit in 40 KB of static shared memory.
 template <typename T, int P> struct P2MCfg {
@@ -112,80 +110,15 @@ __device__ __forceinline__ void jk_of(int t, int& j, int& k) {
 }
 
 // ---------------------------------------------------------------- M2M (+ setRmax)
-template <typename T, int P>
-__global__ void __launch_bounds__(32 * SphCfg<T>::W)
-    k_m2m(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
-          const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
-          int ncoef, int use_rmax, T theta, int write_r) {
-  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
-  constexpr int W = SphCfg<T>::W;
-  __shared__ T sy[W][NC], sm[W][NC];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int v = lo + blockIdx.x * W + wl;
-  if (v >= hi) return;
-  const int c = npos[v];
-  const int nch = nchild[c];
-  if (nch == 0) return;
-  const int c0 = ichild[c];
-  const vec4<T> Xp = cX[c];
-  T ar[KO], ai[KO];
-  int oj[KO], ok[KO];
-#pragma unroll
-  for (int i = 0; i < KO; i++) {
-    ar[i] = ai[i] = 0;
-    jk_of(lane + 32 * i, oj[i], ok[i]);
-  }
-  T rmax = 0;
-  for (int ch = 0; ch < nch; ch++) {
-    const int cc = c0 + ch;
-    const vec4<T> Xc = cX[cc];
-    {
-      T yr[NT], yi[NT];
-      sph::Angles<T> a = sph::angles(Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
-      sph::multipole<T, P>(a, a.r, yr, yi);
-      __syncwarp();
-      spread_y<T, NT>(yr, yi, sy[wl], lane);
-      for (int t = lane; t < NC; t += 32) sm[wl][t] = M[(size_t)cc * ncoef + t];
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < KO; i++) {
-      if (lane + 32 * i < NT) {
-        T r, im;
-        sph::m2m_term<T>(oj[i], ok[i], sy[wl], sy[wl] + NT, sm[wl], r, im);
-        ar[i] += r;
-        ai[i] += im;
-      }
-    }
-    if (lane == ch) {
-      const T d = sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z)));
-      rmax = add_rn(d, Xc.w);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < KO; i++) {
-    const int t = lane + 32 * i;
-    if (t < NT) {
-      M[(size_t)c * ncoef + 2 * t] = ar[i];
-      M[(size_t)c * ncoef + 2 * t + 1] = ai[i];
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const T x = __shfl_xor_sync(0xffffffffu, rmax, o);
-    rmax = x > rmax ? x : rmax;
-  }
-  if (lane == 0 && write_r) {
-    T R = Xp.w;
-    if (use_rmax) R = rmax < R ? rmax : R;
-    cX[c].w = div_rn(R, theta);
-  }
+// output degrees per M2M / L2L pass: at most 24 complex outputs per pass in FP32, 12 in
+// FP64 (the same registers)
+template <typename T> __host__ __device__ constexpr int tr_pass_outs() {
+  return sizeof(T) == 4 ? 24 : 12;
 }
-
-// output degrees per FP32 M2M / L2L pass: at most 24 complex outputs per pass
+template <typename T>
 __host__ __device__ constexpr int tr_pass_end(int P, int J0) {
   int j = J0 + 1;
-  while (j < P && sph::NT(j + 1) - sph::NT(J0) <= 24) j++;
+  while (j < P && sph::NT(j + 1) - sph::NT(J0) <= tr_pass_outs<T>()) j++;
   return j;
 }
 
@@ -194,7 +127,7 @@ template <typename T, int P, int J0>
 __device__ __forceinline__ void m2m_passes(const T* yr, const T* yi, const T* Mc, bool has,
                                            int slot, T* Mp, T m0) {
   if constexpr (J0 < P) {
-    constexpr int J1 = tr_pass_end(P, J0);
+    constexpr int J1 = tr_pass_end<T>(P, J0);
     constexpr int NO = 2 * (sph::sidx(J1, 0) - sph::sidx(J0, 0));
     T acc[NO];
 #pragma unroll
@@ -214,23 +147,24 @@ __device__ __forceinline__ void m2m_passes(const T* yr, const T* yi, const T* Mc
   }
 }
 
-// FP32 M2M: 8 lanes per parent (one per child slot), 4 parents per warp; each lane
-// translates its child with compile-time indices, the group sums in a fixed order, and the
-// monopole is re-summed in child order (the reference's sequence) so that the radii of the
-// error-optimised MAC see the same M[0] bits.
-// Threads per block of the FP32 M2M / L2L kernels; each thread stages the expansion it
-// translates (its child's multipole, its parent's local) in its own row of shared memory
-// first, with all the loads issued at once: read term by term from global memory, their
-// latencies added up along the translation's dependent chain (~40 us per level).
-constexpr int kTrThreads = 64;
+// M2M (either precision): 8 lanes per parent (one per child slot), 4 parents per warp;
+// each lane translates its child with compile-time indices, the group sums in a fixed
+// order, and the monopole is re-summed in child order (the reference's sequence) so that
+// the radii of the error-optimised MAC see the same M[0] bits.
+// Threads per block of the M2M / L2L kernels (64 in FP32, 32 in FP64: the same shared
+// memory); each thread stages the expansion it translates (its child's multipole, its
+// parent's local) in its own row of shared memory first, with all the loads issued at once:
+// read term by term from global memory, their latencies added up along the translation's
+// dependent chain (~40 us per level).
+template <typename T> constexpr int tr_threads() { return sizeof(T) == 4 ? 64 : 32; }
 
 template <typename T, int P>
-__global__ void __launch_bounds__(kTrThreads)
+__global__ void __launch_bounds__(tr_threads<T>())
     k_m2m_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
               const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
               int ncoef, int use_rmax, T theta, int write_r) {
   constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;  // odd row stride: no bank conflicts
-  __shared__ T rows[kTrThreads * STR];
+  __shared__ T rows[tr_threads<T>() * STR];
   T* row = rows + threadIdx.x * STR;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = lo + (gt >> 3);
@@ -278,7 +212,7 @@ __global__ void __launch_bounds__(kTrThreads)
 template <typename T, int P, int J0>
 __device__ __forceinline__ void l2l_passes(const T* yr, const T* yi, const T* Lp, T* Lc) {
   if constexpr (J0 < P) {
-    constexpr int J1 = tr_pass_end(P, J0);
+    constexpr int J1 = tr_pass_end<T>(P, J0);
     constexpr int NO = 2 * (sph::sidx(J1, 0) - sph::sidx(J0, 0));
     T acc[NO];
 #pragma unroll
@@ -290,14 +224,14 @@ __device__ __forceinline__ void l2l_passes(const T* yr, const T* yi, const T* Lp
   }
 }
 
-// FP32 L2L: thread per cell, compile-time indices, the parent's local staged in the
-// thread's shared row.
+// L2L (either precision): thread per cell, compile-time indices, the parent's local staged
+// in the thread's shared row.
 template <typename T, int P>
-__global__ void __launch_bounds__(kTrThreads)
+__global__ void __launch_bounds__(tr_threads<T>())
     k_l2l_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
               const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
   constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;
-  __shared__ T rows[kTrThreads * STR];
+  __shared__ T rows[tr_threads<T>() * STR];
   T* row = rows + threadIdx.x * STR;
   const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= hi) return;
@@ -314,44 +248,47 @@ __global__ void __launch_bounds__(kTrThreads)
 }
 
 // ---------------------------------------------------------------- M2L
-// FP32: warp per target, lane per source cell, harmonics and local expansion in registers,
-// one warp reduction per target cell at the end.  Each pair is contracted in the source's
-// azimuthal frame (m2l_pair_rot: real harmonic factors, half the multiply-adds of the
-// complex form).  The outputs are split into passes over their degree (separate launches)
-// so that each pass's registers stay within one block of 12 warps per SM.
-constexpr int kM2LWarps = 12;
-// FP32 M2L passes over the output degrees.  Registers of a pass [J0, J1) (besides the
-// phases e^(i m beta)): the real harmonic factors of degrees >= J0, the accumulators (two
-// per output), and either the pair's rotated sums A (two per output: source coefficients
+// Warp per target, lane per source cell, harmonics and local expansion in registers, one
+// warp reduction per target cell at the end (either precision).  Each pair is contracted in
+// the source's azimuthal frame (m2l_pair_rot: real harmonic factors, half the multiply-adds
+// of the complex form).  The outputs are split into passes over their degree (separate
+// launches) so that each pass's registers stay within its block's share.
+// Passes over the output degrees.  Registers of a pass [J0, J1) (besides the phases
+// e^(i m beta)): the real harmonic factors of degrees >= J0, the accumulators (two per
+// output), and either the pair's rotated sums A (two per output: source coefficients
 // streamed, m2l_pair_rot) or the rotated source coefficients of degrees < P - J0 (two per
-// coefficient: outputs streamed, m2l_pair_rot_out).  The last pass streams its outputs
-// once the remaining degrees fit kM2LOutRegs; the passes before it stream the source and
-// add degrees while they fit kM2LInRegs.
-constexpr int kM2LInRegs = 115, kM2LOutRegs = 150;
+// coefficient: outputs streamed, m2l_pair_rot_out).  The last pass streams its outputs once
+// the remaining degrees fit OUT values; the passes before it stream the source and add
+// degrees while they fit IN values.
+//   FP32: 12 warps per block (3 per SM sub-partition, whose 16 K registers then allow 168
+//         per thread); P = 10 takes the passes [0, 5) and [5, 10), at 168 registers each,
+//         the second with a small spill.
+//   FP64: 8 warps per block (255 registers per thread), the budgets in values about half
+//         of FP32's in registers; P = 10 takes four passes, none spilling.
+template <typename T> struct M2LBudget {
+  static constexpr int W = sizeof(T) == 4 ? 12 : 8;
+  static constexpr int IN = sizeof(T) == 4 ? 115 : 100;
+  static constexpr int OUT = sizeof(T) == 4 ? 150 : 105;
+};
 __host__ __device__ constexpr int m2l_regs_out(int P, int J0) {
   return sph::NT(P) - sph::sidx(J0, 0) + 2 * (sph::NT(P) - sph::sidx(J0, 0)) +
          2 * sph::NT(P - J0);
 }
-__host__ __device__ constexpr bool m2l_pass_out(int P, int J0) {
-  return m2l_regs_out(P, J0) <= kM2LOutRegs;
+template <typename T> __host__ __device__ constexpr bool m2l_pass_out(int P, int J0) {
+  return m2l_regs_out(P, J0) <= M2LBudget<T>::OUT;
 }
-__host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
-  if (m2l_pass_out(P, J0)) return P;
+template <typename T> __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
+  if (m2l_pass_out<T>(P, J0)) return P;
   const int rho = sph::NT(P) - sph::sidx(J0, 0);
   int j = J0, outs = 0;
   while (j < P) {
     const int o = outs + j + 1;
-    if (j > J0 && (rho + 4 * o > kM2LInRegs || m2l_pass_out(P, j))) break;
+    if (j > J0 && (rho + 4 * o > M2LBudget<T>::IN || m2l_pass_out<T>(P, j))) break;
     outs = o;
     j++;
   }
   return j;
 }
-
-// warps per block of one FP32 M2L pass: 12 (3 per SM sub-partition, whose 16 K registers
-// then allow 168 per thread; P = 10 takes the passes [0, 5) and [5, 10), at 168 registers
-// each, the second with a small spill)
-__host__ __device__ constexpr int m2l_pass_warps(int, int) { return kM2LWarps; }
 
 // Each warp runs its target's batches of 32 sources on its own; targets arrive ordered by
 // their number of batches, so the warps of a block have about the same amount of work and
@@ -387,7 +324,7 @@ __global__ void __launch_bounds__(32 * W)
       sph::Angles<T> a =
           sph::angles_rs(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz, invr);
       sph::local_rho<T, P, J0>(a, invr, rho, cr, ci);
-      if constexpr (m2l_pass_out(P, J0))
+      if constexpr (m2l_pass_out<T>(P, J0))
         sph::m2l_pair_rot_out<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
       else
         sph::m2l_pair_rot<T, P, J0, J1>(rho, cr, ci, M + (size_t)j * ncoef, Lr, Li);
@@ -407,8 +344,8 @@ __global__ void __launch_bounds__(32 * W)
 template <typename T, int P, int J0>
 static void launch_m2l_passes(Solver<T>& s) {
   if constexpr (J0 < P) {
-    constexpr int J1 = m2l_pass_end(P, J0);
-    constexpr int W = m2l_pass_warps(P, J0);
+    constexpr int J1 = m2l_pass_end<T>(P, J0);
+    constexpr int W = M2LBudget<T>::W;
     k_m2l_reg<T, P, J0, J1, W><<<ceil_div(s.m2l_ntgt, W), 32 * W, 0, s.stream>>>(
         s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef,
         (T)s.cfg.cycle);
@@ -460,101 +397,6 @@ __device__ __forceinline__ void m2l_term(int P, int j, int k, const T* y, const 
   outi = si;
 }
 
-// FP64: lanes over output coefficients; outputs dealt so heavy (low j) and light (high j)
-// coefficients pair up on a lane.
-template <typename T, int P>
-__global__ void __launch_bounds__(32 * SphCfg<T>::W)
-    k_m2l_lanes(int ncells, const int* __restrict__ off,
-                const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
-                const T* __restrict__ M, T* __restrict__ L, int ncoef, T cycle) {
-  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
-  constexpr int W = SphCfg<T>::W;
-  __shared__ T sy[W][NC], sm[W][NC];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int c = blockIdx.x * W + wl;
-  if (c >= ncells) return;
-  const int s0 = off[c], s1 = off[c + 1];
-  if (s0 == s1) return;
-  const vec4<T> Xi = cX[c];
-  T ar[KO], ai[KO];
-  int ot[KO], oj[KO], ok[KO];
-#pragma unroll
-  for (int i = 0; i < KO; i++) {
-    ar[i] = ai[i] = 0;
-    const int cnt = NT - 32 * i < 32 ? NT - 32 * i : 32;  // outputs in block i
-    ot[i] = (i & 1) ? (lane < cnt ? 32 * i + cnt - 1 - lane : NT) : lane + 32 * i;
-    jk_of(ot[i] < NT ? ot[i] : 0, oj[i], ok[i]);
-  }
-  for (int s = s0; s < s1; s++) {
-    const unsigned src = (unsigned)pairs[s];
-    const int j = pair_cell(src);
-    T px, py, pz;  // periodic shift of the source (0 without images)
-    img_shift<T>(pair_img(src), cycle, px, py, pz);
-    const vec4<T> Xj = cX[j];
-    {
-      T yr[NT], yi[NT];
-      sph::Angles<T> a = sph::angles(Xi.x - Xj.x - px, Xi.y - Xj.y - py, Xi.z - Xj.z - pz);
-      sph::local<T, P>(a, yr, yi);
-      __syncwarp();
-      spread_y<T, NT>(yr, yi, sy[wl], lane);
-      for (int t = lane; t < NC; t += 32) sm[wl][t] = M[(size_t)j * ncoef + t];
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < KO; i++) {
-      if (ot[i] < NT) {
-        T r, im;
-        m2l_term<T>(P, oj[i], ok[i], sy[wl], sm[wl], r, im);
-        ar[i] += r;
-        ai[i] += im;
-      }
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < KO; i++) {
-    if (ot[i] < NT) {
-      L[(size_t)c * ncoef + 2 * ot[i]] += ar[i];
-      L[(size_t)c * ncoef + 2 * ot[i] + 1] += ai[i];
-    }
-  }
-}
-
-// ---------------------------------------------------------------- L2L
-template <typename T, int P>
-__global__ void __launch_bounds__(32 * SphCfg<T>::W)
-    k_l2l(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
-          const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
-  constexpr int NT = sph::NT(P), NC = 2 * NT, KO = (NT + 31) / 32;
-  constexpr int W = SphCfg<T>::W;
-  __shared__ T sy[W][NC], sl[W][NC];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int v = lo + blockIdx.x * W + wl;
-  if (v >= hi) return;
-  const int c = npos[v];
-  const int p = iparent[c];
-  const vec4<T> Xc = cX[c], Xp = cX[p];
-  {
-    T yr[NT], yi[NT];
-    sph::Angles<T> a = sph::angles(Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
-    sph::multipole<T, P>(a, a.r, yr, yi);
-    spread_y<T, NT>(yr, yi, sy[wl], lane);
-    for (int t = lane; t < NC; t += 32) sl[wl][t] = L[(size_t)p * ncoef + t];
-  }
-  __syncwarp();
-#pragma unroll
-  for (int i = 0; i < KO; i++) {
-    const int t = lane + 32 * i;
-    if (t < NT) {
-      int j, k;
-      jk_of(t, j, k);
-      T r, im;
-      sph::l2l_term<T>(P, j, k, sy[wl], sy[wl] + NT, sl[wl], r, im);
-      L[(size_t)c * ncoef + 2 * t] += r;
-      L[(size_t)c * ncoef + 2 * t + 1] += im;
-    }
-  }
-}
-
 // L2P with one thread per body (tree order), its leaf from the map P2M wrote, the leaf's
 // local expansion read through L1 (the bodies of a warp share one to three leaves): every
 // lane busy whatever the leaf sizes; the arithmetic per body is that of k_l2p
@@ -566,6 +408,7 @@ __global__ void __launch_bounds__(128)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = body_leaf[i];
+  if (c < 0) return;  // a body outside the cells of a single-operator call
   const vec4<T> C = cX[c];
   const vec4<T> b = bodies[i];
   T pot, gx, gy, gz;
@@ -591,40 +434,18 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
-  if constexpr (sizeof(T) == 4) {
-    k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), kTrThreads), kTrThreads, 0, s.stream>>>(
-        lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
-        (T)s.cfg.theta, s.write_r);
-    FMM_LAUNCH_CHECK();
-  } else {
-    constexpr int W = SphCfg<T>::W;
-    k_m2m<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(
-        lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
-        (T)s.cfg.theta, s.write_r);
-    FMM_LAUNCH_CHECK();
-  }
+  constexpr int NTH = tr_threads<T>();
+  k_m2m_reg<T, P><<<ceil_div(8LL * (hi - lo), NTH), NTH, 0, s.stream>>>(
+      lo, hi, s.npos.p, s.c_ichild.p, s.c_nchild.p, s.cX.p, s.M.p, s.ncoef, s.cfg.use_rmax,
+      (T)s.cfg.theta, s.write_r);
+  FMM_LAUNCH_CHECK();
 }
-template <typename T, int P> static void m2l_(Solver<T>& s) {
-  if constexpr (sizeof(T) == 4) {
-    launch_m2l_passes<T, P, 0>(s);
-  } else {
-    constexpr int W = SphCfg<T>::W;
-    k_m2l_lanes<T, P><<<ceil_div(s.ncells, W), 32 * W, 0, s.stream>>>(
-        s.ncells, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef, (T)s.cfg.cycle);
-    FMM_LAUNCH_CHECK();
-  }
-}
+template <typename T, int P> static void m2l_(Solver<T>& s) { launch_m2l_passes<T, P, 0>(s); }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
-  if constexpr (sizeof(T) == 4) {
-    k_l2l_reg<T, P><<<ceil_div(hi - lo, kTrThreads), kTrThreads, 0, s.stream>>>(
-        lo, hi, s.npos.p, s.c_iparent.p, s.cX.p, s.L.p, s.ncoef);
-    FMM_LAUNCH_CHECK();
-  } else {
-    constexpr int W = SphCfg<T>::W;
-    k_l2l<T, P><<<ceil_div(hi - lo, W), 32 * W, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
+  constexpr int NTH = tr_threads<T>();
+  k_l2l_reg<T, P><<<ceil_div(hi - lo, NTH), NTH, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
                                                                 s.cX.p, s.L.p, s.ncoef);
-    FMM_LAUNCH_CHECK();
-  }
+  FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   if (!s.nleaves) return;

@@ -578,13 +578,13 @@ def main():
         t = solver.timings()
         phase_sum = t if phase_sum is None else {k: phase_sum[k] + t[k] for k in t}
     torch.cuda.synchronize()
+    launches = (fmm.kernel_launches() - launches0) // args.steps
     # keep the GPU under the same load until the sampler has a few readings
     t_extra = time.perf_counter()
     while len(clocks.rows) < 5 and time.perf_counter() - t_extra < 3.0:
         step(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         torch.cuda.synchronize()
     clk = clocks.stop()
-    launches = (fmm.kernel_launches() - launches0) // args.steps
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = float(sum(step_ms))
     if pg:

@@ -27,6 +27,7 @@ FMM_OK, FMM_ERR_INVALID, FMM_ERR_CUDA, FMM_ERR_NOT_SUPPORTED = 0, 1, 2, 3
 FMM_ERR_NO_MEMORY, FMM_ERR_STATE, FMM_ERR_NO_DEVICE, FMM_ERR_DEVICE = 4, 5, 6, 7
 SPHERICAL, CARTESIAN = 0, 1
 FP32, FP64 = 0, 1
+TREE_ADAPTIVE, TREE_UNIFORM = 0, 1
 PHASES = ("bounds", "tree", "upward", "traverse", "m2l", "p2p", "downward", "total")
 
 
@@ -42,7 +43,7 @@ class Config(C.Structure):
                 ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
                 ("use_ropt", C.c_int), ("precision", C.c_int), ("eps2", C.c_double),
                 ("images", C.c_int), ("device", C.c_int), ("cycle", C.c_double),
-                ("mutual", C.c_int)]
+                ("mutual", C.c_int), ("tree", C.c_int)]
 
 
 # every entry point of include/exafmm_b200.h with its ctypes signature
@@ -81,6 +82,16 @@ SIGNATURES = {
     "fmm_b200_num_lists": (_i, [_vp, _vp, _vp, _vp]),
     "fmm_b200_get_lists": (_i, [_vp, _vp, _vp]),
     "fmm_b200_get_timings": (_i, [_vp, _vp]),
+    "fmm_b200_kernel_set_cells": (_i, [_vp, _i] + [_vp] * 7),
+    "fmm_b200_kernel_set_expansion": (_i, [_vp, _i, _vp]),
+    "fmm_b200_kernel_set_trg": (_i, [_vp, _vp]),
+    "fmm_b200_kernel_get_trg": (_i, [_vp, _vp]),
+    "fmm_b200_kernel_p2m": (_i, [_vp, _i, _vp]),
+    "fmm_b200_kernel_m2m": (_i, [_vp, _i, _vp]),
+    "fmm_b200_kernel_m2l": (_i, [_vp, _i, _vp, _vp, _vp, _i]),
+    "fmm_b200_kernel_l2l": (_i, [_vp, _i, _vp]),
+    "fmm_b200_kernel_l2p": (_i, [_vp, _i, _vp]),
+    "fmm_b200_kernel_p2p": (_i, [_vp, _i, _vp, _vp, _vp, _i, _d]),
     "fmm_b200_server_create": (_i, [_vp, _d, _i, _i, _vp]),
     "fmm_b200_server_submit": (_i, [_vp, _i, _vp, _vp, _i, _vp]),
     "fmm_b200_server_set_theta": (_i, [_vp, _i, _d]),
@@ -205,7 +216,9 @@ class Solver:
 
     def __init__(self, basis="spherical", P=10, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
                  use_ropt=1, precision="f32", eps2=0.0, images=0, device=0,
-                 cycle=2 * np.pi, mutual=0):
+                 cycle=2 * np.pi, mutual=0, tree="adaptive"):
+        """tree: "adaptive" (BuildTree of include/build_tree_tbb.h) or "uniform" (the uniform
+        Morton tree of include/build_tree_omp.h)."""
         self.lib = load_library()
         cfg = Config()
         self.lib.fmm_b200_default_config(C.byref(cfg))
@@ -213,6 +226,7 @@ class Solver:
         cfg.nspawn, cfg.use_rmax, cfg.use_ropt = nspawn, use_rmax, use_ropt
         cfg.precision, cfg.eps2, cfg.images, cfg.device = _prec(precision), eps2, images, device
         cfg.cycle, cfg.mutual = cycle, mutual
+        cfg.tree = {"adaptive": TREE_ADAPTIVE, "uniform": TREE_UNIFORM}[tree]
         self.cfg = cfg
         self.h = C.c_void_p()
         rc = self.lib.fmm_b200_create(C.byref(cfg), C.byref(self.h))

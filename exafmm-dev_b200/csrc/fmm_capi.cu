@@ -10,14 +10,10 @@
 #include <vector>
 #include <string>
 
-#include "fmm_solver.cuh"
+#include "fmm_handle.cuh"
 
 using namespace fmmb200;
 
-struct fmm_b200_solver {
-  int precision = FMM_FP32;
-  SolverBase* base = nullptr;
-};
 
 static thread_local std::string g_create_error;
 
@@ -85,24 +81,6 @@ __global__ void k_to_double(size_t n, const T* __restrict__ in, double* __restri
 }  // namespace fmmb200
 
 namespace {
-
-template <typename T> Solver<T>& S(fmm_b200_solver* h) { return *static_cast<Solver<T>*>(h->base); }
-
-template <typename F> int guarded(fmm_b200_solver* h, F&& f) {
-  if (!h || !h->base) return FMM_ERR_INVALID;
-  try {
-    FMM_CUDA(cudaSetDevice(h->base->cfg.device));
-    f();
-    h->base->err.clear();
-    return FMM_OK;
-  } catch (const FmmError& e) {
-    h->base->err = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    h->base->err = e.what();
-    return FMM_ERR_INVALID;
-  }
-}
 
 // body ranges of a batch of solves from their counts (host); false on a bad count
 bool set_segments(SolverBase& s, int nsolves, const int* counts, int* total) {
@@ -354,6 +332,7 @@ int fmm_b200_default_config(fmm_b200_config* c) {
   c->device = 0;
   c->cycle = 2 * M_PI;
   c->mutual = 0;
+  c->tree = FMM_TREE_ADAPTIVE;
   return FMM_OK;
 }
 
@@ -380,6 +359,10 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
   }
   if (cfg->mutual != 0 && cfg->mutual != 1) {
     g_create_error = "mutual must be 0 or 1";
+    return FMM_ERR_INVALID;
+  }
+  if (cfg->tree != FMM_TREE_ADAPTIVE && cfg->tree != FMM_TREE_UNIFORM) {
+    g_create_error = "tree must be FMM_TREE_ADAPTIVE or FMM_TREE_UNIFORM";
     return FMM_ERR_INVALID;
   }
   std::vector<int> ords = cfg->basis == FMM_CARTESIAN ? cartesian_orders() : spherical_orders();
@@ -500,19 +483,6 @@ const char* fmm_b200_last_error(const fmm_b200_solver* h) {
   if (!h || !h->base) return g_create_error.c_str();
   return h->base->err.c_str();
 }
-
-#define FMM_DISPATCH(h, ...)                                   \
-  guarded(h, [&] {                                             \
-    if (h->precision == FMM_FP64) {                            \
-      using T = double;                                        \
-      Solver<T>& s = S<T>(h);                                  \
-      __VA_ARGS__;                                             \
-    } else {                                                   \
-      using T = float;                                         \
-      Solver<T>& s = S<T>(h);                                  \
-      __VA_ARGS__;                                             \
-    }                                                          \
-  })
 
 int fmm_b200_set_bodies_host(fmm_b200_solver* h, int n, const double* x, const double* q) {
   if (n < 0 || (n > 0 && (!x || !q))) return FMM_ERR_INVALID;

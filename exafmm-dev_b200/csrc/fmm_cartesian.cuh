@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(128)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = body_leaf[i];
+  if (c < 0) return;  // a body outside the cells of a single-operator call
   const vec4<T> X = cX[c];
   const vec4<T> b = bodies[i];
   T pot, gx, gy, gz;

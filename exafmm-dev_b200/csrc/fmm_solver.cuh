@@ -138,6 +138,11 @@ struct SolverBase {
   cudaStream_t side = nullptr;
   cudaStream_t side_lo = nullptr;  // lowest priority: the upward expansions beside the traversal
   cudaEvent_t fork = nullptr, join = nullptr;
+  // single-operator calls (fmm_kernels.cu): host copies of the cells' index fields for
+  // argument checks (valid while kc_valid), the operator's cell list, saved values
+  bool kc_valid = false;
+  std::vector<int> kc_ibody, kc_nbody, kc_ichild, kc_nchild, kc_iparent;
+  DevArr<int> k_list, k_saved_leaves;
   virtual ~SolverBase() {}
 };
 
@@ -149,6 +154,8 @@ template <typename T> struct Solver : SolverBase {
   DevArr<T> pM, pM2, pC;  // periodic cell multipoles and per-shift M2L terms
   DevArr<int> c_root_cells;
   DevArr<T> minmax_part;
+  DevArr<T> k_rows;             // single-operator calls: saved expansion rows
+  DevArr<vec4<T>> k_cx, k_trg;  // saved cell centres / radii, saved targets (sum, error)
 };
 
 // ---- stage implementations (one translation unit each) ---------------------------------

@@ -601,9 +601,239 @@ static bool planned_levels(Solver<T>& s, int nroots, DevArr<int>** narr, int nna
   return true;
 }
 
+// ---------------------------------------------------------------- uniform Morton tree
+// BuildTree of include/build_tree_omp.h:214-262 (the builder of an OpenMP build without TBB,
+// include/build_tree.h:12-13): every leaf at the depth `level` the host computes as the
+// reference does (:218), bodies keyed by the interleaved bits of their grid cell at the
+// leaf size d (getKey :36-57), stably sorted by key (radixSort :59-121), one leaf per run of
+// equal keys (bodies2leafs :130-158), the parents of each level one per run of equal
+// key / 8^l (leafs2cells :160-198), then the cell array reversed (reverseOrder :200-211):
+// root first, each level in descending key order, children contiguous.  The cells are
+// formed in the reference's construction order (leaves ascending, then each level above)
+// and written at index ncells - 1 - c, with the reference's values throughout, including
+// its root IPARENT (ncells - 1) and leaf ICHILD (ncells).
+constexpr int kUniformMaxLevel = 10;  // the reference's `int id` holds 3 level bits (:45)
+
+// the cell size of a level as getKey declares it: `float d = 2 * box.R / (1 << level)`
+// evaluated in the working precision, then made a float (:38); a level above doubles it
+// in float (:166)
+template <typename T>
+__device__ __forceinline__ float uniform_d(const T* __restrict__ box, int level) {
+  return (float)div_rn(mul_rn(T(2), box[3]), (T)(1 << level));
+}
+// grid index along one axis: (X - Xmin) / d in the working precision (d promoted), truncated
+template <typename T> __device__ __forceinline__ int uniform_ix(T x, T xmin, float d) {
+  return (int)div_rn(sub_rn(x, xmin), (T)d);
+}
+
+template <typename T>
+__global__ void k_ukeys(const vec4<T>* __restrict__ b, int n, const T* __restrict__ box,
+                        int level, unsigned long long* __restrict__ key, int* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float d = uniform_d(box, level);
+  const vec4<T> x = b[i];
+  int ix = uniform_ix(x.x, box[4], d), iy = uniform_ix(x.y, box[5], d),
+      iz = uniform_ix(x.z, box[6], d);
+  int id = 0;
+  for (int l = 0; l < level; l++) {
+    id += (ix & 1) << (3 * l);
+    id += (iy & 1) << (3 * l + 1);
+    id += (iz & 1) << (3 * l + 2);
+    ix >>= 1;
+    iy >>= 1;
+    iz >>= 1;
+  }
+  key[i] = (unsigned long long)id;
+  idx[i] = i;
+}
+
+// run heads one level up: child c (construction index cb + c; its first body fb[cb + c], or
+// the body c itself when fb is null) starts a new cell when its key shifted right by
+// `shift` differs from its predecessor's; flags[m] = 0 closes the scan
+__global__ void k_uheads(int m, int cb, const int* __restrict__ fb,
+                         const unsigned long long* __restrict__ key, int shift,
+                         int* __restrict__ flags) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > m) return;
+  if (c == m) {
+    flags[m] = 0;
+    return;
+  }
+  const int b = fb ? fb[cb + c] : c;
+  const int bp = c == 0 ? 0 : (fb ? fb[cb + c - 1] : c - 1);
+  flags[c] = c == 0 || (key[b] >> shift) != (key[bp] >> shift);
+}
+
+// the cells of one level from the run heads of the level below (construction order: the new
+// cells from ce on); body runs for the leaves (fb == null), cell runs above (ch0, par)
+__global__ void k_uemit(int m, int cb, int ce, const int* __restrict__ flags,
+                        const int* __restrict__ pos, int* __restrict__ fb,
+                        int* __restrict__ ch0, int* __restrict__ par, bool leaves) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m) return;
+  const int r = pos[c] + flags[c] - 1;  // the new cell this child (or body) belongs to
+  if (flags[c]) {
+    fb[ce + r] = leaves ? c : fb[cb + c];
+    ch0[ce + r] = leaves ? 0 : cb + c;
+  }
+  if (!leaves) par[cb + c] = ce + r;
+}
+
+struct UniformLevels {
+  int begin[kUniformMaxLevel + 2];  // construction range of level l: [begin[l], end[l])
+  int end[kUniformMaxLevel + 2];
+};
+
+// cell records at index ncells - 1 - c for construction index c (reverseOrder)
+template <typename T>
+__global__ void k_ucells(int nc, int n, int level, UniformLevels lv, const T* __restrict__ box,
+                         const int* __restrict__ fb, const int* __restrict__ ch0,
+                         const int* __restrict__ par, const unsigned long long* __restrict__ key,
+                         const vec4<T>* __restrict__ bodies, int* __restrict__ iparent,
+                         int* __restrict__ ichild, int* __restrict__ nchild,
+                         int* __restrict__ ibody, int* __restrict__ nbody,
+                         int* __restrict__ clevel, unsigned long long* __restrict__ icell,
+                         vec4<T>* __restrict__ cX, int* __restrict__ croot) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  int L = level;
+  while (c >= lv.end[L]) L--;  // levels are laid out leaves first
+  const int f = nc - 1 - c;
+  const int b = fb[c];
+  const int nb = (c + 1 < lv.end[L] ? fb[c + 1] : n) - b;
+  int nch = 0;
+  if (L < level) nch = (c + 1 < lv.end[L] ? ch0[c + 1] : lv.end[L + 1]) - ch0[c];
+  // reverseOrder: ICHILD = perm[ICHILD] - NCHILD + 1 (a leaf's ICHILD 0 goes to nc),
+  // IPARENT = perm[IPARENT] (the root's IPARENT 0 goes to nc - 1)
+  ichild[f] = (nc - 1 - (L < level ? ch0[c] : 0)) - nch + 1;
+  iparent[f] = nc - 1 - (L > 0 ? par[c] : 0);
+  nchild[f] = nch;
+  ibody[f] = b;
+  nbody[f] = nb;
+  clevel[f] = L;
+  icell[f] = key[b] >> (3 * (level - L));
+  // centre and radius from the cell's first body at the level's cell size (:148-151,
+  // :182-185): d (ix + .5) + Xmin in double, stored in the working precision
+  float dl = uniform_d(box, level);
+  for (int k = L; k < level; k++) dl *= 2.f;
+  const vec4<T> x = bodies[b];
+  const T xs[3] = {x.x, x.y, x.z};
+  T X[3];
+  for (int k = 0; k < 3; k++) {
+    const int ik = uniform_ix(xs[k], box[4 + k], dl);
+    X[k] = (T)__dadd_rn(__dmul_rn((double)dl, (double)ik + 0.5), (double)box[4 + k]);
+  }
+  cX[f] = make_v4<T>(X[0], X[1], X[2], (T)__dmul_rn((double)dl, 0.5));
+  croot[f] = 0;
+}
+
+__global__ void k_iota(int n, int first, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = first + i;
+}
+
+// depth of the uniform tree for n bodies (include/build_tree_omp.h:218): host arithmetic,
+// the reference's own expression (integer n / ncrit, libm log)
+int uniform_level(int n, int ncrit) {
+  return n >= ncrit ? 1 + int(log((double)(n / ncrit)) / M_LN2 / 3) : 0;
+}
+
+template <typename T> static void build_uniform(Solver<T>& s) {
+  const int n = s.n, TB = 256;
+  const int level = uniform_level(n, s.cfg.ncrit);
+  if (level > kUniformMaxLevel)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED,
+                   "uniform tree deeper than 10 levels (the reference's 32-bit Morton keys "
+                   "overflow there)");
+  // getKey, radixSort (stable, on the key's 3 level bits), permute
+  s.keys.ensure(n);
+  s.keys2.ensure(n);
+  s.idx.ensure(n);
+  s.idx2.ensure(n);
+  k_ukeys<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(s.bodies_in.p, n, s.box.p, level, s.keys.p,
+                                                   s.idx.p);
+  FMM_LAUNCH_CHECK();
+  sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.idx2.p, n, std::max(3 * level, 1));
+  s.order.ensure(n);
+  FMM_CUDA(cudaMemcpyAsync(s.order.p, s.idx2.p, sizeof(int) * n, cudaMemcpyDeviceToDevice,
+                           s.stream));
+  s.bodies.ensure(n);
+  k_permute<T><<<ceil_div(n, TB), TB, 0, s.stream>>>(n, s.bodies_in.p, s.order.p, s.bodies.p);
+  FMM_LAUNCH_CHECK();
+  // cells in construction order, level by level from the leaves: first body (nbegin),
+  // first child (nfirst), parent (nparent); run heads and their scan in nsplit / coff.
+  // Level l holds at most min(n, 8^l) cells.
+  size_t cap = 16;
+  for (int L = 0; L <= level; L++) cap += std::min<size_t>((size_t)n, (size_t)1 << (3 * L));
+  s.nbegin.ensure(cap);
+  s.nfirst.ensure(cap);
+  s.nparent.ensure(cap);
+  s.nsplit.ensure((size_t)n + 1);
+  s.coff.ensure((size_t)n + 1);
+  UniformLevels lv{};
+  int cb = 0, m = n, ce = 0;  // the level below: construction range [cb, cb + m)
+  for (int L = level; L >= 0; L--) {
+    const bool leaves = L == level;
+    const int shift = 3 * (level - L);
+    k_uheads<<<ceil_div(m + 1, TB), TB, 0, s.stream>>>(m, cb, leaves ? nullptr : s.nbegin.p,
+                                                       s.keys2.p, shift, s.nsplit.p);
+    FMM_LAUNCH_CHECK();
+    exclusive_sum_int(s, s.nsplit.p, s.coff.p, m + 1);
+    FMM_CUDA(cudaMemcpyAsync(s.scal_host, s.coff.p + m, sizeof(int), cudaMemcpyDeviceToHost,
+                             s.stream));
+    k_uemit<<<ceil_div(m, TB), TB, 0, s.stream>>>(m, cb, ce, s.nsplit.p, s.coff.p, s.nbegin.p,
+                                                  s.nfirst.p, s.nparent.p, leaves);
+    FMM_LAUNCH_CHECK();
+    FMM_CUDA(cudaStreamSynchronize(s.stream));
+    const int cnt = s.scal_host[0];
+    lv.begin[L] = ce;
+    lv.end[L] = ce + cnt;
+    cb = ce;
+    m = cnt;
+    ce += cnt;
+  }
+  const int nc = ce;
+  // reverseOrder into the reference's cell layout
+  s.c_iparent.ensure(nc); s.c_ichild.ensure(nc); s.c_nchild.ensure(nc);
+  s.c_ibody.ensure(nc); s.c_nbody.ensure(nc); s.c_level.ensure(nc);
+  s.c_icell.ensure(nc);
+  s.cX.ensure(nc);
+  s.c_root.ensure(nc);
+  k_ucells<T><<<ceil_div(nc, TB), TB, 0, s.stream>>>(
+      nc, n, level, lv, s.box.p, s.nbegin.p, s.nfirst.p, s.nparent.p, s.keys2.p, s.bodies.p,
+      s.c_iparent.p, s.c_ichild.p, s.c_nchild.p, s.c_ibody.p, s.c_nbody.p, s.c_level.p,
+      s.c_icell.p, s.cX.p, s.c_root.p);
+  FMM_LAUNCH_CHECK();
+  s.c_info.ensure(nc);
+  k_cell_info<<<ceil_div(nc, TB), TB, 0, s.stream>>>(nc, s.c_nchild.p, s.c_ichild.p,
+                                                     s.c_nbody.p, s.c_info.p);
+  FMM_LAUNCH_CHECK();
+  // the level passes walk cells level by level: node v is cell v (npos the identity), the
+  // cells of level l at [nc - end[l], nc - begin[l]); every leaf is on the deepest level
+  s.npos.ensure(nc);
+  k_iota<<<ceil_div(nc, TB), TB, 0, s.stream>>>(nc, 0, s.npos.p);
+  FMM_LAUNCH_CHECK();
+  const int nleaves = lv.end[level] - lv.begin[level];
+  s.leaves.ensure(nleaves);
+  k_iota<<<ceil_div(nleaves, TB), TB, 0, s.stream>>>(nleaves, nc - nleaves, s.leaves.p);
+  FMM_LAUNCH_CHECK();
+  s.level_lo.clear();
+  for (int L = 0; L <= level; L++) s.level_lo.push_back(nc - lv.end[L]);
+  s.level_lo.push_back(nc);
+  s.cbase.ensure(2);
+  FMM_CUDA(cudaMemsetAsync(s.cbase.p, 0, sizeof(int), s.stream));
+  s.root_cell.assign(1, 0);
+  s.maxlevel = level;
+  s.ncells = nc;
+  s.nleaves = nleaves;
+  s.tree_plan = 0;
+}
+
 template <typename T> void build_tree(Solver<T>& s) {
   const int n = s.n;
   const int TB = 256;
+  s.kc_valid = false;  // the host copies of the cells' index fields are stale
   s.level_lo.clear();
   s.ncells = s.maxlevel = s.nleaves = 0;
   // roots: non-empty solves in order
@@ -617,6 +847,10 @@ template <typename T> void build_tree(Solver<T>& s) {
     }
   rfirst.push_back(n);
   const int nroots = (int)s.root_solve.size();
+  if (s.cfg.tree == FMM_TREE_UNIFORM && (nroots > 1 || s.ij))
+    throw FmmError(FMM_ERR_NOT_SUPPORTED,
+                   "the uniform tree builds one tree per call (no batches, no separate target "
+                   "and source trees)");
   s.nroots = nroots;
   s.box.ensure(16 * (size_t)std::max(nroots, 1));
   if (nroots == 0) {
@@ -654,6 +888,10 @@ template <typename T> void build_tree(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
   phase_end(s, FMM_PHASE_BOUNDS);
   phase_begin(s, FMM_PHASE_TREE);
+  if (s.cfg.tree == FMM_TREE_UNIFORM) {
+    build_uniform(s);
+    return;
+  }
   // keys and first sort (within each root's range)
   s.keys.ensure(n);
   s.keys2.ensure(n);

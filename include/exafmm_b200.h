@@ -7,7 +7,8 @@
  *
  * Reference interfaces each group replaces:
  *   fmm_b200_build_tree     BoundBox::getBounds (include/bound_box.h:76-88) +
- *                           BuildTree::buildTree (include/build_tree_tbb.h:365-374)
+ *                           BuildTree::buildTree (include/build_tree_tbb.h:365-374, or
+ *                           include/build_tree_omp.h:216-262 with FMM_TREE_UNIFORM)
  *   fmm_b200_upward_pass    UpDownPass::upwardPass (include/up_down_pass.h:119-132)
  *   fmm_b200_traverse       Traversal::dualTreeTraversal (include/traversal.h:240-264),
  *                           applying kernel::M2L / kernel::P2P (include/kernel.h:6-14)
@@ -66,7 +67,16 @@ typedef struct fmm_b200_config {
                     * cell pair visited once and applied both ways (open boundary, one tree);
                     * the device evaluates both ways from the target side, so the results are
                     * the reference's mutual ones to rounding */
+  int tree;        /* FMM_TREE_ADAPTIVE: BuildTree of include/build_tree_tbb.h (the -DTBB
+                    * build); FMM_TREE_UNIFORM: BuildTree of include/build_tree_omp.h (an
+                    * OpenMP build without TBB, include/build_tree.h:12-13), every leaf at depth
+                    * 1 + int(log(N / ncrit) / ln 2 / 3); one tree per call (batches and
+                    * separate target/source sets return FMM_ERR_NOT_SUPPORTED), depth <= 10 */
 } fmm_b200_config;
+
+/* tree builders (fmm_b200_config.tree) */
+#define FMM_TREE_ADAPTIVE 0
+#define FMM_TREE_UNIFORM 1
 
 typedef struct fmm_b200_solver fmm_b200_solver;
 
@@ -84,7 +94,7 @@ typedef struct fmm_b200_solver fmm_b200_solver;
 
 /* ---- lifecycle --------------------------------------------------------------------- */
 /* Defaults: spherical, P = 10, theta = 0.4, ncrit = 64, nspawn = 1000, use_rmax = 1,
- * use_ropt = 1, FP32, eps2 = 0, images = 0, device 0. */
+ * use_ropt = 1, FP32, eps2 = 0, images = 0, device 0, adaptive tree. */
 int fmm_b200_default_config(fmm_b200_config* cfg);
 int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out);
 int fmm_b200_destroy(fmm_b200_solver* s);
@@ -160,6 +170,51 @@ int fmm_b200_num_lists(fmm_b200_solver* s, long long* num_m2l, long long* num_p2
                        long long* p2p_body_pairs);
 int fmm_b200_get_lists(fmm_b200_solver* s, long long* m2l, long long* p2p);
 int fmm_b200_get_timings(fmm_b200_solver* s, double* ms); /* FMM_NUM_PHASES values */
+
+/* ---- single operators: namespace kernel (include/kernel.h:6-14) --------------------------
+ * The reference's kernel plugin interface, kernel::P2M / M2M / M2L / L2L / L2P / P2P, which
+ * examples/kernel.cxx:23-92, the up/down passes and the traversal call one cell (pair) at a
+ * time, as calls over lists of cells of a handle: the cells of its last tree build, or cells
+ * set up by hand with fmm_b200_kernel_set_cells over the bodies of fmm_b200_set_bodies_* in
+ * their given order.  Each call runs the handle's own kernels (its basis, order P and
+ * precision) and accumulates as the reference does: P2M / M2M add to the cells' M, M2L /
+ * L2L to their L, L2P / P2P to the bodies' targets (phi, grad phi per unit target charge;
+ * the reference's TRG carries the target charge until L2P divides by it).  Multipoles are
+ * unnormalised (the reference's non-MASS build).  Entries of one call run concurrently, so
+ * a call must not list a cell with its child (M2M) or parent (L2L), the same cell twice
+ * (P2M, M2M, L2L, L2P), or target cells whose bodies overlap (L2P, P2P); such lists and any
+ * index out of range return FMM_ERR_INVALID before the device is touched.  Pairs carry an
+ * optional image code per pair (NULL: no shift; the code of fmm_b200_get_lists, shift
+ * (ix, iy, iz) times the handle's period) and the mutual flag (each pair of two different
+ * cells also applied in reverse).  The calls leave the expansions readable
+ * (fmm_b200_get_expansion) and the handle's interaction lists stale. */
+/* Cells by hand: X (3 per cell) and R, the body range [ibody, ibody + nbody) of each cell,
+ * children [ichild, ichild + nchild) and parent iparent (include/types.h:79-94); M, L and
+ * the targets start at zero. */
+int fmm_b200_kernel_set_cells(fmm_b200_solver* s, int ncells, const double* X, const double* R,
+                              const int* ibody, const int* nbody, const int* ichild,
+                              const int* nchild, const int* iparent);
+/* which = 0: M, 1: L, in the fmm_b200_get_expansion layout; NULL sets zero */
+int fmm_b200_kernel_set_expansion(fmm_b200_solver* s, int which, const double* in);
+/* targets of the bodies in cell order (4 per body); NULL sets zero */
+int fmm_b200_kernel_set_trg(fmm_b200_solver* s, const double* trg);
+int fmm_b200_kernel_get_trg(fmm_b200_solver* s, double* trg);
+/* kernel::P2M(C) for each listed cell: M += sum of q Y(body - X) (LaplaceSphericalCPU.cxx:103-118) */
+int fmm_b200_kernel_p2m(fmm_b200_solver* s, int n, const int* cells);
+/* kernel::M2M(Ci, C0): M += the cell's children's multipoles shifted to its centre (:120-147) */
+int fmm_b200_kernel_m2m(fmm_b200_solver* s, int n, const int* cells);
+/* kernel::M2L(Ci, Cj, Xperiodic, mutual): L of ci[k] += M of cj[k] translated (:149-191) */
+int fmm_b200_kernel_m2l(fmm_b200_solver* s, int n, const int* ci, const int* cj,
+                        const int* image, int mutual);
+/* kernel::L2L(Ci, C0): L += the parent's local expansion shifted to the cell's centre (:193-224) */
+int fmm_b200_kernel_l2l(fmm_b200_solver* s, int n, const int* cells);
+/* kernel::L2P(Ci): the cell's bodies' targets += its local expansion evaluated (:226-256) */
+int fmm_b200_kernel_l2p(fmm_b200_solver* s, int n, const int* cells);
+/* kernel::P2P(Ci, Cj, eps2, Xperiodic, mutual) and the self form P2P(C, eps2) (ci[k] ==
+ * cj[k]): targets of ci[k]'s bodies += the field of cj[k]'s bodies, r^2 == 0 pairs skipped
+ * (kernels/LaplaceP2PCPU.cxx:4-331) */
+int fmm_b200_kernel_p2p(fmm_b200_solver* s, int n, const int* ci, const int* cj,
+                        const int* image, int mutual, double eps2);
 
 /* ---- separate target and source sets ----------------------------------------------------
  * Targets (nt, with charges qt that shape their own tree's radii) and sources (ns) in two

@@ -290,7 +290,10 @@ static void nodes2cells(Oracle* o, int v, int c, int CN, int level, int iparent)
   }
 }
 
-/* BuildTree::buildTree (include/build_tree_tbb.h:365-374) = growTree (:313) + linkTree (:347) */
+static int build_uniform(Oracle* o);
+
+/* BuildTree::buildTree (include/build_tree_tbb.h:365-374) = growTree (:313) + linkTree (:347);
+ * with tree = ORACLE_TREE_UNIFORM, BuildTree::buildTree of include/build_tree_omp.h:216-262 */
 int oracle_build_tree(void* h) {
   Oracle* o = (Oracle*)h;
   if (!o->box_fixed) make_box(o);
@@ -302,6 +305,7 @@ int oracle_build_tree(void* h) {
   o->cX = o->R = o->Rbuilt = o->M = o->L = NULL;
   o->nc = 0;
   if (o->n == 0) return 0;
+  if (o->p.tree == ORACLE_TREE_UNIFORM) return build_uniform(o);
   real* xb = (real*)malloc(sizeof(real) * 3 * o->n);
   real* qb = (real*)malloc(sizeof(real) * o->n);
   int* ib = (int*)malloc(sizeof(int) * o->n);
@@ -325,6 +329,166 @@ int oracle_build_tree(void* h) {
   o->L = (real*)calloc((size_t)na * o->ncoef, sizeof(real));
   nodes2cells(o, o->root, 0, 1, 0, 0);
   memcpy(o->Rbuilt, o->R, sizeof(real) * nc);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ uniform Morton tree */
+/* BuildTree of include/build_tree_omp.h:214-262, the builder an OpenMP build without TBB
+ * uses (include/build_tree.h:12-13): every leaf at depth
+ * level = 1 + int(log(N / ncrit) / ln 2 / 3) (integer N / ncrit, :218), or 0 for N < ncrit. */
+int oracle_uniform_level(int n, int ncrit) {
+  return n >= ncrit ? 1 + (int)(log((double)(n / ncrit)) / M_LN2 / 3) : 0;
+}
+
+/* the cell size of a level, as getKey / bodies2leafs declare it: `float d`, computed as
+ * 2 R / 2^level in real_t (:38, :135) */
+static float uniform_d(const Oracle* o, int level) { return (float)(2 * o->R0 / (1 << level)); }
+
+/* grid index of a position along one axis: (X - Xmin) / d truncated to int, with d a float
+ * promoted to real_t (:42-44) */
+static int uniform_ix(real x, real xmin, float d) { return (int)((x - xmin) / d); }
+
+typedef struct { unsigned long long key; int idx; } KeyIdx;
+static int cmp_keyidx(const void* a, const void* b) {
+  const KeyIdx *u = (const KeyIdx*)a, *v = (const KeyIdx*)b;
+  if (u->key != v->key) return u->key < v->key ? -1 : 1;
+  return u->idx < v->idx ? -1 : (u->idx > v->idx);
+}
+
+static int build_uniform(Oracle* o) {
+  const int n = o->n, level = oracle_uniform_level(n, o->p.ncrit);
+  /* the reference's `int id` holds bits up to 3 level - 1; above level 10 its shifts leave
+   * the int (:47-49), which neither this restatement nor the device reproduces */
+  if (level > 10) return 1;
+  real Xmin[3], Xmax[3];
+  for (int d = 0; d < 3; d++) Xmin[d] = Xmax[d] = o->x[d];
+  update_bounds(o, Xmin, Xmax);
+  /* getKey (:36-57) */
+  const float d = uniform_d(o, level);
+  KeyIdx* ki = (KeyIdx*)malloc(sizeof(KeyIdx) * n);
+  for (int b = 0; b < n; b++) {
+    int ix = uniform_ix(o->x[3 * b], Xmin[0], d), iy = uniform_ix(o->x[3 * b + 1], Xmin[1], d),
+        iz = uniform_ix(o->x[3 * b + 2], Xmin[2], d);
+    int id = 0;
+    for (int l = 0; l != level; ++l) {
+      id += (ix & 1) << (3 * l);
+      id += (iy & 1) << (3 * l + 1);
+      id += (iz & 1) << (3 * l + 2);
+      ix >>= 1;
+      iy >>= 1;
+      iz >>= 1;
+    }
+    ki[b].key = (unsigned long long)id;
+    ki[b].idx = b;
+  }
+  /* radixSort (:59-121) is an LSD sort, stable in the input order; permute (:123-128) */
+  qsort(ki, n, sizeof(KeyIdx), cmp_keyidx);
+  real* xb = (real*)malloc(sizeof(real) * 3 * n);
+  real* qb = (real*)malloc(sizeof(real) * n);
+  int* ib = (int*)malloc(sizeof(int) * n);
+  unsigned long long* key = (unsigned long long*)malloc(sizeof(unsigned long long) * n);
+  for (int b = 0; b < n; b++) {
+    const int s = ki[b].idx;
+    for (int k = 0; k < 3; k++) xb[3 * b + k] = o->x[3 * s + k];
+    qb[b] = o->q[s];
+    ib[b] = o->ibody[s];
+    key[b] = ki[b].key;
+  }
+  memcpy(o->x, xb, sizeof(real) * 3 * n);
+  memcpy(o->q, qb, sizeof(real) * n);
+  memcpy(o->ibody, ib, sizeof(int) * n);
+  free(xb); free(qb); free(ib); free(ki);
+  /* cells in construction order: bodies2leafs (:130-158) then leafs2cells (:160-198) */
+  int cap = n + 16, nc = 0;
+  int *fb = (int*)malloc(sizeof(int) * cap), *nb = (int*)malloc(sizeof(int) * cap);
+  int *ch0 = (int*)malloc(sizeof(int) * cap), *nch = (int*)malloc(sizeof(int) * cap);
+  int *par = (int*)malloc(sizeof(int) * cap), *lev = (int*)malloc(sizeof(int) * cap);
+  unsigned long long* ic = (unsigned long long*)malloc(sizeof(unsigned long long) * cap);
+  real* X = (real*)malloc(sizeof(real) * 3 * cap);
+  real* R = (real*)malloc(sizeof(real) * cap);
+  /* cell centre and radius at cell size dl from the cell's first body (:148-151, :182-185):
+   * d (ix + .5) + Xmin evaluated in double, stored in real_t */
+#define UNIFORM_CELL(c, b, dl)                                                         \
+  do {                                                                                 \
+    for (int k = 0; k < 3; k++) {                                                      \
+      int ik = uniform_ix(o->x[3 * (b) + k], Xmin[k], dl);                             \
+      X[3 * (c) + k] = (real)((double)(dl) * (ik + .5) + (double)Xmin[k]);             \
+    }                                                                                  \
+    R[c] = (real)((double)(dl) * .5);                                                  \
+  } while (0)
+  {
+    long long prev = -1;
+    for (int b = 0; b < n; b++) {
+      const int IC = (int)key[b];
+      if (IC != prev) {
+        fb[nc] = b; nb[nc] = 0; ch0[nc] = 0; nch[nc] = 0; lev[nc] = level; ic[nc] = IC;
+        UNIFORM_CELL(nc, b, d);
+        nc++;
+        prev = IC;
+      }
+      nb[nc - 1]++;
+    }
+  }
+  int begin = 0, end = nc;
+  float dl = d;
+  for (int l = 1; l <= level; l++) {
+    const int div = 1 << (3 * l);
+    dl *= 2;
+    long long prev = -1;
+    int p = end - 1;
+    for (int c = begin; c != end; c++) {
+      const int b = fb[c];
+      const int IC = (int)(key[b] / div);
+      if (IC != prev) {
+        fb[nc] = b; nb[nc] = 0; ch0[nc] = c; nch[nc] = 0; lev[nc] = level - l; ic[nc] = IC;
+        UNIFORM_CELL(nc, b, dl);
+        nc++;
+        p++;
+        prev = IC;
+      }
+      nch[p]++;
+      nb[p] += nb[c];
+      par[c] = p;
+    }
+    begin = end;
+    end = nc;
+  }
+#undef UNIFORM_CELL
+  par[nc - 1] = 0;
+  /* reverseOrder (:200-211): cell c goes to nc - 1 - c, ICHILD to the lowest index of its
+   * (now descending) children, leaves (ICHILD 0) to nc, the root's parent 0 to nc - 1 */
+  free_cells(o);
+  int na = nc + 27;  /* + the periodic cells of traversePeriodic, as the adaptive build */
+  o->iparent = (int*)calloc(na, sizeof(int));
+  o->ichild = (int*)calloc(na, sizeof(int));
+  o->nchild = (int*)calloc(na, sizeof(int));
+  o->cibody = (int*)calloc(na, sizeof(int));
+  o->cnbody = (int*)calloc(na, sizeof(int));
+  o->clevel = (int*)calloc(na, sizeof(int));
+  o->icell = (unsigned long long*)calloc(na, sizeof(unsigned long long));
+  o->cX = (real*)calloc(3 * na, sizeof(real));
+  o->R = (real*)calloc(na, sizeof(real));
+  o->Rbuilt = (real*)calloc(na, sizeof(real));
+  o->M = (real*)calloc((size_t)na * o->ncoef, sizeof(real));
+  o->L = (real*)calloc((size_t)na * o->ncoef, sizeof(real));
+  for (int c = 0; c < nc; c++) {
+    const int f = nc - 1 - c;
+    o->ichild[f] = (nc - 1 - ch0[c]) - nch[c] + 1;
+    o->iparent[f] = nc - 1 - par[c];
+    o->nchild[f] = nch[c];
+    o->cibody[f] = fb[c];
+    o->cnbody[f] = nb[c];
+    o->clevel[f] = lev[c];
+    o->icell[f] = ic[c];
+    for (int k = 0; k < 3; k++) o->cX[3 * f + k] = X[3 * c + k];
+    o->R[f] = R[c];
+  }
+  o->nc = nc;
+  o->maxlevel = level;
+  memcpy(o->Rbuilt, o->R, sizeof(real) * nc);
+  /* the root box the upward pass and the traversal never read; kept for get_box */
+  free(fb); free(nb); free(ch0); free(nch); free(par); free(lev); free(ic); free(X); free(R);
+  free(key);
   return 0;
 }
 
@@ -1337,7 +1501,7 @@ static Oracle* op_setup(int basis, int P, int nb, const double* xq) {
     for (int d = 0; d < 3; d++) x[3 * b + d] = xq[4 * b + d];
     q[b] = xq[4 * b + 3];
   }
-  oracle_params prm = {basis, P, 0.5, 16, 1000, 0, 0, 0, 0, 0.0};
+  oracle_params prm = {.basis = basis, .P = P, .theta = 0.5, .ncrit = 16, .nspawn = 1000};
   Oracle* o = (Oracle*)oracle_new(nb, x, q, &prm);
   if (nb) { free(x); free(q); }
   o->nc = 2;

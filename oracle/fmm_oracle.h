@@ -34,7 +34,11 @@ typedef struct oracle_params {
   double cycle;   /* period of the box (Traversal::dualTreeTraversal's cycle) */
   int mutual;     /* dualTreeTraversal's mutual flag (open boundary, one tree): each
                    * unordered cell pair visited once and applied both ways */
+  int tree;       /* ORACLE_TREE_ADAPTIVE: BuildTree of include/build_tree_tbb.h;
+                   * ORACLE_TREE_UNIFORM: BuildTree of include/build_tree_omp.h */
 } oracle_params;
+
+enum { ORACLE_TREE_ADAPTIVE = 0, ORACLE_TREE_UNIFORM = 1 };
 
 /* Pairs in the lists are packed (target << 32) | source | image << 27, image 0 for the
  * unshifted source and, for periodic runs, the shift (ix, iy, iz) in {-1, 0, 1}^3 coded
@@ -44,6 +48,8 @@ void* oracle_new(int n, const double* x, const double* q, const oracle_params* p
 void oracle_free(void* h);
 /* Stages as in examples/serial.cxx:46-60. Return 0 on success. */
 int oracle_build_tree(void* h);
+/* depth of the uniform tree for n bodies (include/build_tree_omp.h:218) */
+int oracle_uniform_level(int n, int ncrit);
 int oracle_upward(void* h);
 int oracle_traverse(void* h); /* also applies M2L/P2P as the traversal visits pairs */
 int oracle_downward(void* h);

@@ -16,6 +16,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SPHERICAL, CARTESIAN = 0, 1
+TREE_ADAPTIVE, TREE_UNIFORM = 0, 1
 
 
 class _Params(C.Structure):
@@ -23,7 +24,7 @@ class _Params(C.Structure):
                 ("ncrit", C.c_int), ("nspawn", C.c_int), ("use_rmax", C.c_int),
                 ("use_ropt", C.c_int), ("mass", C.c_int), ("kahan", C.c_int),
                 ("eps2", C.c_double), ("images", C.c_int), ("cycle", C.c_double),
-                ("mutual", C.c_int)]
+                ("mutual", C.c_int), ("tree", C.c_int)]
 
 
 def _ptr(a):
@@ -108,6 +109,8 @@ class Oracle:
         L = self.lib
         L.oracle_new.restype = C.c_void_p
         L.oracle_new.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(_Params)]
+        L.oracle_uniform_level.restype = C.c_int
+        L.oracle_uniform_level.argtypes = [C.c_int, C.c_int]
         for f in ("build_tree", "upward", "traverse", "downward", "solve"):
             getattr(L, "oracle_" + f).restype = C.c_int
             getattr(L, "oracle_" + f).argtypes = [C.c_void_p]
@@ -135,12 +138,12 @@ class Oracle:
 
     def run(self, x, q, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
             use_ropt=0, mass=0, kahan=0, eps2=0.0, stages=15, images=0, cycle=2 * np.pi,
-            mutual=0):
+            mutual=0, tree=TREE_ADAPTIVE):
         x = np.ascontiguousarray(x, np.float64)
         q = np.ascontiguousarray(q, np.float64)
         n = len(q)
         prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2,
-                      images, cycle, mutual)
+                      images, cycle, mutual, tree)
         h = self.lib.oracle_new(n, _ptr(x), _ptr(q), C.byref(prm))
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
         run = OracleRun(self.lib, "oracle_", h, n, nterm, basis == SPHERICAL)
@@ -168,7 +171,7 @@ class Oracle:
         xs = np.ascontiguousarray(xs, np.float64)
         qs = np.ascontiguousarray(qs, np.float64)
         prm = _Params(basis, P, theta, ncrit, nspawn, use_rmax, use_ropt, mass, kahan, eps2, 0,
-                      2 * np.pi, 0)
+                      2 * np.pi, 0, TREE_ADAPTIVE)
         hi = self.lib.oracle_new(len(qt), _ptr(xt), _ptr(qt), C.byref(prm))
         hj = self.lib.oracle_new(len(qs), _ptr(xs), _ptr(qs), C.byref(prm))
         nterm = P * (P + 1) // 2 if basis == SPHERICAL else P * (P + 1) * (P + 2) // 6
@@ -189,6 +192,10 @@ class Oracle:
 
     def kernel_chain(self, basis, P, mass=0, seed=-1):
         return self.lib.oracle_kernel_chain(basis, P, mass, seed)
+
+    def uniform_level(self, n, ncrit):
+        """Depth of the uniform Morton tree (include/build_tree_omp.h:218)."""
+        return self.lib.oracle_uniform_level(n, ncrit)
 
 
 class OracleRun(_Run):
@@ -242,7 +249,7 @@ class Reference:
             lib.ref_run.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
-            for f in ("P", "nterm", "fp64", "spherical", "mass", "kahan"):
+            for f in ("P", "nterm", "fp64", "spherical", "mass", "kahan", "uniform"):
                 getattr(lib, "ref_" + f).restype = C.c_int
                 getattr(lib, "ref_" + f).argtypes = []
             lib.ref_run_ij.restype = C.c_void_p
@@ -262,6 +269,7 @@ class Reference:
         self.P, self.nterm = L.ref_P(), L.ref_nterm()
         self.fp64, self.spherical = bool(L.ref_fp64()), bool(L.ref_spherical())
         self.mass, self.kahan = bool(L.ref_mass()), bool(L.ref_kahan())
+        self.uniform = bool(L.ref_uniform())
 
     def run(self, x, q, ncrit=64, nspawn=1000, theta=0.4, use_rmax=1, use_ropt=0, eps2=0.0,
             stages=15, record=True, threads=0, images=0, cycle=2 * np.pi, mutual=0):

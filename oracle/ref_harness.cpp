@@ -5,7 +5,9 @@
 // product links or calls it.
 //
 // Pipeline driven exactly as examples/serial.cxx:41-60 drives it:
-//   BoundBox::getBounds -> BuildTree::buildTree (adaptive, include/build_tree_tbb.h)
+//   BoundBox::getBounds -> BuildTree::buildTree (adaptive, include/build_tree_tbb.h; with
+//   -DREF_UNIFORM the uniform Morton tree of include/build_tree_omp.h, which an OpenMP build
+//   without TBB selects, include/build_tree.h:12-13)
 //   -> UpDownPass::upwardPass -> Traversal::dualTreeTraversal(cells, cells, cycle, mutual)
 //   -> UpDownPass::downwardPass
 // with the bodies injected from the caller instead of include/dataset.h.
@@ -13,7 +15,11 @@
 // Interaction lists are recorded by linking ref_record.cpp in place of namespace
 // kernel (the reference kernels are compiled with -Dkernel=refkernel and forwarded to).
 #include "bound_box.h"
+#ifdef REF_UNIFORM
+#include "build_tree_omp.h"
+#else
 #include "build_tree_tbb.h"
+#endif
 #include "traversal.h"
 #include "up_down_pass.h"
 #include <omp.h>
@@ -51,6 +57,13 @@ int ref_spherical() {
 }
 int ref_mass() {
 #if MASS
+  return 1;
+#else
+  return 0;
+#endif
+}
+int ref_uniform() {
+#ifdef REF_UNIFORM
   return 1;
 #else
   return 0;
@@ -227,7 +240,11 @@ void ref_get_cells(void* h, int* iparent, int* ichild, int* nchild, int* ibody, 
     iparent[c] = C.IPARENT;
     ichild[c] = C.ICHILD;
     nchild[c] = C.NCHILD;
+#ifdef REF_UNIFORM
+    ibody[c] = (int)(C.BODY - run->bodies.begin());  // the uniform build sets BODY only
+#else
     ibody[c] = C.IBODY;
+#endif
     nbody[c] = C.NBODY;
     icell[c] = C.ICELL;
     level[c] = run->level[c];

@@ -1,0 +1,137 @@
+"""The uniform Morton tree (BuildTree of include/build_tree_omp.h, fmm_b200_config.tree =
+FMM_TREE_UNIFORM) on the GPU against the oracle's restatement of it, which
+tests/test_oracle.py pins bit for bit against the reference compiled with that builder.
+
+Bar: cells (IPARENT, ICHILD, NCHILD, IBODY, NBODY, level, ICELL, X, R) and the body order
+bit-exact, including the reference's layout quirks (root IPARENT = ncells - 1, leaf
+ICHILD = ncells); interaction lists bit-exact (use_ropt = 0); potentials and gradients FP64
+within 1e-10 and FP32 within 2e-5 rel-L2 of the oracle on the same tree.  Where the
+reference build is present (oracle/_ref), the GPU cells and lists are also compared with it
+directly.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import (CARTESIAN, SPHERICAL, TREE_UNIFORM, Oracle, Reference, have_reference,
+                    rel_l2)
+
+pytestmark = pytest.mark.gpu
+fmm = importlib.import_module("exafmm-dev_b200")
+
+CASES = {
+    # name: (basis, P, precision, distribution, N, parameters); depths 3, 4, 4, 1, 0, 4
+    "sph6_f64_cube": ("spherical", 6, "f64", "cube", 16384, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    "sph8_f32_plummer": ("spherical", 8, "f32", "plummer", 20000,
+                         dict(ncrit=32, theta=0.4, use_ropt=0)),
+    "cart4_f64_sphere": ("cartesian", 4, "f64", "sphere", 12000,
+                         dict(ncrit=16, theta=0.5, use_ropt=0)),
+    "sph6_f64_level1": ("spherical", 6, "f64", "cube", 100, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    "sph6_f64_level0": ("spherical", 6, "f64", "plummer", 30, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    "sph10_f32_plummer_ropt": ("spherical", 10, "f32", "plummer", 40000,
+                               dict(ncrit=64, theta=0.35, use_ropt=1)),
+}
+REFERENCE = {"sph6_f64_cube": "uni_sph_p6_f64", "cart4_f64_sphere": "uni_cart_p4_f64",
+             "sph8_f32_plummer": "uni_sph_p8_f32k"}
+CELL_KEYS = ("iparent", "ichild", "nchild", "ibody", "nbody", "level", "icell", "X")
+
+_cache = {}
+
+
+def oracle_run(name, datasets):
+    if name not in _cache:
+        basis, P, prec, dist, n, kw = CASES[name]
+        x, q = datasets.make(dist, n, seed=17, precision=prec)
+        o = Oracle(prec).run(x, q, basis=SPHERICAL if basis == "spherical" else CARTESIAN, P=P,
+                             kahan=int(prec == "f32"), tree=TREE_UNIFORM, **kw)
+        _cache[name] = (x, q, o)
+    return _cache[name]
+
+
+def solver(name):
+    basis, P, prec, dist, n, kw = CASES[name]
+    return fmm.Solver(basis=basis, P=P, precision=prec, tree="uniform", **kw)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_cells_and_order_bit_exact(name, datasets):
+    x, q, o = oracle_run(name, datasets)
+    s = solver(name)
+    s.set_bodies(x, q)
+    s.build_tree()
+    g, r = s.cells(), o.cells()
+    nc = len(r["nbody"])
+    assert s.num_cells() == (nc, o.maxlevel)
+    assert np.array_equal(s.box(), o.box())
+    for k in CELL_KEYS:
+        assert np.array_equal(g[k], r[k]), k
+    assert np.array_equal(g["R"], r["R_built"])
+    assert np.array_equal(s.order(), o.order())
+    # the reference's layout: root first with IPARENT = ncells - 1, leaves (all on the
+    # deepest level, in descending key order) with ICHILD = ncells
+    assert g["iparent"][0] == nc - 1
+    leaves = g["nchild"] == 0
+    assert (g["ichild"][leaves] == nc).all() and (g["level"][leaves] == o.maxlevel).all()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_lists_and_solve(name, datasets):
+    x, q, o = oracle_run(name, datasets)
+    basis, P, prec, dist, n, kw = CASES[name]
+    s = solver(name)
+    trg = s.solve(x, q)
+    m2l, p2p = s.lists()
+    om2l, op2p = np.sort(o.m2l()), np.sort(o.p2p())
+    if kw["use_ropt"] == 0:
+        assert np.array_equal(m2l, om2l)
+        assert np.array_equal(p2p, op2p)
+    else:  # error-optimised radii through the GPU's powf: a few borderline pairs may flip
+        diff = len(np.setxor1d(m2l, om2l)) + len(np.setxor1d(p2p, op2p))
+        assert diff <= max(2, 1e-4 * (len(om2l) + len(op2p))), diff
+    pot, acc = rel_l2(trg, o.trg())
+    tol = 2e-5 if prec == "f32" else 1e-10
+    assert pot < tol and acc < tol, (pot, acc)
+
+
+@pytest.mark.parametrize("name", sorted(REFERENCE))
+def test_matches_reference_build(name, datasets):
+    cfg = REFERENCE[name]
+    if not have_reference(cfg):
+        pytest.skip("reference build oracle/_ref/parity/ref_%s.so absent" % cfg)
+    x, q, _ = oracle_run(name, datasets)
+    kw = CASES[name][5]
+    r = Reference(cfg).run(x, q, **kw)
+    s = solver(name)
+    s.set_bodies(x, q)
+    s.build_tree()
+    g, rc = s.cells(), r.cells()
+    for k in CELL_KEYS:
+        assert np.array_equal(g[k], rc[k]), k
+    assert np.array_equal(s.order(), r.order())
+    s.upward_pass()
+    s.traverse()
+    m2l, p2p = s.lists()
+    assert np.array_equal(m2l, np.sort(r.m2l()))
+    assert np.array_equal(p2p, np.sort(r.p2p()))
+
+
+def test_full_size_cube_1m(datasets):
+    """N = 2^20 bodies in the cube (P = 10, theta = 0.35, FP32) on the uniform tree: depth 5,
+    32,768 leaves of ~32 bodies; within 1e-4 of FP64 direct and deterministic."""
+    x, q = datasets.make("cube", 1 << 20, seed=43, precision="f32")
+    s = fmm.Solver(P=10, theta=0.35, ncrit=64, use_ropt=0, tree="uniform")
+    a = s.solve(x, q)
+    assert s.num_cells()[1] == 5
+    idx = datasets.sample_targets(len(q), 512)
+    pot, acc = rel_l2(a[idx], fmm.direct(x[idx], x, q))
+    assert pot < 1e-4 and acc < 1e-4, (pot, acc)
+    assert np.array_equal(a, s.solve(x, q))
+
+
+def test_batches_are_not_supported(datasets):
+    x, q = datasets.make("cube", 1000, seed=1, precision="f32")
+    s = fmm.Solver(P=6, tree="uniform")
+    with pytest.raises(fmm.FmmError) as e:
+        s.solve_batch([x, x], [q, q])
+    assert e.value.code == fmm.FMM_ERR_NOT_SUPPORTED

@@ -11,7 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from oracle import CARTESIAN, SPHERICAL, Oracle, Reference, have_reference, rel_l2
+from oracle import (CARTESIAN, SPHERICAL, TREE_ADAPTIVE, TREE_UNIFORM, Oracle, Reference,
+                    have_reference, rel_l2)
 
 CELL_KEYS = ("iparent", "ichild", "nchild", "ibody", "nbody", "level", "X", "R_built", "R")
 
@@ -103,13 +104,20 @@ def test_empty_and_single_body():
     ("sph_p8_f32k_mass", "f32", "plummer", 30000, dict(ncrit=64, theta=0.4, use_ropt=1)),
     ("cart_p5_f32", "f32", "sphere", 30000, dict(ncrit=32, theta=0.5, use_ropt=0)),
     ("cart_p4_f64", "f64", "cube", 10000, dict(ncrit=16, theta=0.6, use_ropt=0)),
+    # the uniform Morton tree (include/build_tree_omp.h): depths 3, 4, 4, 1 and 0
+    ("uni_sph_p6_f64", "f64", "cube", 16384, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    ("uni_sph_p8_f32k", "f32", "plummer", 20000, dict(ncrit=32, theta=0.4, use_ropt=0)),
+    ("uni_cart_p4_f64", "f64", "sphere", 12000, dict(ncrit=16, theta=0.5, use_ropt=0)),
+    ("uni_sph_p6_f64", "f64", "cube", 100, dict(ncrit=64, theta=0.4, use_ropt=0)),
+    ("uni_sph_p6_f64", "f64", "plummer", 30, dict(ncrit=64, theta=0.4, use_ropt=0)),
 ])
 def test_oracle_matches_reference(cfg, prec, dist, n, kw, datasets):
     R = Reference(cfg)
     x, q = datasets.make(dist, n, seed=7, precision=prec)
     r = R.run(x, q, **kw)
     o = Oracle(prec).run(x, q, basis=SPHERICAL if R.spherical else CARTESIAN, P=R.P,
-                         mass=int(R.mass), kahan=int(R.kahan), **kw)
+                         mass=int(R.mass), kahan=int(R.kahan),
+                         tree=TREE_UNIFORM if R.uniform else TREE_ADAPTIVE, **kw)
     rc, oc = r.cells(), o.cells()
     for k in CELL_KEYS:
         assert np.array_equal(rc[k], oc[k]), k
@@ -139,6 +147,16 @@ def test_oracle_matches_reference_periodic(cfg, prec, images, datasets):
     pot, acc = rel_l2(o.trg(), r.trg())
     tol = 2e-6 if prec == "f32" else 5e-7
     assert pot < tol and acc < tol, (pot, acc)
+
+
+def test_uniform_level_rule():
+    """include/build_tree_omp.h:218: 1 + int(log(N / ncrit) / ln 2 / 3) with integer N / ncrit,
+    0 below ncrit; exact powers of 8 of N / ncrit start a new level."""
+    o = Oracle("f64")
+    assert o.uniform_level(30, 64) == 0 and o.uniform_level(64, 64) == 1
+    assert o.uniform_level(64 * 8 - 1, 64) == 1 and o.uniform_level(64 * 8, 64) == 2
+    assert o.uniform_level(16384, 64) == 3 and o.uniform_level(1 << 20, 64) == 5
+    assert o.uniform_level(64 * 4096, 64) == 5 and o.uniform_level(64 * 4095, 64) == 4
 
 
 def test_periodic_direct_sum():

@@ -411,6 +411,68 @@ class Solver:
             return (a[:, 0] + 1j * a[:, 1]).reshape(nc, self.nterm)
         return a.reshape(nc, self.nterm)
 
+    # ---- single operators (namespace kernel, include/kernel.h:6-14) -----------------------
+    def kernel_set_cells(self, X, R, ibody, nbody, ichild, nchild, iparent):
+        """Cells by hand over the bodies of set_bodies (in their given order)."""
+        X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+        arr = [np.ascontiguousarray(a, np.int32) for a in (ibody, nbody, ichild, nchild, iparent)]
+        R = np.ascontiguousarray(R, np.float64)
+        self._check(self.lib.fmm_b200_kernel_set_cells(self.h, len(X), _p(X), _p(R),
+                                                       *[_p(a) for a in arr]))
+
+    def kernel_set_expansion(self, which, values):
+        """which 0: M, 1: L; values in the layout expansion() returns (None: zero)."""
+        if values is None:
+            self._check(self.lib.fmm_b200_kernel_set_expansion(self.h, which, None))
+            return
+        v = np.asarray(values)
+        if self.spherical:
+            v = np.stack([v.real, v.imag], axis=-1)
+        v = np.ascontiguousarray(v, np.float64)
+        self._check(self.lib.fmm_b200_kernel_set_expansion(self.h, which, _p(v)))
+
+    def kernel_set_trg(self, trg=None):
+        t = None if trg is None else np.ascontiguousarray(trg, np.float64)
+        self._check(self.lib.fmm_b200_kernel_set_trg(self.h, None if t is None else _p(t)))
+
+    def kernel_trg(self):
+        """(n, 4) targets of the bodies in cell order."""
+        t = np.zeros((self.n, 4))
+        self._check(self.lib.fmm_b200_kernel_get_trg(self.h, _p(t)))
+        return t
+
+    def _cells(self, name, cells):
+        c = np.ascontiguousarray(cells, np.int32)
+        self._check(getattr(self.lib, "fmm_b200_kernel_" + name)(self.h, len(c), _p(c)))
+
+    def kernel_p2m(self, cells):
+        self._cells("p2m", cells)
+
+    def kernel_m2m(self, cells):
+        self._cells("m2m", cells)
+
+    def kernel_l2l(self, cells):
+        self._cells("l2l", cells)
+
+    def kernel_l2p(self, cells):
+        self._cells("l2p", cells)
+
+    def _pairs(self, ci, cj, image):
+        ci = np.ascontiguousarray(ci, np.int32)
+        cj = np.ascontiguousarray(cj, np.int32)
+        im = None if image is None else np.ascontiguousarray(image, np.int32)
+        return ci, cj, im
+
+    def kernel_m2l(self, ci, cj, image=None, mutual=0):
+        ci, cj, im = self._pairs(ci, cj, image)
+        self._check(self.lib.fmm_b200_kernel_m2l(self.h, len(ci), _p(ci), _p(cj),
+                                                 None if im is None else _p(im), mutual))
+
+    def kernel_p2p(self, ci, cj, image=None, mutual=0, eps2=0.0):
+        ci, cj, im = self._pairs(ci, cj, image)
+        self._check(self.lib.fmm_b200_kernel_p2p(self.h, len(ci), _p(ci), _p(cj),
+                                                 None if im is None else _p(im), mutual, eps2))
+
     def list_counts(self):
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         self._check(self.lib.fmm_b200_num_lists(self.h, C.byref(a), C.byref(b), C.byref(c)))

@@ -20,6 +20,7 @@
 // target side on the device).  Traversal::direct runs the FP64 direct sum on the GPU (one
 // call per periodic shift).
 #pragma once
+#include <algorithm>
 #include <complex>
 #include <cstdint>
 #include <memory>
@@ -83,6 +84,7 @@ class Error : public std::runtime_error {
 struct Context {
   fmm_b200_config cfg;
   std::shared_ptr<fmm_b200_solver> solver;
+  std::shared_ptr<fmm_b200_solver> ksolver;  // the handle of the namespace kernel calls
   Bodies* bodies = nullptr;
   Context() { fmm_b200_default_config(&cfg); }
   static Context& global() {
@@ -103,6 +105,15 @@ struct Context {
     return solver.get();
   }
   void reset() { solver.reset(); }
+  fmm_b200_solver* kget() {
+    if (!ksolver) {
+      fmm_b200_solver* s = nullptr;
+      int rc = fmm_b200_create(&cfg, &s);
+      if (rc != FMM_OK) throw Error(rc, fmm_b200_last_error(nullptr));
+      ksolver.reset(s, [](fmm_b200_solver* p) { fmm_b200_destroy(p); });
+    }
+    return ksolver.get();
+  }
 };
 
 inline int nterm(const fmm_b200_config& c) {
@@ -303,6 +314,185 @@ class Traversal {
  private:
   Context& ctx_;
 };
+
+// namespace kernel (include/kernel.h:6-14): the translation operators one cell (pair) at
+// a time, with the reference's signatures and semantics.  Each call moves the cells and
+// bodies it touches to the device, runs the library's kernel for the Context's basis, order
+// and precision (fmm_b200_kernel_*), and writes the results back into the host Cells and
+// Bodies: M (P2M, M2M) and L (M2L, L2L) accumulate; TRG accumulates as the reference's does,
+// times the target charge in P2P (LaplaceP2PCPU.cxx:151), divided by it at the start of L2P
+// (LaplaceSphericalCPU.cxx:235).  Multipoles are the unnormalised ones of the reference's
+// non-MASS build.  A periodic shift Xperiodic must be (ix, iy, iz) cycle with |i| <= 1, as the
+// traversal forms it.  For many cells at once use the list form, fmm_b200_kernel_*.
+namespace kernel {
+namespace detail {
+
+inline int nt(Context& ctx) { return nterm(ctx.cfg); }
+inline int width(Context& ctx) { return ctx.cfg.basis == FMM_SPHERICAL ? 2 : 1; }
+
+// cells uploaded for one call: bodies (x, q), cell records, M and L rows
+struct Batch {
+  Context& ctx;
+  std::vector<double> x, q, X, R, M, L;
+  std::vector<int> ibody, nbody, ichild, nchild, iparent;
+  explicit Batch(Context& c) : ctx(c) {}
+  int add_bodies(B_iter B, int n) {
+    const int first = (int)q.size();
+    for (int i = 0; i < n; i++, ++B) {
+      for (int d = 0; d < 3; d++) x.push_back(B->X[d]);
+      q.push_back(B->SRC);
+    }
+    return first;
+  }
+  void put(std::vector<double>& dst, const std::vector<complex_t>& e) {
+    for (int t = 0; t < nt(ctx); t++) {
+      const complex_t v = t < (int)e.size() ? e[t] : complex_t(0, 0);
+      dst.push_back(v.real());
+      if (width(ctx) == 2) dst.push_back(v.imag());
+    }
+  }
+  int add_cell(const Cell& C, int ib, int nb, int ic = 0, int nc = 0, int ip = 0) {
+    for (int d = 0; d < 3; d++) X.push_back(C.X[d]);
+    R.push_back(C.R);
+    ibody.push_back(ib);
+    nbody.push_back(nb);
+    ichild.push_back(ic);
+    nchild.push_back(nc);
+    iparent.push_back(ip);
+    put(M, C.M);
+    put(L, C.L);
+    return (int)R.size() - 1;
+  }
+  fmm_b200_solver* upload() {
+    fmm_b200_solver* h = ctx.kget();
+    ctx.check(fmm_b200_set_bodies_host(h, (int)q.size(), x.data(), q.data()));
+    ctx.check(fmm_b200_kernel_set_cells(h, (int)R.size(), X.data(), R.data(), ibody.data(),
+                                        nbody.data(), ichild.data(), nchild.data(),
+                                        iparent.data()));
+    ctx.check(fmm_b200_kernel_set_expansion(h, 0, M.data()));
+    ctx.check(fmm_b200_kernel_set_expansion(h, 1, L.data()));
+    return h;
+  }
+  void fetch(int which, int cell, std::vector<complex_t>& out) {
+    std::vector<double> e(M.size());
+    ctx.check(fmm_b200_get_expansion(ctx.kget(), which, e.data()));
+    const int w = width(ctx), n = nt(ctx);
+    out.resize(n);
+    for (int t = 0; t < n; t++) {
+      const size_t k = ((size_t)cell * n + t) * w;
+      out[t] = w == 2 ? complex_t(e[k], e[k + 1]) : complex_t(e[k], 0);
+    }
+  }
+  std::vector<double> trg() {
+    std::vector<double> t(4 * q.size());
+    if (!q.empty()) ctx.check(fmm_b200_kernel_get_trg(ctx.kget(), t.data()));
+    return t;
+  }
+};
+
+// image code of a shift (ix, iy, iz) cycle, |i| <= 1 (the code of fmm_b200_get_lists), with
+// the handle's period set to that cycle
+inline int image_code(Context& ctx, const vec3& Xp) {
+  double c = 0;
+  for (int d = 0; d < 3; d++) c = std::max(c, Xp[d] < 0 ? -Xp[d] : Xp[d]);
+  if (c == 0) return 0;
+  int code = 0;
+  for (int d = 0; d < 3; d++) {
+    const int i = Xp[d] == 0 ? 0 : (Xp[d] == c ? 1 : (Xp[d] == -c ? 2 : -1));
+    if (i < 0) throw Error(FMM_ERR_NOT_SUPPORTED, "Xperiodic must be (ix, iy, iz) * cycle");
+    code = 3 * code + i;
+  }
+  ctx.check(fmm_b200_set_periodic(ctx.kget(), 1, c));
+  return code;
+}
+
+}  // namespace detail
+
+inline void P2M(C_iter C, Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*C, b.add_bodies(C->BODY, C->NBODY), C->NBODY);
+  const int c0 = 0;
+  ctx.check(fmm_b200_kernel_p2m(b.upload(), 1, &c0));
+  b.fetch(0, 0, C->M);
+}
+
+inline void M2M(C_iter Ci, C_iter C0, Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*Ci, 0, 0, 1, Ci->NCHILD);
+  for (int k = 0; k < Ci->NCHILD; k++) b.add_cell(*(C0 + Ci->ICHILD + k), 0, 0);
+  const int c0 = 0;
+  ctx.check(fmm_b200_kernel_m2m(b.upload(), 1, &c0));
+  b.fetch(0, 0, Ci->M);
+}
+
+inline void M2L(C_iter Ci, C_iter Cj, vec3 Xperiodic, bool mutual,
+                Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*Ci, 0, 0);
+  b.add_cell(*Cj, 0, 0);
+  const int i = 0, j = 1, img = detail::image_code(ctx, Xperiodic);
+  fmm_b200_solver* h = b.upload();
+  ctx.check(fmm_b200_kernel_m2l(h, 1, &i, &j, &img, mutual ? 1 : 0));
+  b.fetch(1, 0, Ci->L);
+  if (mutual) b.fetch(1, 1, Cj->L);
+}
+
+inline void L2L(C_iter Ci, C_iter C0, Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*Ci, 0, 0, 0, 0, 1);
+  b.add_cell(*(C0 + Ci->IPARENT), 0, 0);
+  const int c0 = 0;
+  ctx.check(fmm_b200_kernel_l2l(b.upload(), 1, &c0));
+  b.fetch(1, 0, Ci->L);
+}
+
+inline void L2P(C_iter Ci, Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*Ci, b.add_bodies(Ci->BODY, Ci->NBODY), Ci->NBODY);
+  fmm_b200_solver* h = b.upload();
+  std::vector<double> t(4 * (size_t)Ci->NBODY);
+  B_iter B = Ci->BODY;
+  for (int k = 0; k < Ci->NBODY; k++, ++B)
+    for (int d = 0; d < 4; d++) t[4 * k + d] = B->TRG[d] / B->SRC;  // TRG /= SRC first
+  ctx.check(fmm_b200_kernel_set_trg(h, t.data()));
+  const int c0 = 0;
+  ctx.check(fmm_b200_kernel_l2p(h, 1, &c0));
+  t = b.trg();
+  B = Ci->BODY;
+  for (int k = 0; k < Ci->NBODY; k++, ++B)
+    for (int d = 0; d < 4; d++) B->TRG[d] = t[4 * k + d];
+}
+
+inline void P2P(C_iter Ci, C_iter Cj, real_t eps2, vec3 Xperiodic, bool mutual,
+                Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*Ci, b.add_bodies(Ci->BODY, Ci->NBODY), Ci->NBODY);
+  b.add_cell(*Cj, b.add_bodies(Cj->BODY, Cj->NBODY), Cj->NBODY);
+  const int i = 0, j = 1, img = detail::image_code(ctx, Xperiodic);
+  ctx.check(fmm_b200_kernel_p2p(b.upload(), 1, &i, &j, &img, mutual ? 1 : 0, (double)eps2));
+  const std::vector<double> t = b.trg();
+  B_iter B = Ci->BODY;
+  for (int k = 0; k < Ci->NBODY; k++, ++B)
+    for (int d = 0; d < 4; d++) B->TRG[d] += B->SRC * t[4 * k + d];
+  if (mutual) {
+    B = Cj->BODY;
+    for (int k = 0; k < Cj->NBODY; k++, ++B)
+      for (int d = 0; d < 4; d++) B->TRG[d] += B->SRC * t[4 * (Ci->NBODY + k) + d];
+  }
+}
+
+inline void P2P(C_iter C, real_t eps2, Context& ctx = Context::global()) {
+  detail::Batch b(ctx);
+  b.add_cell(*C, b.add_bodies(C->BODY, C->NBODY), C->NBODY);
+  const int c0 = 0;
+  ctx.check(fmm_b200_kernel_p2p(b.upload(), 1, &c0, &c0, nullptr, 0, (double)eps2));
+  const std::vector<double> t = b.trg();
+  B_iter B = C->BODY;
+  for (int k = 0; k < C->NBODY; k++, ++B)
+    for (int d = 0; d < 4; d++) B->TRG[d] += B->SRC * t[4 * k + d];
+}
+
+}  // namespace kernel
 
 // Verify (include/verify.h:18-83)
 struct Verify {

@@ -134,6 +134,15 @@ class Oracle:
         L.oracle_kernel_chain.restype = C.c_double
         L.oracle_kernel_chain.argtypes = [C.c_int, C.c_int, C.c_int, C.c_long]
         L.oracle_real_bytes.restype = C.c_int
+        for f in ("m2l", "m2m", "l2l"):
+            getattr(L, "oracle_op_" + f).restype = None
+            getattr(L, "oracle_op_" + f).argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.oracle_op_p2m.restype = None
+        L.oracle_op_p2m.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_void_p]
+        L.oracle_op_l2p.restype = None
+        L.oracle_op_l2p.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_void_p]
         self.precision = precision
 
     def run(self, x, q, basis=SPHERICAL, P=6, theta=0.4, ncrit=64, nspawn=1000, use_rmax=1,
@@ -192,6 +201,44 @@ class Oracle:
 
     def kernel_chain(self, basis, P, mass=0, seed=-1):
         return self.lib.oracle_kernel_chain(basis, P, mass, seed)
+
+    # single operators (kernel::M2L / M2M / L2L / P2M / L2P on hand-made cells, unnormalised
+    # multipoles); expansions as flat doubles (spherical: re, im per coefficient)
+    def op_m2l(self, basis, P, Xi, Xj, Mj, Li):
+        Li = np.array(Li, np.float64)
+        self.lib.oracle_op_m2l(basis, P, _ptr(np.asarray(Xi, np.float64)),
+                               _ptr(np.asarray(Xj, np.float64)),
+                               _ptr(np.ascontiguousarray(Mj, np.float64)), _ptr(Li))
+        return Li
+
+    def op_m2m(self, basis, P, Xp, Xc, Mc, Mp):
+        Mp = np.array(Mp, np.float64)
+        self.lib.oracle_op_m2m(basis, P, _ptr(np.asarray(Xp, np.float64)),
+                               _ptr(np.asarray(Xc, np.float64)),
+                               _ptr(np.ascontiguousarray(Mc, np.float64)), _ptr(Mp))
+        return Mp
+
+    def op_l2l(self, basis, P, Xc, Xp, Lp, Lc):
+        Lc = np.array(Lc, np.float64)
+        self.lib.oracle_op_l2l(basis, P, _ptr(np.asarray(Xc, np.float64)),
+                               _ptr(np.asarray(Xp, np.float64)),
+                               _ptr(np.ascontiguousarray(Lp, np.float64)), _ptr(Lc))
+        return Lc
+
+    def op_p2m(self, basis, P, Xc, xq, M):
+        M = np.array(M, np.float64)
+        xq = np.ascontiguousarray(xq, np.float64)
+        self.lib.oracle_op_p2m(basis, P, _ptr(np.asarray(Xc, np.float64)), len(xq), _ptr(xq),
+                               _ptr(M))
+        return M
+
+    def op_l2p(self, basis, P, Xc, L, x):
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.zeros((len(x), 4))
+        self.lib.oracle_op_l2p(basis, P, _ptr(np.asarray(Xc, np.float64)),
+                               _ptr(np.ascontiguousarray(L, np.float64)), len(x), _ptr(x),
+                               _ptr(out))
+        return out
 
     def uniform_level(self, n, ncrit):
         """Depth of the uniform Morton tree (include/build_tree_omp.h:218)."""

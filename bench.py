@@ -331,9 +331,30 @@ def bench_serving(fmm, datasets, device):
         wall = time.perf_counter() - t0
         return outs, np.array(lat), np.array(que), wall
 
+    # each request alone (its own handle per order, same host-buffer path, after a warm-up):
+    # the latency a request would have on an idle GPU, the denominator of its slowdown
+    alone = np.zeros(R)
+    solo = {}
+    for i, (x, q, P) in enumerate(reqs):
+        s1 = solo.setdefault(P, fmm.Solver(P=P, theta=SERVE["theta"][P], ncrit=SERVE["ncrit"],
+                                           use_ropt=SERVE["use_ropt"], device=device))
+        s1.solve(x, q)
+        t0 = time.perf_counter()
+        s1.solve(x, q)
+        alone[i] = time.perf_counter() - t0
+    del solo
+    decades = np.floor(np.log10(sizes)).astype(int)
+
     def row(load, lam, lat, que, wall):
+        slow = lat / alone
+        by_size = {"1e%d" % d: {"requests": int((decades == d).sum()),
+                                "p50_ms": 1e3 * float(np.median(lat[decades == d])),
+                                "p99_ms": 1e3 * float(np.percentile(lat[decades == d], 99))}
+                   for d in sorted(set(decades.tolist()))}
         return {"load": load, "lambda_rps": lam, "p50_ms": 1e3 * float(np.median(lat)),
                 "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "slowdown_p50": float(np.median(slow)), "slowdown_p99": float(np.percentile(slow, 99)),
+                "latency_by_size": by_size,
                 "queue_p50_ms": 1e3 * float(np.median(que)), "particles_per_s": total / wall}
 
     b0 = srv.stats()["batches"]
@@ -385,7 +406,9 @@ def bench_serving(fmm, datasets, device):
         "accuracy": accuracy,
         "accuracy_sample": "256 stride-sampled targets of every request of >= %d bodies (last "
                            "burst), FP64 direct sum on the GPU" % SERVE["acc_min_n"],
-        "latency": "submit to result ready, host clock; Poisson gaps at load x capacity"}
+        "alone_ms": {"p50": 1e3 * float(np.median(alone)), "max": 1e3 * float(alone.max())},
+        "latency": "submit to result ready, host clock; Poisson gaps at load x capacity; "
+                   "slowdown = latency / the same request solved alone through the host C ABI"}
 
 
 def cpu_model():
@@ -663,6 +686,13 @@ def main():
     tuner.set_stream(stream.cuda_stream)
     best, tms = tuner.autotune_ncrit(x, q, candidates=(32, 48, 64, 96, 128), repeats=3)
     autotune = {"best_ncrit": best, "median_ms": {str(k): v for k, v in tms.items()}}
+    # P2P threads per target group on the headline tree (ncrit = 64): leaf-size thresholds
+    # for 4 and 2 lanes per target
+    tuner.autotune_ncrit(x, q, candidates=(WORKLOAD["ncrit"],), repeats=1)  # back to 64
+    tuner.solve(x, q)
+    g, gms = tuner.autotune_p2p(repeats=5)
+    autotune["p2p_lanes"] = {"best": {"lanes4_max": g[0], "lanes2_max": g[1]},
+                             "p2p_median_ms": {"%d/%d" % k: v for k, v in gms.items()}}
     del tuner
 
     batched = None if args.no_batch else bench_batched(fmm, datasets, torch, dev, stream, flush,

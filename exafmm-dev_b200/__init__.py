@@ -56,6 +56,7 @@ SIGNATURES = {
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
     "fmm_b200_set_mutual": (_i, [_vp, _i]),
     "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
+    "fmm_b200_autotune_p2p": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp]),
     "fmm_b200_solve_ij_host": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
     "fmm_b200_solve_ij_device": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp]),
     "fmm_b200_last_error": (C.c_char_p, [_vp]),
@@ -252,6 +253,18 @@ class Solver:
             raise FmmError(rc, self.lib.fmm_b200_last_error(self.h).decode())
 
     # ---- configuration
+    def autotune_p2p(self, candidates=((8, 16), (4, 16), (0, 16), (8, 8), (4, 8), (0, 0)),
+                     repeats=5):
+        """On the lists of the last solve, time the P2P at each (lanes4_max, lanes2_max) leaf-size
+        threshold pair; the fastest becomes the solver's.  Returns (best pair, {pair: ms})."""
+        g4 = np.ascontiguousarray([c[0] for c in candidates], np.int32)
+        g2 = np.ascontiguousarray([c[1] for c in candidates], np.int32)
+        ms = np.zeros(len(candidates))
+        best = C.c_int()
+        self._check(self.lib.fmm_b200_autotune_p2p(self.h, _p(g4), _p(g2), len(candidates),
+                                                   repeats, C.byref(best), _p(ms)))
+        return tuple(candidates[best.value]), {tuple(c): float(t) for c, t in zip(candidates, ms)}
+
     def autotune_ncrit(self, x, q, candidates=(16, 32, 48, 64, 96, 128), repeats=3):
         """Time solves of these bodies at each ncrit; the fastest becomes the solver's ncrit.
         Returns (best ncrit, {ncrit: median ms})."""

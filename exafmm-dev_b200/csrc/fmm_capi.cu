@@ -295,6 +295,58 @@ static int autotune_ncrit_t(Solver<T>& s, const int* cand, int ncand, int repeat
   return FMM_OK;
 }
 
+// P2P lane-group autotuner: on the lists of the handle's last solve, each candidate pair of
+// leaf-size thresholds (4 lanes per target up to g4 bodies, 2 up to g2) runs the P2P
+// `repeats` times after one untimed run; the median device time decides.
+template <typename T>
+static int autotune_p2p_t(Solver<T>& s, const int* g4, const int* g2, int ncand, int repeats,
+                          int* best, double* times_ms) {
+  if (s.stage < ST_DOWN) throw FmmError(FMM_ERR_STATE, "solve first: the P2P lists are tuned on");
+  const int k4 = s.p2p_g4, k2 = s.p2p_g2;
+  cudaEvent_t e0, e1;
+  FMM_CUDA(cudaEventCreate(&e0));
+  FMM_CUDA(cudaEventCreate(&e1));
+  double best_ms = 1e300;
+  int bi = 0;
+  try {
+    for (int i = 0; i < ncand; i++) {
+      s.p2p_g4 = g4[i];
+      s.p2p_g2 = g2[i];
+      run_p2p(s);
+      std::vector<float> ms;
+      for (int r = 0; r < repeats; r++) {
+        FMM_CUDA(cudaEventRecord(e0, s.stream));
+        run_p2p(s);
+        FMM_CUDA(cudaEventRecord(e1, s.stream));
+        FMM_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        FMM_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        ms.push_back(t);
+      }
+      std::sort(ms.begin(), ms.end());
+      const double med = ms[ms.size() / 2];
+      if (times_ms) times_ms[i] = med;
+      if (med < best_ms) {
+        best_ms = med;
+        bi = i;
+      }
+    }
+  } catch (...) {
+    s.p2p_g4 = k4;
+    s.p2p_g2 = k2;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s.p2p_g4 = g4[bi];
+  s.p2p_g2 = g2[bi];
+  s.stage = ST_BODIES;  // the targets now hold the tuning runs' near field: solve again
+  if (best) *best = bi;
+  return FMM_OK;
+}
+
 // targets (segment 0) and sources (segment 1) as two trees on a common box
 template <typename T>
 static void solve_ij_t(fmm_b200_solver* h, Solver<T>& s, int nt, int ns, int common_box) {
@@ -516,6 +568,18 @@ int fmm_b200_autotune_ncrit(fmm_b200_solver* h, const int* candidates, int ncand
   for (int i = 0; i < ncand; i++)
     if (candidates[i] < 1) return FMM_ERR_INVALID;
   return FMM_DISPATCH(h, autotune_ncrit_t(s, candidates, ncand, repeats, best_ncrit, times_ms));
+}
+
+int fmm_b200_autotune_p2p(fmm_b200_solver* h, const int* lanes4_max, const int* lanes2_max,
+                          int ncand, int repeats, int* best, double* times_ms) {
+  if (!h || !h->base || !lanes4_max || !lanes2_max || ncand < 1 || repeats < 1)
+    return FMM_ERR_INVALID;
+  for (int i = 0; i < ncand; i++)
+    if (lanes4_max[i] < 0 || lanes4_max[i] > 8 || lanes2_max[i] < lanes4_max[i] ||
+        lanes2_max[i] > 16)
+      return FMM_ERR_INVALID;
+  return FMM_DISPATCH(h, autotune_p2p_t(s, lanes4_max, lanes2_max, ncand, repeats, best,
+                                        times_ms));
 }
 
 int fmm_b200_solve_device(fmm_b200_solver* h, int n, const void* d_bodies, void* d_trg) {

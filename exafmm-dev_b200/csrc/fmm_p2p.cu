@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
     k_p2p(const int* __restrict__ leaves, int nleaves, const int* __restrict__ off,
           const unsigned long long* __restrict__ pairs, const int* __restrict__ ibody,
           const int* __restrict__ nbody, const vec4<T>* __restrict__ bodies, T eps2, T cycle,
-          vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+          vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e, int g4, int g2) {
   // one row of 32 sources per warp
   __shared__ __align__(16) unsigned char smem[kP2PWarps][32 * sizeof(vec4<T>)];
   const int wl = threadIdx.x >> 5;
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
   const int lane = lane_id();
   const int c = leaves[w];
   const int b0 = ibody[c], nb = nbody[c];
-  const int G = nb <= 8 ? 4 : (nb <= 16 ? 2 : 1);
+  const int G = nb <= g4 ? 4 : (nb <= g2 ? 2 : 1);
   const int s0 = off[c], s1 = off[c + 1];
   void* row = smem[wl];
   if (nb <= 32) {
@@ -360,7 +360,8 @@ template <typename T> void run_p2p(Solver<T>& s) {
   constexpr bool comp = sizeof(T) == 4;
   k_p2p<T, comp><<<ceil_div(s.nleaves, kP2PWarps), 32 * kP2PWarps, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.p2p_off.p, s.p2p.p, s.c_ibody.p, s.c_nbody.p, s.bodies.p,
-      (T)s.cfg.eps2, (T)s.cfg.cycle, s.trg_s.p, s.trg_e.p);
+      (T)s.cfg.eps2, (T)s.cfg.cycle, s.trg_s.p, s.trg_e.p, std::min(s.p2p_g4, 8),
+      std::min(s.p2p_g2, 16));
   FMM_LAUNCH_CHECK();
 }
 

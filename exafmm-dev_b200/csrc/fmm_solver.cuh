@@ -110,6 +110,9 @@ struct SolverBase {
   int trav_steps = 0, trav_maxlevel = 0;  // the last traversal's steps, and its tree depth
   int tree_plan = 0;        // levels of the handle's last tree (0: none; builds level by level)
   int write_r = 1;          // P2M / M2M set the cell radii (else the structure pass did)
+  // P2P lanes per target by target leaf size: 4 up to p2p_g4 bodies, 2 up to p2p_g2, else 1
+  // (p2p_g4 <= 8 and p2p_g2 <= 16: a warp holds 32 / lanes targets); fmm_b200_autotune_p2p
+  int p2p_g4 = 8, p2p_g2 = 16;
   DevArr<int> d_lvl;        // level ends of the planned node build
   // targets and sources in two trees (segments 0 and 1) on a common box, traversed from
   // (target root, source root) only (fmm_b200_solve_ij_*)

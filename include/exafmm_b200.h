@@ -241,6 +241,16 @@ int fmm_b200_solve_ij_device(fmm_b200_solver* s, int nt, const void* d_targets, 
  * counterpart (the reference takes ncrit from the command line, include/args.h:98). */
 int fmm_b200_autotune_ncrit(fmm_b200_solver* s, const int* candidates, int ncand, int repeats,
                             int* best_ncrit, double* times_ms);
+/* Picks the P2P kernel's threads per target group (lanes that share one target body) on the
+ * interaction lists of the handle's last solve: candidate i gives a target 4 lanes in leaves
+ * of at most lanes4_max[i] bodies, 2 lanes in leaves of at most lanes2_max[i], else 1
+ * (0 <= lanes4_max <= 8, lanes4_max <= lanes2_max <= 16; the default is 8 / 16).  Each runs the
+ * P2P `repeats` times after one untimed run; the median device time goes to times_ms[i]
+ * (may be NULL) and the fastest becomes the handle's (index in *best).  The split of a
+ * target's sources over its lanes changes only the rounding of its sums.  The handle must
+ * solve again before its results are read.  No reference counterpart. */
+int fmm_b200_autotune_p2p(fmm_b200_solver* s, const int* lanes4_max, const int* lanes2_max,
+                          int ncand, int repeats, int* best, double* times_ms);
 
 /* ---- serving: continuous batching of independent solves ------------------------------ *
  * A server owns nworkers worker threads (one CUDA stream and one solver handle per order

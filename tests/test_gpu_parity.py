@@ -7,6 +7,7 @@ differ from glibc's in the last bit, so a handful of borderline MAC decisions ma
 the same tree; FP32 within 2e-5 rel-L2 of the FP32 oracle, and within the oracle's own FMM
 error (+ 2e-6) of an FP64 direct sum.
 """
+import ctypes as C
 import importlib
 import json
 import os
@@ -299,6 +300,51 @@ def test_gromacs_wrapper(datasets):
     ef = d[:, 1:] - coef * dip
     assert np.sqrt(((p - ep) ** 2).sum() / (ep ** 2).sum()) < 1e-3
     assert np.sqrt(((f.reshape(-1, 3) - ef) ** 2).sum() / (ef ** 2).sum()) < 1e-3
+
+
+def test_charmm_wrapper(datasets):
+    """fmm_coulomb_ (wrappers/charmm.cxx:119-202) on one rank: only bodies with
+    icpumap == 1 are solved (every other entry becomes 0); positions are wrapped into
+    [-cycle/2, cycle/2] (include/vec.h:193-204); p and f accumulate, per original index,
+    (TRG - dipole correction) * q * 332.0716 (charmm.cxx:183-189, up_down_pass.h:160-168),
+    and the other bodies' p and f are left as they were."""
+    lib = fmm.load_library()
+    rng = np.random.default_rng(12)
+    nglobal = 6000
+    x, q = datasets.make("cube", nglobal, seed=8, precision="f64")
+    cycle = 1.5  # positions in [-1, 1]: some leave [-0.75, 0.75] and are wrapped
+    icpumap = rng.choice(np.array([0, 1, 1, 1, 2], np.int32), nglobal).astype(np.int32)
+    local = np.flatnonzero(icpumap == 1)
+    p0 = rng.uniform(-1, 1, nglobal)
+    f0 = rng.uniform(-1, 1, 3 * nglobal)
+    p, f = p0.copy(), f0.copy()
+    xf = np.ascontiguousarray(x.reshape(-1))
+    images, theta, verbose = C.c_int(0), C.c_double(0.4), C.c_int(0)
+    lib.fmm_init_(C.byref(images), C.byref(theta), C.byref(verbose))
+    ng, cyc = C.c_int(nglobal), C.c_double(cycle)
+    lib.fmm_coulomb_(C.byref(ng), fmm._p(icpumap), fmm._p(xf), fmm._p(q), fmm._p(p), fmm._p(f),
+                     C.byref(cyc))
+    lib.fmm_finalize_()
+    assert set(np.unique(icpumap)) <= {0, 1}
+    assert np.array_equal(np.flatnonzero(icpumap == 1), local)
+    other = np.setdiff1d(np.arange(nglobal), local)
+    assert np.array_equal(p[other], p0[other])
+    assert np.array_equal(f.reshape(-1, 3)[other], f0.reshape(-1, 3)[other])
+    xl = x[local].copy()
+    xl[xl < -cycle / 2] += cycle
+    xl[xl > cycle / 2] -= cycle
+    ql = q[local]
+    n = len(local)
+    d = Oracle("f64").direct(xl, xl, ql)
+    dip = (xl * ql[:, None]).sum(0)
+    coef = 4 * np.pi / (3 * cycle ** 3)
+    celec = 332.0716
+    ep = (d[:, 0] - coef * (dip ** 2).sum() / n / ql) * ql * celec
+    ef = (d[:, 1:] - coef * dip) * ql[:, None] * celec
+    gp = p[local] - p0[local]
+    gf = f.reshape(-1, 3)[local] - f0.reshape(-1, 3)[local]
+    assert np.sqrt(((gp - ep) ** 2).sum() / (ep ** 2).sum()) < 1e-3
+    assert np.sqrt(((gf - ef) ** 2).sum() / (ef ** 2).sum()) < 1e-3
 
 
 def test_timings_and_errors(datasets):

@@ -10,6 +10,8 @@ import importlib
 import numpy as np
 import pytest
 
+from oracle import rel_l2
+
 pytestmark = pytest.mark.gpu
 fmm = importlib.import_module("exafmm-dev_b200")
 
@@ -55,3 +57,20 @@ def test_autotune_ncrit_picks_the_fastest_candidate(datasets):
     # the handle now solves with the tuned ncrit: bitwise a fresh handle at that ncrit
     got = s.solve(x, q)
     assert np.array_equal(got, fmm.Solver(P=8, theta=0.4, ncrit=best).solve(x, q))
+
+
+def test_autotune_p2p_lanes(datasets):
+    """fmm_b200_autotune_p2p: the thresholds picked are a candidate, and the solves after it
+    agree with the default mapping to rounding (only the split of a target's sources over its
+    lanes changes)."""
+    x, q = datasets.make("plummer", 60000, seed=5, precision="f32")
+    s = fmm.Solver(P=8, theta=0.4, ncrit=64, use_ropt=0)
+    ref = s.solve(x, q)
+    cands = ((8, 16), (0, 16), (0, 0))
+    best, ms = s.autotune_p2p(candidates=cands, repeats=2)
+    assert best in cands and all(v > 0 for v in ms.values())
+    got = s.solve(x, q)
+    pot, acc = rel_l2(got, ref)
+    assert pot < 1e-6 and acc < 1e-6, (pot, acc)
+    with pytest.raises(fmm.FmmError):
+        s.autotune_p2p(candidates=((9, 16),))

@@ -363,17 +363,21 @@ def bench_serving(fmm, datasets, device):
     #                   grows the buffers that the first batches did not reach)
     bursts, caps, outs = [], [], None
     for _ in range(SERVE["passes"]):  # bursts: every request at t = 0
+        a0 = fmm.device_allocations()
         outs, lat, que, wall = run(np.zeros(R))
         caps.append(R / wall)
         bursts.append(row("burst", None, lat, que, wall))
+        bursts[-1]["device_allocations"] = fmm.device_allocations() - a0
     capacity = float(np.median(caps))
     sweep = list(bursts)
     for f in SERVE["load"]:
         lam = f * capacity
         gaps = rng.exponential(1.0 / lam, R)
         gaps[0] = 0.0
+        a0 = fmm.device_allocations()
         _, lat, que, wall = run(gaps)
         sweep.append(row(f, lam, lat, que, wall))
+        sweep[-1]["device_allocations"] = fmm.device_allocations() - a0
     st = srv.stats()
     prof = srv.profile()
     srv.close()

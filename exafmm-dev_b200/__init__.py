@@ -105,6 +105,7 @@ SIGNATURES = {
     "fmm_b200_direct_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_fp32_peak": (_i, [_i, _vp]),
     "fmm_b200_kernel_launches": (_ll, []),
+    "fmm_b200_device_allocations": (_ll, []),
     "FMM_Init": (None, [_i]),
     "FMM_Finalize": (None, []),
     "FMM_Partition": (None, [_vp, _vp, _vp, _vp, _d]),
@@ -181,6 +182,11 @@ def direct_noalloc(xt, xs, qs, eps2=0.0, device=0):
     if rc != FMM_OK:
         raise FmmError(rc, lib.fmm_b200_last_error(None).decode())
     return out
+
+
+def device_allocations():
+    """cudaMalloc calls of the solver handles so far (fmm_b200_device_allocations)."""
+    return load_library().fmm_b200_device_allocations()
 
 
 def fp32_peak_tflops(device=0):

@@ -118,6 +118,7 @@ struct FmmError : std::runtime_error {
 // every kernel launch of this library is followed by FMM_LAUNCH_CHECK(): it counts the
 // launch (fmm_b200_kernel_launches) and surfaces launch errors
 extern std::atomic<long long> g_launches;
+extern std::atomic<long long> g_device_allocs;  // cudaMalloc calls of the solvers' arrays
 #define FMM_LAUNCH_CHECK()                                          \
   do {                                                              \
     ::fmmb200::g_launches.fetch_add(1, std::memory_order_relaxed);  \

@@ -50,6 +50,7 @@ template <typename U> struct DevArr {
     p = nullptr;
     cap = 0;
     size_t want = n + n / 4 + 256;
+    g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaMalloc((void**)&p, want * sizeof(U));
     if (e != cudaSuccess) {
       (void)cudaGetLastError();

@@ -13,6 +13,7 @@
 
 namespace fmmb200 {
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_device_allocs{0};
 }
 using namespace fmmb200;
 
@@ -123,6 +124,7 @@ void noalloc_setup(int device, double** base, cudaStream_t* stream) {
 extern "C" {
 
 long long fmm_b200_kernel_launches(void) { return g_launches.load(); }
+long long fmm_b200_device_allocations(void) { return g_device_allocs.load(); }
 
 int fmm_b200_direct_noalloc(int device, int nt, const double* xt, int ns, const double* xs,
                             const double* qs, double eps2, double* out) {

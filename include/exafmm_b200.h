@@ -320,6 +320,10 @@ int fmm_b200_fp32_peak(int device, double* tflops);
 /* Number of this library's own kernel launches so far (library calls such as CUB sorts are
  * not counted).  No reference counterpart. */
 long long fmm_b200_kernel_launches(void);
+/* Number of device allocations (cudaMalloc) the solver handles have made so far: a handle
+ * grows its arrays the first time a solve needs more, and each growth synchronises the
+ * device.  No reference counterpart. */
+long long fmm_b200_device_allocations(void);
 
 /* ---- reference wrapper ABI (single GPU, single rank) ----------------------------------
  * (Left out when EXAFMM_B200_NO_GROMACS_ABI is defined: the PetIGA wrapper library,

@@ -250,7 +250,17 @@ def bench_batched(fmm, datasets, torch, dev, stream, flush, device, steps):
         for _ in range(3):
             timed(batch)
         ms = [timed(batch) for _ in range(max(3, steps // 2))]
-        r = {"theta": theta, "value": total / (float(np.median(ms)) * 1e-3),
+        tuned = None
+        if one_by_one_too:
+            # the ncrit autotuner on the batch itself (the forest the last call built); the
+            # timed batches run at the ncrit it picks
+            best, tms = s.autotune_ncrit(candidates=(32, 48, 64, 96, 128), repeats=3)
+            tuned = {"best_ncrit": best, "median_ms": {str(k): v for k, v in tms.items()}}
+            for _ in range(2):
+                timed(batch)
+            ms = [timed(batch) for _ in range(max(3, steps // 2))]
+        r = {"theta": theta, "ncrit": s.cfg.ncrit, "autotune_ncrit": tuned,
+             "value": total / (float(np.median(ms)) * 1e-3),
              "unit": "particles/s",
              "ms_per_batch": {"p50": float(np.median(ms)), "p99": float(np.percentile(ms, 99))},
              "phases_ms": s.timings()}
@@ -545,6 +555,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="warm-ups, then one solve between cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off), then exit")
+    ap.add_argument("--profile-precision", default="f32", choices=["f32", "f64"],
+                    help="working precision of the --profile solve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     datasets = importlib.import_module("exafmm-dev_b200.datasets")
@@ -565,10 +577,12 @@ def main():
     n = args.n
     x, q = datasets.make(WORKLOAD["dist"], n, seed=43 + rank, precision="f32")
     kw = {k: WORKLOAD[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax", "use_ropt")}
-    solver = fmm.Solver(precision="f32", device=local, **kw)
+    prec = args.profile_precision if args.profile else "f32"
+    solver = fmm.Solver(precision=prec, device=local, **kw)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
-    bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1), dtype=torch.float32, device=dev)
+    bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1),
+                          dtype=torch.float32 if prec == "f32" else torch.float64, device=dev)
     out = torch.empty_like(bodies)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
@@ -588,7 +602,7 @@ def main():
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
         if rank == 0:
-            print(json.dumps({"profile": WORKLOAD_NAME, "n_bodies": n,
+            print(json.dumps({"profile": WORKLOAD_NAME, "n_bodies": n, "precision": prec,
                               "phases_ms": solver.timings(), "lists": solver.list_counts()}))
         return
     if pg:

@@ -53,6 +53,7 @@ SIGNATURES = {
     "fmm_b200_create": (_i, [_vp, _vp]),
     "fmm_b200_destroy": (_i, [_vp]),
     "fmm_b200_set_stream": (_i, [_vp, _vp]),
+    "fmm_b200_trim": (_i, [_vp]),
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
     "fmm_b200_set_mutual": (_i, [_vp, _i]),
     "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
@@ -254,6 +255,10 @@ class Solver:
     def close(self):
         self.__del__()
 
+    def trim(self):
+        """Free the device buffers the solver has grown out of (fmm_b200_trim)."""
+        self._check(self.lib.fmm_b200_trim(self.h))
+
     def _check(self, rc):
         if rc != FMM_OK:
             raise FmmError(rc, self.lib.fmm_b200_last_error(self.h).decode())
@@ -271,10 +276,12 @@ class Solver:
                                                    repeats, C.byref(best), _p(ms)))
         return tuple(candidates[best.value]), {tuple(c): float(t) for c, t in zip(candidates, ms)}
 
-    def autotune_ncrit(self, x, q, candidates=(16, 32, 48, 64, 96, 128), repeats=3):
+    def autotune_ncrit(self, x=None, q=None, candidates=(16, 32, 48, 64, 96, 128), repeats=3):
         """Time solves of these bodies at each ncrit; the fastest becomes the solver's ncrit.
+        Without x, q: the bodies the solver last held (a batch of solves included).
         Returns (best ncrit, {ncrit: median ms})."""
-        self.set_bodies(x, q)
+        if x is not None:
+            self.set_bodies(x, q)
         cand = np.ascontiguousarray(candidates, np.int32)
         times = np.zeros(len(cand))
         best = C.c_int()

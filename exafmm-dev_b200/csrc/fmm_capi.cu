@@ -463,21 +463,46 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out) {
   return FMM_OK;
 }
 
-#define FMM_RELEASE_ALL(s)                                                                 \
+// every device array of a handle (the typed ones through the precision); OP is a member
+// function of DevArr (release, free_retired)
+#define FMM_FOR_ALL_ARRAYS(h, OP)                                                          \
   do {                                                                                     \
-    DevArr<int>* ia[] = {&s.nbegin,   &s.ncount,   &s.nparent,  &s.nchildn, &s.nfirst,     \
-                         &s.nnode,    &s.npos,     &s.ncb,      &s.nlevel,  &s.nsplit,     \
-                         &s.coff,     &s.leaves,   &s.idx,      &s.idx2,    &s.scal,       \
-                         &s.c_iparent, &s.c_ichild, &s.c_nchild, &s.c_ibody, &s.c_nbody,   \
-                         &s.c_level,  &s.order,    &s.m2l_off,  &s.p2p_off, &s.seg_cnt,    \
-                         &s.d_lvl,    &s.seg_cnt2, &s.body_leaf};                          \
-    for (auto* a : ia) a->release();                                                       \
-    s.keys.release(); s.keys2.release(); s.c_icell.release(); s.m2l.release();             \
-    s.c_info.release();                                                                    \
-    s.p2p.release(); s.list_tmp.release(); s.p2p_pairs_count.release();                   \
-    s.cub_tmp.release(); s.front.release(); s.front2.release();                           \
-    s.seg_keys2.release(); s.cub_tmp2.release();                                           \
+    SolverBase& s_ = *(h)->base;                                                           \
+    DevArr<int>* ia[] = {&s_.nbegin,   &s_.ncount,   &s_.nparent,  &s_.nchildn, &s_.nfirst, \
+                         &s_.nnode,    &s_.npos,     &s_.ncb,      &s_.nlevel,  &s_.nsplit, \
+                         &s_.coff,     &s_.leaves,   &s_.idx,      &s_.idx2,    &s_.scal,   \
+                         &s_.c_iparent, &s_.c_ichild, &s_.c_nchild, &s_.c_ibody, &s_.c_nbody, \
+                         &s_.c_level,  &s_.order,    &s_.m2l_off,  &s_.p2p_off, &s_.seg_cnt, \
+                         &s_.d_lvl,    &s_.seg_cnt2, &s_.body_leaf, &s_.d_seg,  &s_.d_root_first, \
+                         &s_.d_root_count, &s_.nsid, &s_.c_root,   &s_.cbase,   &s_.fs_pos, \
+                         &s_.fs_pos2,  &s_.fs_idx,   &s_.m2l_tgt,  &s_.k_list,  &s_.k_saved_leaves}; \
+    for (auto* a : ia) a->OP();                                                            \
+    s_.keys.OP(); s_.keys2.OP(); s_.c_icell.OP(); s_.m2l.OP(); s_.fs_keys.OP();            \
+    s_.c_info.OP(); s_.fs_root.OP(); s_.fs_root2.OP();                                     \
+    s_.p2p.OP(); s_.list_tmp.OP(); s_.p2p_pairs_count.OP();                                \
+    s_.cub_tmp.OP(); s_.front.OP(); s_.front2.OP();                                        \
+    s_.seg_keys2.OP(); s_.cub_tmp2.OP(); s_.dtmp.OP();                                     \
+    if ((h)->precision == FMM_FP64) {                                                      \
+      Solver<double>& d_ = *static_cast<Solver<double>*>((h)->base);                       \
+      d_.bodies_in.OP(); d_.bodies.OP(); d_.trg_s.OP(); d_.trg_e.OP(); d_.trg_out.OP();    \
+      d_.cX.OP(); d_.box.OP(); d_.M.OP(); d_.L.OP(); d_.nX.OP(); d_.m0.OP();               \
+      d_.pM.OP(); d_.pM2.OP(); d_.pC.OP(); d_.c_root_cells.OP(); d_.minmax_part.OP();      \
+      d_.k_rows.OP(); d_.k_cx.OP(); d_.k_trg.OP();                                         \
+    } else {                                                                               \
+      Solver<float>& d_ = *static_cast<Solver<float>*>((h)->base);                         \
+      d_.bodies_in.OP(); d_.bodies.OP(); d_.trg_s.OP(); d_.trg_e.OP(); d_.trg_out.OP();    \
+      d_.cX.OP(); d_.box.OP(); d_.M.OP(); d_.L.OP(); d_.nX.OP(); d_.m0.OP();               \
+      d_.pM.OP(); d_.pM2.OP(); d_.pC.OP(); d_.c_root_cells.OP(); d_.minmax_part.OP();      \
+      d_.k_rows.OP(); d_.k_cx.OP(); d_.k_trg.OP();                                         \
+    }                                                                                      \
   } while (0)
+
+int fmm_b200_trim(fmm_b200_solver* h) {
+  return guarded(h, [&] {
+    FMM_CUDA(cudaStreamSynchronize(h->base->stream));
+    FMM_FOR_ALL_ARRAYS(h, free_retired);
+  });
+}
 
 int fmm_b200_destroy(fmm_b200_solver* h) {
   if (!h) return FMM_ERR_INVALID;
@@ -485,19 +510,7 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     SolverBase& s = *h->base;
     cudaSetDevice(s.cfg.device);
     cudaStreamSynchronize(s.stream);
-    FMM_RELEASE_ALL(s);
-    if (h->precision == FMM_FP64) {
-      Solver<double>& d = *static_cast<Solver<double>*>(h->base);
-      d.bodies_in.release(); d.bodies.release(); d.trg_s.release(); d.trg_e.release();
-      d.trg_out.release(); d.cX.release(); d.box.release(); d.M.release(); d.L.release();
-      d.nX.release(); d.minmax_part.release();
-    } else {
-      Solver<float>& d = *static_cast<Solver<float>*>(h->base);
-      d.bodies_in.release(); d.bodies.release(); d.trg_s.release(); d.trg_e.release();
-      d.trg_out.release(); d.cX.release(); d.box.release(); d.M.release(); d.L.release();
-      d.nX.release(); d.minmax_part.release();
-    }
-    h->base->dtmp.release();
+    FMM_FOR_ALL_ARRAYS(h, release);
     for (int i = 0; i < 2 * FMM_NUM_PHASES; i++)
       if (s.ev[i]) cudaEventDestroy(s.ev[i]);
     if (s.fork) cudaEventDestroy(s.fork);

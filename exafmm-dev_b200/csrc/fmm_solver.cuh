@@ -23,44 +23,58 @@
 namespace fmmb200 {
 
 // A grow-only device array owned by one solver: freed with it, moved (never copied).
+// Buffers it grows out of are retired, not freed, until the array is released: cudaFree
+// synchronises the whole device, which would stall every other stream at each growth (the
+// serving loop's other workers among them).  Growth is geometric (x1.5), so the retired
+// buffers add up to at most twice the final size.
 template <typename U> struct DevArr {
   U* p = nullptr;
   size_t cap = 0;
+  std::vector<U*> retired;
   DevArr() = default;
   DevArr(const DevArr&) = delete;
   DevArr& operator=(const DevArr&) = delete;
-  DevArr(DevArr&& o) noexcept : p(o.p), cap(o.cap) {
+  DevArr(DevArr&& o) noexcept : p(o.p), cap(o.cap), retired(std::move(o.retired)) {
     o.p = nullptr;
     o.cap = 0;
+    o.retired.clear();
   }
   DevArr& operator=(DevArr&& o) noexcept {
     if (this != &o) {
       release();
       p = o.p;
       cap = o.cap;
+      retired = std::move(o.retired);
       o.p = nullptr;
       o.cap = 0;
+      o.retired.clear();
     }
     return *this;
   }
   ~DevArr() { release(); }
   void ensure(size_t n) {
     if (n <= cap) return;
-    if (p) cudaFree(p);
+    if (p) retired.push_back(p);
     p = nullptr;
     cap = 0;
-    size_t want = n + n / 4 + 256;
+    size_t want = n + n / 2 + 256;
     g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaMalloc((void**)&p, want * sizeof(U));
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
+      p = nullptr;
       throw FmmError(FMM_ERR_NO_MEMORY, "cudaMalloc of " + std::to_string(want * sizeof(U)) +
                                             " bytes failed: " + cudaGetErrorString(e));
     }
     cap = want;
   }
+  void free_retired() {
+    for (U* q : retired) cudaFree(q);
+    retired.clear();
+  }
   void release() {
     if (p) cudaFree(p);
+    free_retired();
     p = nullptr;
     cap = 0;
   }

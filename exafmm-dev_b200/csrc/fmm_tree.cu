@@ -509,13 +509,18 @@ __global__ void k_leaf_scatter(int nnodes, const int* __restrict__ nchildn,
   if (v < nnodes && nchildn[v] == 0) leaves[off[v]] = npos[v];
 }
 
-// grow a node array keeping its contents
+// grow a node array keeping its contents (the old buffer is retired, as DevArr::ensure does)
 template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
   if (n <= a.cap) return;
   DevArr<U> b;
   b.ensure(n > 2 * a.cap ? n : 2 * a.cap);
   if (a.p) FMM_CUDA(cudaMemcpyAsync(b.p, a.p, a.cap * sizeof(U), cudaMemcpyDeviceToDevice, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
+  if (a.p) b.retired.push_back(a.p);
+  b.retired.insert(b.retired.end(), a.retired.begin(), a.retired.end());
+  a.p = nullptr;
+  a.cap = 0;
+  a.retired.clear();
   a = std::move(b);
 }
 

@@ -100,6 +100,12 @@ int fmm_b200_create(const fmm_b200_config* cfg, fmm_b200_solver** out);
 int fmm_b200_destroy(fmm_b200_solver* s);
 /* Work is issued on this stream (a cudaStream_t; NULL = the legacy default stream). */
 int fmm_b200_set_stream(fmm_b200_solver* s, void* stream);
+/* A handle grows its device arrays when a solve needs more, and keeps the buffers it grew
+ * out of instead of freeing them during the solve (cudaFree synchronises the whole device,
+ * which would stall the caller's other streams); they add up to at most twice the arrays'
+ * final size and are freed with the handle.  fmm_b200_trim frees them now: a device-wide
+ * synchronisation, for a moment when the device is idle.  No reference counterpart. */
+int fmm_b200_trim(fmm_b200_solver* s);
 /* Periodic boundary of the next traversals: image levels and period (the arguments the
  * reference passes to Traversal() and dualTreeTraversal(); include/traversal.h:216-264). */
 int fmm_b200_set_periodic(fmm_b200_solver* s, int images, double cycle);

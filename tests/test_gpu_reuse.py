@@ -74,3 +74,22 @@ def test_autotune_p2p_lanes(datasets):
     assert pot < 1e-6 and acc < 1e-6, (pot, acc)
     with pytest.raises(fmm.FmmError):
         s.autotune_p2p(candidates=((9, 16),))
+
+
+def test_growth_keeps_grown_out_buffers_until_trim(datasets):
+    """A handle that grows (a larger solve after a smaller one) allocates without freeing
+    during the solve; fmm_b200_trim then frees the buffers it grew out of, and later solves
+    give bitwise the same results."""
+    xs, qs = datasets.make("plummer", 20000, seed=31, precision="f32")
+    xl, ql = datasets.make("plummer", 200000, seed=32, precision="f32")
+    s = fmm.Solver(P=8, theta=0.4, ncrit=64, use_ropt=0)
+    s.solve(xs, qs)
+    a0 = fmm.device_allocations()
+    big = s.solve(xl, ql)
+    assert fmm.device_allocations() > a0  # the arrays grew
+    s.trim()
+    assert np.array_equal(s.solve(xl, ql), big)
+    a1 = fmm.device_allocations()
+    small = s.solve(xs, qs)
+    assert fmm.device_allocations() == a1  # no growth for a smaller solve
+    assert np.array_equal(small, fmm.Solver(P=8, theta=0.4, ncrit=64, use_ropt=0).solve(xs, qs))

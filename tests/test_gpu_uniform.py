@@ -135,3 +135,34 @@ def test_batches_are_not_supported(datasets):
     with pytest.raises(fmm.FmmError) as e:
         s.solve_batch([x, x], [q, q])
     assert e.value.code == fmm.FMM_ERR_NOT_SUPPORTED
+
+
+@pytest.mark.parametrize("prec,basis,P,kw", [
+    ("f64", "spherical", 6, dict(images=2, cycle=2.0)),
+    ("f32", "cartesian", 5, dict(images=1, cycle=2.0)),
+    ("f64", "spherical", 8, dict(mutual=1)),
+])
+def test_periodic_and_mutual_on_the_uniform_tree(prec, basis, P, kw, datasets):
+    """Periodic images and the mutual traversal run on the uniform tree as on the adaptive
+    one: lists bit-exact against the oracle (which the reference pins for both), results
+    within the precision's bound."""
+    x, q = datasets.make("cube", 6000, seed=23, precision=prec)
+    base = dict(ncrit=32, theta=0.4, use_ropt=0)
+    o = Oracle(prec).run(x, q, basis=SPHERICAL if basis == "spherical" else CARTESIAN, P=P,
+                         kahan=int(prec == "f32"), tree=TREE_UNIFORM, **base, **kw)
+    s = fmm.Solver(basis=basis, P=P, precision=prec, tree="uniform", **base, **kw)
+    trg = s.solve(x, q)
+    m2l, p2p = s.lists()
+    om2l, op2p = np.sort(o.m2l()), np.sort(o.p2p())
+    if kw.get("mutual"):
+        # the device emits both directions of every mutual pair; the oracle the reference's
+        # unordered set in visiting order
+        def both(pairs):
+            t, src = pairs >> 32, pairs & 0xffffffff
+            return np.sort(np.unique(np.concatenate([pairs, (src << 32) | t])))
+        om2l, op2p = both(om2l), both(op2p)
+    assert np.array_equal(m2l, om2l)
+    assert np.array_equal(p2p, op2p)
+    pot, acc = rel_l2(trg, o.trg())
+    tol = 2e-5 if prec == "f32" else 1e-10
+    assert pot < tol and acc < tol, (pot, acc)

@@ -5,8 +5,7 @@
 // that every order can be held to the same accuracy.  A scheduler thread forms batches from
 // whatever is pending whenever a worker is free: the oldest request decides the order P (and
 // angle), later requests of the same P and angle join in arrival order while the
-// batch fits the free part of the device-memory budget and the batch-size limit, and the
-// batch goes preferably to a free worker that last ran the same order.  Each
+// batch fits the free part of the device-memory budget and the batch-size limit.  Each
 // worker owns a CUDA stream and one solver handle per order, so batches on different
 // workers overlap on the GPU; requests that arrive while batches run are admitted into the
 // next batch as soon as a worker and budget free up.  A request's result does not depend on
@@ -50,8 +49,6 @@ struct Worker {
   std::map<std::pair<int, double>, fmm_b200_solver*> handles;  // per (order, theta)
   std::vector<std::shared_ptr<Request>> batch;
   bool busy = false;
-  int last_P = 0;  // order and opening angle of the worker's last batch (0: none yet)
-  double last_theta = 0;
   std::thread thread;
   // pinned staging for the batch's inputs / outputs; staging it has grown out of is kept
   // until the worker exits (cudaFreeHost synchronises the device, stalling the other workers)
@@ -253,23 +250,6 @@ void scheduler_loop(fmm_b200_server* S) {
     // and angle in arrival order
     const int P = S->pending.front()->P;
     const double theta = S->pending.front()->theta;
-    // order affinity: the batch goes to a free worker that last ran this order and angle if
-    // there is one, else to a free worker that has no handle for it yet, so that each
-    // handle's arrays reach the sizes of its order's batches and stop growing (a growth is
-    // a cudaMalloc of a new buffer)
-    for (auto& w : S->workers)
-      if (!w->busy && w->last_P == P && w->last_theta == theta) {
-        free_w = w.get();
-        break;
-      }
-    if (free_w->last_P != P || free_w->last_theta != theta)
-      for (auto& w : S->workers)
-        if (!w->busy && w->last_P == 0) {
-          free_w = w.get();
-          break;
-        }
-    free_w->last_P = P;
-    free_w->last_theta = theta;
     std::vector<std::shared_ptr<Request>> batch;
     for (auto it = S->pending.begin(); it != S->pending.end() && (int)batch.size() < S->max_batch;) {
       if ((*it)->P == P && (*it)->theta == theta && S->in_flight + (*it)->bytes <= S->budget) {

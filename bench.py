@@ -178,7 +178,8 @@ BATCH_THETA_1E4 = 0.3
 # the reference's FP32 + Kahan build: worst 4.1e-5 at P = 6, 2.6e-5 at P = 8, 2.1e-5 at P = 10)
 SERVE = dict(requests=48, n_min=1000, n_max=1000000, orders=(6, 8, 10),
              theta={6: 0.22, 8: 0.30, 10: 0.35}, ncrit=64, use_ropt=0, workers=3, max_batch=64,
-             hbm_budget_gb=60.0, load=(0.3, 0.6, 0.9), passes=3, acc_min_n=10000)
+             hbm_budget_gb=60.0, load=(0.3, 0.6, 0.9), passes=3, warmup_passes=4,
+             acc_min_n=10000)
 
 
 def log_uniform_sizes(rng, count, lo, hi):
@@ -368,9 +369,13 @@ def bench_serving(fmm, datasets, device):
                 "queue_p50_ms": 1e3 * float(np.median(que)), "particles_per_s": total / wall}
 
     b0 = srv.stats()["batches"]
-    run(np.zeros(R))  # warm-up: handles per order, pinned staging, device buffers grown
-    run(np.zeros(R))  # (the batches of a pass differ from run to run; a second pass
-    #                   grows the buffers that the first batches did not reach)
+    # warm-up bursts: every worker's handle per order grows to the largest batch it meets
+    # (the batches of a pass differ with the arrival timing, so this takes a few passes)
+    warm_allocs = []
+    for _ in range(SERVE["warmup_passes"]):
+        a0 = fmm.device_allocations()
+        run(np.zeros(R))
+        warm_allocs.append(fmm.device_allocations() - a0)
     bursts, caps, outs = [], [], None
     for _ in range(SERVE["passes"]):  # bursts: every request at t = 0
         a0 = fmm.device_allocations()
@@ -412,6 +417,7 @@ def bench_serving(fmm, datasets, device):
                         SERVE["ncrit"], SERVE["use_ropt"], SERVE["workers"],
                         SERVE["max_batch"], SERVE["hbm_budget_gb"]),
         "bodies_per_pass": total, "capacity_rps": capacity,
+        "warmup_device_allocations": warm_allocs,
         "capacity_rps_per_burst": caps,
         "capacity_spread": (max(caps) - min(caps)) / capacity,
         "sweep": sweep,
@@ -490,6 +496,10 @@ def bench_cartesian(fmm, datasets, torch, dev, stream, flush, device, steps, clk
     s.set_stream(stream.cuda_stream)
     bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1), dtype=torch.float32, device=dev)
     out = torch.empty_like(bodies)
+    # the P2P lanes per target picked on this workload's own lists
+    s.solve_device(n, bodies.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    lanes, lanes_ms = s.autotune_p2p(repeats=3)
     ms, phase_sum = [], None
     for it in range(3 + max(3, steps // 2)):
         with torch.cuda.stream(stream):
@@ -516,6 +526,8 @@ def bench_cartesian(fmm, datasets, torch, dev, stream, flush, device, steps, clk
            "value": n / (float(np.median(ms)) * 1e-3), "unit": "particles/s",
            "ms_per_step": float(np.median(ms)), "phases_ms": phases,
            "work": {"m2l_pairs": nm2l, "p2p_cell_pairs": np2p, "p2p_body_pairs": body_pairs},
+           "autotune_p2p_lanes": {"best": {"lanes4_max": lanes[0], "lanes2_max": lanes[1]},
+                                  "p2p_median_ms": {"%d/%d" % k: v for k, v in lanes_ms.items()}},
            "roofline": {"m2l_tflops": m2l_tf, "m2l_frac": m2l_tf / peak,
                         "m2l_flops_per_pair": m2l_flops_per_pair(CART["P"], "cartesian"),
                         "p2p_tflops": p2p_tf, "p2p_frac": p2p_tf / peak, "peak": peak,
@@ -557,6 +569,8 @@ def main():
                          "--profile-from-start off), then exit")
     ap.add_argument("--profile-precision", default="f32", choices=["f32", "f64"],
                     help="working precision of the --profile solve")
+    ap.add_argument("--profile-workload", default="headline", choices=["headline", "cartesian"],
+                    help="--profile solve: the headline workload, or the Cartesian P = 5 one")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     datasets = importlib.import_module("exafmm-dev_b200.datasets")
@@ -575,8 +589,11 @@ def main():
         pg = dist
     dev = torch.device("cuda", local)
     n = args.n
-    x, q = datasets.make(WORKLOAD["dist"], n, seed=43 + rank, precision="f32")
-    kw = {k: WORKLOAD[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax", "use_ropt")}
+    wl = CART if args.profile and args.profile_workload == "cartesian" else WORKLOAD
+    if wl is CART and n == WORKLOAD["n"]:
+        n = CART["n"]
+    x, q = datasets.make(wl["dist"], n, seed=43 + rank, precision="f32")
+    kw = {k: wl[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax", "use_ropt")}
     prec = args.profile_precision if args.profile else "f32"
     solver = fmm.Solver(precision=prec, device=local, **kw)
     stream = torch.cuda.Stream(device=dev)
@@ -602,7 +619,8 @@ def main():
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
         if rank == 0:
-            print(json.dumps({"profile": WORKLOAD_NAME, "n_bodies": n, "precision": prec,
+            print(json.dumps({"profile": CART_NAME if wl is CART else WORKLOAD_NAME,
+                              "n_bodies": n, "precision": prec,
                               "phases_ms": solver.timings(), "lists": solver.list_counts()}))
         return
     if pg:

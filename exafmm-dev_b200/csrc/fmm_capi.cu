@@ -179,7 +179,7 @@ template <typename T> void solve_all(Solver<T>& s) {
     FMM_CUDA(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
   }
   cudaStream_t main = s.stream;
-  if (s.cfg.basis == FMM_SPHERICAL && s.ncells > 0) {
+  if (s.ncells > 0) {
     FMM_CUDA(cudaEventRecord(s.fork, s.stream));
     FMM_CUDA(cudaStreamWaitEvent(s.side_lo, s.fork, 0));
     s.stream = s.side_lo;  // below the traversal, which is on the critical path

@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(32 * CartCfg<T, P>::W)
     k_cp2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ ibody,
            const int* __restrict__ nbody, vec4<T>* __restrict__ cX,
            const vec4<T>* __restrict__ bodies, T* __restrict__ M, int ncoef, int use_rmax,
-           T theta, int* __restrict__ body_leaf) {
+           T theta, int write_r, int* __restrict__ body_leaf) {
   constexpr int NT = cart::NT(P), RS = CartCfg<T, P>::RS, KA = (NT + 31) / 32;
   constexpr int W = CartCfg<T, P>::W;
   __shared__ T rows[W][32 * RS];
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(32 * CartCfg<T, P>::W)
     const T v = __shfl_xor_sync(0xffffffffu, rmax, o);
     rmax = v > rmax ? v : rmax;
   }
-  if (lane == 0) {
+  if (lane == 0 && write_r) {
     T R = X.w;
     if (use_rmax) R = rmax < R ? rmax : R;
     cX[c].w = div_rn(R, theta);
@@ -86,7 +86,7 @@ template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_cm2m(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
            const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
-           int ncoef, int use_rmax, T theta) {
+           int ncoef, int use_rmax, T theta, int write_r) {
   constexpr int NT = cart::NT(P), KO = (NT + 31) / 32, W = 4;
   __shared__ T sc[W][NT], sm[W][NT];
   const int wl = threadIdx.x >> 5, lane = lane_id();
@@ -133,29 +133,31 @@ __global__ void __launch_bounds__(128)
     const T x = __shfl_xor_sync(0xffffffffu, rmax, o);
     rmax = x > rmax ? x : rmax;
   }
-  if (lane == 0) {
+  if (lane == 0 && write_r) {
     T R = Xp.w;
     if (use_rmax) R = rmax < R ? rmax : R;
     cX[c].w = div_rn(R, theta);
   }
 }
 
+// M2L, thread per target: the targets with pairs in order of descending pair count (so
+// the threads of a warp run about the same number of pairs), each contracting its sources
+// one after the other into the whole local expansion held in registers; no reduction.
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
-    k_cm2l(int ncells, const int* __restrict__ off, const unsigned long long* __restrict__ pairs,
-           const vec4<T>* __restrict__ cX, const T* __restrict__ M, T* __restrict__ L, int ncoef,
-           T cycle) {
+    k_cm2l(int ntgt, const int* __restrict__ tgt, const int* __restrict__ off,
+           const unsigned long long* __restrict__ pairs, const vec4<T>* __restrict__ cX,
+           const T* __restrict__ M, T* __restrict__ L, int ncoef, T cycle) {
   constexpr int NT = cart::NT(P);
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = lane_id();
-  if (c >= ncells) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntgt) return;
+  const int c = tgt[t];
   const int s0 = off[c], s1 = off[c + 1];
-  if (s0 == s1) return;
   const vec4<T> Xi = cX[c];
   T acc[NT];
 #pragma unroll
-  for (int t = 0; t < NT; t++) acc[t] = 0;
-  for (int s = s0 + lane; s < s1; s += 32) {
+  for (int k = 0; k < NT; k++) acc[k] = 0;
+  for (int s = s0; s < s1; s++) {
     const unsigned src = (unsigned)pairs[s];
     const int j = pair_cell(src);
     T px, py, pz;  // periodic shift of the source (0 without images)
@@ -168,11 +170,9 @@ __global__ void __launch_bounds__(128)
     cart::derivs<T, P>(C, dx, dy, dz, invR2, sqrt(invR2));
     cart::m2l_pair<T, P>(C, M + (size_t)j * ncoef, acc);
   }
+  T* Lc = L + (size_t)c * ncoef;
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
-    const T r = warp_sum(acc[t]);
-    if (lane == (t & 31)) L[(size_t)c * ncoef + t] += r;
-  }
+  for (int k = 0; k < NT; k++) Lc[k] += acc[k];
 }
 
 template <typename T, int P>
@@ -237,20 +237,21 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
   s.body_leaf.ensure(std::max(s.n, 1));
   k_cp2m<T, P><<<ceil_div(s.nleaves, W), 32 * W, 0, s.stream>>>(
       s.leaves.p, s.nleaves, s.c_ibody.p, s.c_nbody.p, s.cX.p, s.bodies.p, s.M.p, s.ncoef,
-      s.cfg.use_rmax, (T)s.cfg.theta, s.body_leaf.p);
+      s.cfg.use_rmax, (T)s.cfg.theta, s.write_r, s.body_leaf.p);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
   k_cm2m<T, P><<<ceil_div(hi - lo, 4), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_ichild.p,
                                                              s.c_nchild.p, s.cX.p, s.M.p,
                                                              s.ncoef, s.cfg.use_rmax,
-                                                             (T)s.cfg.theta);
+                                                             (T)s.cfg.theta, s.write_r);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2l_(Solver<T>& s) {
-  k_cm2l<T, P><<<ceil_div(s.ncells, 4), 128, 0, s.stream>>>(s.ncells, s.m2l_off.p, s.m2l.p,
-                                                              s.cX.p, s.M.p, s.L.p, s.ncoef,
-                                                              (T)s.cfg.cycle);
+  if (!s.m2l_ntgt) return;
+  k_cm2l<T, P><<<ceil_div(s.m2l_ntgt, 128), 128, 0, s.stream>>>(
+      s.m2l_ntgt, s.m2l_tgt.p, s.m2l_off.p, s.m2l.p, s.cX.p, s.M.p, s.L.p, s.ncoef,
+      (T)s.cfg.cycle);
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {

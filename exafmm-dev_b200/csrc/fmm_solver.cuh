@@ -80,6 +80,16 @@ template <typename U> struct DevArr {
   }
 };
 
+// Move a's buffers (its current one and those it retired) into b's retired list, leaving a
+// empty, for a grow-and-copy that replaces a with b without freeing during a solve.
+template <typename U> void retire_into(DevArr<U>& a, DevArr<U>& b) {
+  if (a.p) b.retired.push_back(a.p);
+  b.retired.insert(b.retired.end(), a.retired.begin(), a.retired.end());
+  a.p = nullptr;
+  a.cap = 0;
+  a.retired.clear();
+}
+
 enum Stage { ST_NONE = 0, ST_BODIES = 1, ST_TREE = 2, ST_UP = 3, ST_TRAV = 4, ST_DOWN = 5 };
 
 struct SolverBase {

@@ -449,13 +449,19 @@ __global__ void __launch_bounds__(kSegBlock)
 
 // M2L targets (cells with at least one source) keyed by their number of 32-source batches,
 // largest first, so that the warps of an M2L block have about the same amount of work
-__global__ void k_m2l_targets(int ncells, const int* __restrict__ off,
+// M2L targets by descending pair count in buckets of 2^shift pairs (targets of one bucket in
+// cell order, which keeps neighbouring targets, and so their shared sources, together);
+// cells without pairs last.  The spherical kernel takes sources in batches of 32 (shift 5),
+// the Cartesian one a thread per target (shift 0: exact counts, even warps).
+constexpr int kTgtKeyBits = 20, kTgtKeyMax = (1 << kTgtKeyBits) - 1;
+__global__ void k_m2l_targets(int ncells, const int* __restrict__ off, int shift,
                               unsigned long long* __restrict__ key, int* __restrict__ cell,
                               int* __restrict__ count) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
   const int n = off[c + 1] - off[c];
-  key[c] = n ? (unsigned long long)(1023 - min(1023, (n + 31) >> 5)) : 1023ULL;
+  const int b = (n + (1 << shift) - 1) >> shift;
+  key[c] = n ? (unsigned long long)(kTgtKeyMax - min(kTgtKeyMax, b)) : (unsigned long long)kTgtKeyMax;
   cell[c] = c;
   if (n) atomicAdd(count, 1);
 }
@@ -599,7 +605,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
       t.ensure(std::max<size_t>(2 * s.m2l.cap, nm2l + am));
       if (nm2l) FMM_CUDA(cudaMemcpyAsync(t.p, s.m2l.p, nm2l * 8, cudaMemcpyDeviceToDevice, s.stream));
       FMM_CUDA(cudaStreamSynchronize(s.stream));
-      s.m2l.release();
+      retire_into(s.m2l, t);  // no cudaFree during a solve (DevArr)
       s.m2l = std::move(t);
     }
     if (np2p + ap > (long long)s.p2p.cap) {
@@ -607,7 +613,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
       t.ensure(std::max<size_t>(2 * s.p2p.cap, np2p + ap));
       if (np2p) FMM_CUDA(cudaMemcpyAsync(t.p, s.p2p.p, np2p * 8, cudaMemcpyDeviceToDevice, s.stream));
       FMM_CUDA(cudaStreamSynchronize(s.stream));
-      s.p2p.release();
+      retire_into(s.p2p, t);  // no cudaFree during a solve (DevArr)
       s.p2p = std::move(t);
     }
     s.front2.ensure(std::max<long long>(an, 1));
@@ -752,7 +758,7 @@ template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
     group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1, s.seg_cnt.p,
                     (unsigned*)s.list_tmp.p, nullptr);
   }
-  // M2L target order: by descending batch count (stable in cell index)
+  // M2L target order: by descending pair count in buckets (stable in cell index)
   {
     int* ntgt = (int*)(cnt + 4);
     FMM_CUDA(cudaMemsetAsync(ntgt, 0, sizeof(int), s.stream));
@@ -760,10 +766,10 @@ template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
     s.keys2.ensure(s.ncells);
     s.idx.ensure(s.ncells);
     s.m2l_tgt.ensure(s.ncells);
-    k_m2l_targets<<<ceil_div(s.ncells, TB), TB, 0, s.stream>>>(s.ncells, s.m2l_off.p, s.keys.p,
-                                                               s.idx.p, ntgt);
+    k_m2l_targets<<<ceil_div(s.ncells, TB), TB, 0, s.stream>>>(
+        s.ncells, s.m2l_off.p, s.cfg.basis == FMM_SPHERICAL ? 5 : 0, s.keys.p, s.idx.p, ntgt);
     FMM_LAUNCH_CHECK();
-    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.m2l_tgt.p, s.ncells, 10);
+    sort_pairs_u64(s, s.keys.p, s.keys2.p, s.idx.p, s.m2l_tgt.p, s.ncells, kTgtKeyBits);
     FMM_CUDA(cudaMemcpyAsync(s.scal_host + 12, ntgt, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
   }
   FMM_CUDA(cudaMemcpyAsync(hc + 3, cnt + 3, 2 * sizeof(unsigned long long) + sizeof(int),

@@ -516,11 +516,7 @@ template <typename U> static void grow(SolverBase& s, DevArr<U>& a, size_t n) {
   b.ensure(n > 2 * a.cap ? n : 2 * a.cap);
   if (a.p) FMM_CUDA(cudaMemcpyAsync(b.p, a.p, a.cap * sizeof(U), cudaMemcpyDeviceToDevice, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
-  if (a.p) b.retired.push_back(a.p);
-  b.retired.insert(b.retired.end(), a.retired.begin(), a.retired.end());
-  a.p = nullptr;
-  a.cap = 0;
-  a.retired.clear();
+  retire_into(a, b);
   a = std::move(b);
 }
 

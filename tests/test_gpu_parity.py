@@ -134,7 +134,11 @@ def test_solve_matches_oracle_and_direct(name, datasets):
 @pytest.mark.parametrize("prec,P,dist,kw", [
     ("f32", 10, "plummer", dict(ncrit=64, theta=0.35, use_ropt=1)),
     ("f64", 6, "cube", dict(ncrit=32, theta=0.4, use_ropt=0)),
-    ("f32", 8, "cube", dict(ncrit=32, theta=0.4, use_ropt=1, images=2, cycle=2.0))])
+    ("f32", 8, "cube", dict(ncrit=32, theta=0.4, use_ropt=1, images=2, cycle=2.0)),
+    ("f32", 5, "sphere", dict(basis="cartesian", ncrit=32, theta=0.5, use_ropt=0)),
+    ("f64", 4, "plummer", dict(basis="cartesian", ncrit=32, theta=0.5, use_ropt=1)),
+    ("f32", 5, "cube", dict(basis="cartesian", ncrit=32, theta=0.5, use_ropt=0, images=2,
+                            cycle=2.0))])
 def test_whole_solve_equals_stages(prec, P, dist, kw, datasets):
     """A whole solve forms the multipoles on a side stream while a structure pass sets the
     cell radii for the traversal: radii, lists and results bitwise those of the stages run

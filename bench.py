@@ -28,6 +28,10 @@ use_rmax = use_ropt = 1, FP32 expansions with compensated potential/gradient sum
   accuracy vs FP64 direct, and the reference CPU build on the same config.
 * multi-GPU (torchrun): replicas only; every rank solves its own instance, no collective
   on the data path (a barrier and a max-reduction of the timings only).
+* partitioned (rank 0): the headline solve split by target parts for 2, 4 and 8 GPUs of a
+  node (exafmm-dev_b200.distributed), the parts run in turn on this GPU: per-part device
+  time, the slowest part plus the collectives' estimate, and the parts' sum checked bit for
+  bit against the whole solve.
 * batched (rank 0): 256 independent solves of uneven N in one batched call (a forest of
   trees in one set of launches), against the same solves one call each.
 * serving (rank 0): the continuous-batching server under Poisson arrivals at three loads,
@@ -483,6 +487,59 @@ def bench_reference(args, datasets):
                 "d2h_bytes_per_step": 0}}))
 
 
+def bench_partitioned(fmm, torch, stream, flush, device, n, bodies, whole, whole_ms, kw,
+                      parts=(2, 4, 8), reps=5):
+    """The headline solve split by target parts (fmm_b200_set_partition), the parts of a
+    node of `parts` GPUs run one after another on this GPU: each part's device time is what
+    its GPU would spend (it builds the whole tree and upward pass and computes its part's
+    targets), so the slowest part plus the all_gather of the bodies and the reduce_scatter
+    of the results bounds the solve on that many GPUs.  The parts' results summed must equal
+    the whole solve bit for bit."""
+    s = fmm.Solver(precision="f32", device=device, **kw)
+    s.set_stream(stream.cuda_stream)
+    o = torch.empty_like(bodies)
+    acc = torch.empty_like(bodies)
+    res = {}
+    for R in parts:
+        acc.zero_()
+        part_ms, part_bodies, part_phases = [], [], []
+        for r in range(R):
+            s.set_partition(r, R)
+            s.solve_device(n, bodies.data_ptr(), o.data_ptr())  # sizes the part's buffers
+            t = []
+            for _ in range(reps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.solve_device(n, bodies.data_ptr(), o.data_ptr())
+                e1.record(stream)
+                torch.cuda.synchronize()
+                t.append(e0.elapsed_time(e1))
+            part_ms.append(float(np.median(t)))
+            part_phases.append({k: round(v, 4) for k, v in s.timings().items()})
+            _, _, b, e = s.partition()
+            part_bodies.append(e - b)
+            with torch.cuda.stream(stream):
+                acc.add_(o)
+            torch.cuda.synchronize()
+        worst = max(part_ms)
+        coll_ms = 2 * 16.0 * n / 770e9 * 1e3
+        res[str(R)] = {
+            "part_ms": part_ms, "max_ms": worst, "mean_ms": float(np.mean(part_ms)),
+            "imbalance": worst / float(np.mean(part_ms)), "bodies_per_part": part_bodies,
+            "slowest_part_phases_ms": part_phases[int(np.argmax(part_ms))],
+            "sum_equals_whole_solve": bool(torch.equal(acc, whole)),
+            "collectives_est_ms": coll_ms,
+            "solve_ms_bound": worst + coll_ms,
+            "speedup_vs_one_gpu": whole_ms / (worst + coll_ms)}
+    s.set_partition(0, 1)
+    return {"method": "target parts of one tree; parts run in turn on one GPU (median of %d "
+                      "solves each, 256 MB L2 flush before each); collectives estimated as "
+                      "2 x 16 B/body at the pool's measured 770 GB/s NVLink peer copy" % reps,
+            "parts": res}
+
+
 def bench_cartesian(fmm, datasets, torch, dev, stream, flush, device, steps, clk_mhz,
                     cpu_baseline):
     """Cartesian P = 5, theta = 0.5, ncrit = 32, N = 4,194,304 bodies on
@@ -562,6 +619,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop line")
+    ap.add_argument("--no-partition", action="store_true",
+                    help="skip the solve split by target parts (one node of GPUs, emulated)")
     ap.add_argument("--no-cart", action="store_true",
                     help="skip the Cartesian P = 5, N = 4,194,304 line")
     ap.add_argument("--profile", action="store_true",
@@ -731,6 +790,8 @@ def main():
                              "p2p_median_ms": {"%d/%d" % k: v for k, v in gms.items()}}
     del tuner
 
+    partitioned = None if args.no_partition else bench_partitioned(
+        fmm, torch, stream, flush, local, n, bodies, out, total_ms / args.steps, kw)
     batched = None if args.no_batch else bench_batched(fmm, datasets, torch, dev, stream, flush,
                                                        local, args.steps)
     serving = None if args.no_serve else bench_serving(fmm, datasets, local)
@@ -802,6 +863,7 @@ def main():
                                     "FMA throughput measured on this GPU in this run" % clk_mhz},
         "cpu_baseline": cpu,
         "autotune_ncrit": autotune,
+        "partitioned": partitioned,
         "batched": batched,
         "serving": serving,
         "cartesian": cart,

@@ -56,6 +56,8 @@ SIGNATURES = {
     "fmm_b200_trim": (_i, [_vp]),
     "fmm_b200_set_periodic": (_i, [_vp, _i, _d]),
     "fmm_b200_set_mutual": (_i, [_vp, _i]),
+    "fmm_b200_set_partition": (_i, [_vp, _i, _i]),
+    "fmm_b200_get_partition": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "fmm_b200_autotune_ncrit": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "fmm_b200_autotune_p2p": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp]),
     "fmm_b200_solve_ij_host": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
@@ -292,6 +294,18 @@ class Solver:
 
     def set_periodic(self, images, cycle):
         self._check(self.lib.fmm_b200_set_periodic(self.h, images, cycle))
+
+    def set_partition(self, part, nparts):
+        """Compute only part `part` of nparts of each following solve (fmm_b200_set_partition):
+        the results of the other parts' bodies are 0, and the sum over the nparts handles of
+        one node's GPUs, given the same bodies, is the whole solve's result."""
+        self._check(self.lib.fmm_b200_set_partition(self.h, part, nparts))
+
+    def partition(self):
+        """(part, nparts, first body, end body): this part's bodies in tree order after a solve."""
+        v = [C.c_int() for _ in range(4)]
+        self._check(self.lib.fmm_b200_get_partition(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def set_stream(self, stream_handle):
         """Issue work on a cudaStream_t (an int handle, e.g. torch.cuda.Stream.cuda_stream)."""

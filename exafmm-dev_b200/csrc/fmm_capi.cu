@@ -119,6 +119,7 @@ template <typename T> void stage_tree(Solver<T>& s) {
   phase_begin(s, FMM_PHASE_TOTAL);
   phase_begin(s, FMM_PHASE_BOUNDS);
   build_tree(s);
+  partition_range(s);
   if (s.n == 0) phase_end(s, FMM_PHASE_BOUNDS);
   else phase_end(s, FMM_PHASE_TREE);
   s.stage = ST_TREE;
@@ -538,6 +539,34 @@ int fmm_b200_set_periodic(fmm_b200_solver* h, int images, double cycle) {
   h->base->cfg.images = images;
   h->base->cfg.cycle = cycle;
   return FMM_OK;
+}
+
+int fmm_b200_set_partition(fmm_b200_solver* h, int part, int nparts) {
+  if (!h || !h->base) return FMM_ERR_INVALID;
+  if (nparts < 1 || part < 0 || part >= nparts) {
+    h->base->err = "partition: need 0 <= part < nparts";
+    return FMM_ERR_INVALID;
+  }
+  h->base->part = part;
+  h->base->nparts = nparts;
+  h->base->err.clear();
+  return FMM_OK;
+}
+
+int fmm_b200_get_partition(fmm_b200_solver* h, int* part, int* nparts, int* body_begin,
+                           int* body_end) {
+  return guarded(h, [&] {
+    fmmb200::SolverBase& s = *h->base;
+    if (part) *part = s.part;
+    if (nparts) *nparts = s.nparts;
+    int r[2] = {0, s.n};
+    if (s.nparts > 1 && s.stage >= fmmb200::ST_TREE && s.n > 0 && s.part_range.p) {
+      FMM_CUDA(cudaMemcpyAsync(r, s.part_range.p, sizeof(r), cudaMemcpyDeviceToHost, s.stream));
+      FMM_CUDA(cudaStreamSynchronize(s.stream));
+    }
+    if (body_begin) *body_begin = r[0];
+    if (body_end) *body_end = r[1];
+  });
 }
 
 int fmm_b200_set_stream(fmm_b200_solver* h, void* stream) {

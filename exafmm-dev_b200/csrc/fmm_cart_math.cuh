@@ -108,6 +108,54 @@ __host__ __device__ __forceinline__ void m2l_pair(const T* C, const T* M, T* L) 
       }
 }
 
+// M2M of one child into the parent's expansion: every output n of m2m_term below, the same
+// terms in the same order, with compile-time indices
+template <typename T, int P>
+__host__ __device__ __forceinline__ void m2m_child(const T* C, const T* Mc, T* acc) {
+#pragma unroll
+  for (int n = 0; n < P; n++)
+#pragma unroll
+    for (int nx = n; nx >= 0; nx--)
+#pragma unroll
+      for (int ny = n - nx; ny >= 0; ny--) {
+        const int nz = n - nx - ny;
+        T s = 0;
+#pragma unroll
+        for (int kx = 0; kx <= nx; kx++)
+#pragma unroll
+          for (int ky = 0; ky <= ny; ky++)
+#pragma unroll
+            for (int kz = 0; kz <= nz; kz++)
+              s += C[idx(nx - kx, ny - ky, nz - kz)] * Mc[idx(kx, ky, kz)];
+        acc[idx(nx, ny, nz)] += s;
+      }
+}
+
+// L2L from the parent into one child: every output n of l2l_term below, the same terms in
+// the same order, with compile-time indices
+template <typename T, int P>
+__host__ __device__ __forceinline__ void l2l_child(const T* C, const T* Lp, T* Lc) {
+#pragma unroll
+  for (int n = 0; n < P; n++)
+#pragma unroll
+    for (int nx = n; nx >= 0; nx--)
+#pragma unroll
+      for (int ny = n - nx; ny >= 0; ny--) {
+        const int nz = n - nx - ny;
+        T s = 0;
+#pragma unroll
+        for (int o = 0; o + n < P; o++)
+#pragma unroll
+          for (int kx = o; kx >= 0; kx--)
+#pragma unroll
+            for (int ky = o - kx; ky >= 0; ky--) {
+              const int kz = o - kx - ky;
+              s += C[idx(kx, ky, kz)] * Lp[idx(nx + kx, ny + ky, nz + kz)];
+            }
+        Lc[idx(nx, ny, nz)] += s;
+      }
+}
+
 // one M2M output term n from one child (Kernels::M2M, MultipoleSum), runtime indices
 template <typename T>
 __host__ __device__ __forceinline__ T m2m_term(int nx, int ny, int nz, const T* C, const T* Mc) {

@@ -82,58 +82,46 @@ __device__ __forceinline__ void spread_c(const T* C, T* sc, int lane) {
     if ((t & 31) == lane) sc[t] = C[t];
 }
 
+// M2M, thread per parent cell of the level: the children's multipoles shifted one after
+// the other (cart::m2m_child, unrolled) into the parent's expansion held in registers
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_cm2m(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ ichild,
            const int* __restrict__ nchild, vec4<T>* __restrict__ cX, T* __restrict__ M,
            int ncoef, int use_rmax, T theta, int write_r) {
-  constexpr int NT = cart::NT(P), KO = (NT + 31) / 32, W = 4;
-  __shared__ T sc[W][NT], sm[W][NT];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int v = lo + blockIdx.x * W + wl;
+  constexpr int NT = cart::NT(P);
+  const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= hi) return;
   const int c = npos[v];
   const int nch = nchild[c];
   if (nch == 0) return;
   const int c0 = ichild[c];
   const vec4<T> Xp = cX[c];
-  T acc[KO];
-  int ox[KO], oy[KO], oz[KO];
+  T acc[NT];
 #pragma unroll
-  for (int i = 0; i < KO; i++) {
-    acc[i] = 0;
-    cart::mi_of(lane + 32 * i, ox[i], oy[i], oz[i]);
-  }
+  for (int t = 0; t < NT; t++) acc[t] = 0;
   T rmax = 0;
   for (int ch = 0; ch < nch; ch++) {
     const int cc = c0 + ch;
     const vec4<T> Xc = cX[cc];
-    {
-      T C[NT];
-      C[0] = 1;
-      cart::power<T, P>(C, Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
-      __syncwarp();
-      spread_c<T, NT>(C, sc[wl], lane);
-      for (int t = lane; t < NT; t += 32) sm[wl][t] = M[(size_t)cc * ncoef + t];
-    }
-    __syncwarp();
+    T C[NT];
+    C[0] = 1;
+    cart::power<T, P>(C, Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z);
+    if constexpr (3 * NT * sizeof(T) <= 1024) {  // the child's expansion in registers too
+      T Mc[NT];
 #pragma unroll
-    for (int i = 0; i < KO; i++)
-      if (lane + 32 * i < NT) acc[i] += cart::m2m_term<T>(ox[i], oy[i], oz[i], sc[wl], sm[wl]);
-    if (lane == ch) {
-      const T d = sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z)));
-      rmax = add_rn(d, Xc.w);
+      for (int t = 0; t < NT; t++) Mc[t] = M[(size_t)cc * ncoef + t];
+      cart::m2m_child<T, P>(C, Mc, acc);
+    } else {  // FP64 at P >= 6: read through L1 where used
+      cart::m2m_child<T, P>(C, M + (size_t)cc * ncoef, acc);
     }
+    const T d = sqrt_rn(norm_rn(sub_rn(Xp.x, Xc.x), sub_rn(Xp.y, Xc.y), sub_rn(Xp.z, Xc.z)));
+    const T r = add_rn(d, Xc.w);
+    rmax = r > rmax ? r : rmax;
   }
 #pragma unroll
-  for (int i = 0; i < KO; i++)
-    if (lane + 32 * i < NT) M[(size_t)c * ncoef + lane + 32 * i] = acc[i];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const T x = __shfl_xor_sync(0xffffffffu, rmax, o);
-    rmax = x > rmax ? x : rmax;
-  }
-  if (lane == 0 && write_r) {
+  for (int t = 0; t < NT; t++) M[(size_t)c * ncoef + t] = acc[t];
+  if (write_r) {
     T R = Xp.w;
     if (use_rmax) R = rmax < R ? rmax : R;
     cX[c].w = div_rn(R, theta);
@@ -175,35 +163,26 @@ __global__ void __launch_bounds__(128)
   for (int k = 0; k < NT; k++) Lc[k] += acc[k];
 }
 
+// L2L, thread per cell of the level: the parent's local expansion shifted to the cell
+// (cart::l2l_child, unrolled) and added to the cell's
 template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_cl2l(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
-           const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
-  constexpr int NT = cart::NT(P), KO = (NT + 31) / 32, W = 4;
-  __shared__ T sc[W][NT], sl[W][NT];
-  const int wl = threadIdx.x >> 5, lane = lane_id();
-  const int v = lo + blockIdx.x * W + wl;
+           const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef,
+           const int4* __restrict__ info, const int* __restrict__ range) {
+  constexpr int NT = cart::NT(P);
+  const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= hi) return;
   const int c = npos[v];
+  if (range && !part_holds(info[c], range)) return;  // no body of this part below the cell
   const int p = iparent[c];
   const vec4<T> Xc = cX[c], Xp = cX[p];
-  {
-    T C[NT];
-    C[0] = 1;
-    cart::power<T, P>(C, Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
-    spread_c<T, NT>(C, sc[wl], lane);
-    for (int t = lane; t < NT; t += 32) sl[wl][t] = L[(size_t)p * ncoef + t];
-  }
-  __syncwarp();
+  T C[NT], Lp[NT];
+  C[0] = 1;
+  cart::power<T, P>(C, Xc.x - Xp.x, Xc.y - Xp.y, Xc.z - Xp.z);
 #pragma unroll
-  for (int i = 0; i < KO; i++) {
-    const int t = lane + 32 * i;
-    if (t < NT) {
-      int nx, ny, nz;
-      cart::mi_of(t, nx, ny, nz);
-      L[(size_t)c * ncoef + t] += cart::l2l_term<T>(P, nx, ny, nz, sc[wl], sl[wl]);
-    }
-  }
+  for (int t = 0; t < NT; t++) Lp[t] = L[(size_t)p * ncoef + t];
+  cart::l2l_child<T, P>(C, Lp, L + (size_t)c * ncoef);
 }
 
 // L2P with one thread per body (tree order), its leaf from the map P2M wrote, the leaf's
@@ -212,9 +191,11 @@ template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_cl2p_bodies(int n, const int* __restrict__ body_leaf, const vec4<T>* __restrict__ cX,
                   const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
-                  vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+                  vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e,
+                  const int* __restrict__ range) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (range && (i < range[0] || i >= range[1])) return;  // another part's body
   const int c = body_leaf[i];
   if (c < 0) return;  // a body outside the cells of a single-operator call
   const vec4<T> X = cX[c];
@@ -241,7 +222,7 @@ template <typename T, int P> static void p2m_(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void m2m_(Solver<T>& s, int lo, int hi) {
-  k_cm2m<T, P><<<ceil_div(hi - lo, 4), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_ichild.p,
+  k_cm2m<T, P><<<ceil_div(hi - lo, 128), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_ichild.p,
                                                              s.c_nchild.p, s.cX.p, s.M.p,
                                                              s.ncoef, s.cfg.use_rmax,
                                                              (T)s.cfg.theta, s.write_r);
@@ -255,14 +236,16 @@ template <typename T, int P> static void m2l_(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
-  k_cl2l<T, P><<<ceil_div(hi - lo, 4), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
-                                                             s.cX.p, s.L.p, s.ncoef);
+  k_cl2l<T, P><<<ceil_div(hi - lo, 128), 128, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
+                                                             s.cX.p, s.L.p, s.ncoef,
+                                                             s.c_info.p, s.part_ptr());
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   if (!s.nleaves) return;
   k_cl2p_bodies<T, P><<<ceil_div(s.n, 128), 128, 0, s.stream>>>(
-      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p);
+      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p,
+      s.part_ptr());
   FMM_LAUNCH_CHECK();
 }
 

@@ -101,6 +101,12 @@ template <typename T> __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// a partitioned solve (fmm_b200_set_partition): does the cell whose (NCHILD, ICHILD, NBODY,
+// IBODY) record is f hold a body of the part's range [range[0], range[1])?
+__device__ __forceinline__ bool part_holds(int4 f, const int* __restrict__ range) {
+  return f.w < range[1] && f.w + f.z > range[0];
+}
+
 // ------------------------------------------------------------------ host error plumbing
 struct FmmError : std::runtime_error {
   int code;

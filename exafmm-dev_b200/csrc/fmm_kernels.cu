@@ -116,6 +116,15 @@ void bad(const std::string& msg) { throw FmmError(FMM_ERR_INVALID, msg); }
 
 // Cells to operate on: a built tree (or set cells) with host copies of their index fields,
 // expansions allocated (zero when the upward pass has not run), targets allocated.
+// The operators apply to the listed cells whatever the handle's target partition
+// (fmm_b200_set_partition): the partition is set aside for the call.
+struct WholeSolve {
+  SolverBase& s;
+  int nparts;
+  explicit WholeSolve(SolverBase& s_) : s(s_), nparts(s_.nparts) { s.nparts = 1; }
+  ~WholeSolve() { s.nparts = nparts; }
+};
+
 template <typename T> void prepare(Solver<T>& s) {
   if (s.stage < ST_TREE) throw FmmError(FMM_ERR_STATE, "no cells: build a tree or set cells");
   const int nc = s.ncells;
@@ -262,6 +271,7 @@ template <typename T, typename F> void with_saved_body_leaf(Solver<T>& s, F&& op
 }
 
 template <typename T> void op_p2m(Solver<T>& s, int n, const int* cells) {
+  WholeSolve whole(s);
   prepare(s);
   check_list(s, n, cells, "P2M");
   if (!n) return;
@@ -290,6 +300,7 @@ template <typename T> void op_p2m(Solver<T>& s, int n, const int* cells) {
 }
 
 template <typename T> void op_m2m(Solver<T>& s, int n, const int* cells) {
+  WholeSolve whole(s);
   prepare(s);
   check_list(s, n, cells, "M2M");
   std::vector<char> listed(s.ncells, 0);
@@ -322,6 +333,7 @@ template <typename T> void op_m2m(Solver<T>& s, int n, const int* cells) {
 }
 
 template <typename T> void op_l2l(Solver<T>& s, int n, const int* cells) {
+  WholeSolve whole(s);
   prepare(s);
   check_list(s, n, cells, "L2L");
   std::vector<char> listed(s.ncells, 0);
@@ -346,6 +358,7 @@ template <typename T> void op_l2l(Solver<T>& s, int n, const int* cells) {
 }
 
 template <typename T> void op_l2p(Solver<T>& s, int n, const int* cells) {
+  WholeSolve whole(s);
   prepare(s);
   check_list(s, n, cells, "L2P");
   check_disjoint_bodies(s, std::vector<int>(cells, cells + n), "L2P");

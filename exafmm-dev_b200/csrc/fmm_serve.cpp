@@ -5,7 +5,8 @@
 // that every order can be held to the same accuracy.  A scheduler thread forms batches from
 // whatever is pending whenever a worker is free: the oldest request decides the order P (and
 // angle), later requests of the same P and angle join in arrival order while the
-// batch fits the free part of the device-memory budget and the batch-size limit.  Each
+// batch fits the free part of the device-memory budget, the batch-size limit and
+// kBatchBodies bodies (a larger request rides alone).  Each
 // worker owns a CUDA stream and one solver handle per order, so batches on different
 // workers overlap on the GPU; requests that arrive while batches run are admitted into the
 // next batch as soon as a worker and budget free up.  A request's result does not depend on
@@ -31,6 +32,12 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// Bodies per batch (unless one request alone is larger).  A batch of this size fills the
+// GPU; the cap keeps the batches, and so each worker's pinned staging and its handles'
+// device arrays, within sizes reached in the first passes, so that later passes do not
+// stop to allocate (a pinned allocation of a few hundred MB takes tens of ms).
+constexpr size_t kBatchBodies = (size_t)1 << 21;
 
 struct Request {
   long long id = 0;
@@ -128,6 +135,11 @@ size_t estimate_bytes(const fmm_b200_config& c, int n, int P) {
 void worker_loop(fmm_b200_server* S, Worker* W) {
   cudaSetDevice(S->cfg.device);
   cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking);
+  // staging for a full batch (x, q, p, f: 8 doubles a body), allocated before any request
+  if (cudaMallocHost((void**)&W->pin, 8 * kBatchBodies * sizeof(double)) == cudaSuccess)
+    W->pin_cap = 8 * kBatchBodies;
+  else
+    W->pin = nullptr;
   for (;;) {
     std::vector<std::shared_ptr<Request>> batch;
     {
@@ -251,9 +263,12 @@ void scheduler_loop(fmm_b200_server* S) {
     const int P = S->pending.front()->P;
     const double theta = S->pending.front()->theta;
     std::vector<std::shared_ptr<Request>> batch;
+    size_t bodies = 0;
     for (auto it = S->pending.begin(); it != S->pending.end() && (int)batch.size() < S->max_batch;) {
-      if ((*it)->P == P && (*it)->theta == theta && S->in_flight + (*it)->bytes <= S->budget) {
+      if ((*it)->P == P && (*it)->theta == theta && S->in_flight + (*it)->bytes <= S->budget &&
+          (batch.empty() || bodies + (size_t)(*it)->n <= kBatchBodies)) {
         S->in_flight += (*it)->bytes;
+        bodies += (size_t)(*it)->n;
         batch.push_back(*it);
         it = S->pending.erase(it);
       } else {
@@ -274,9 +289,14 @@ int fmm_b200_server_create(const fmm_b200_config* cfg, double hbm_budget_bytes, 
                            int max_batch, fmm_b200_server** out) {
   if (!cfg || !out || nworkers < 1 || max_batch < 1 || !(hbm_budget_bytes > 0))
     return FMM_ERR_INVALID;
-  // validate the configuration (and the device) once up front
+  // validate the configuration (and the device) once up front; the order comes with each
+  // request, so the probe takes one the basis is compiled for if cfg->P is not
+  fmm_b200_config pc = *cfg;
+  int ords[64];
+  const int nord = std::min(fmm_b200_supported_orders(pc.basis, ords, 64), 64);
+  if (nord > 0 && std::find(ords, ords + nord, pc.P) == ords + nord) pc.P = ords[0];
   fmm_b200_solver* probe = nullptr;
-  int rc = fmm_b200_create(cfg, &probe);
+  int rc = fmm_b200_create(&pc, &probe);
   if (rc != FMM_OK) return rc;
   fmm_b200_destroy(probe);
   fmm_b200_server* S = new fmm_b200_server();

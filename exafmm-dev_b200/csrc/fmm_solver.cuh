@@ -122,7 +122,7 @@ struct SolverBase {
   int* scal_host = nullptr;  // pinned mirror of scal
   // cells
   DevArr<int> c_iparent, c_ichild, c_nchild, c_ibody, c_nbody, c_level;
-  DevArr<int4> c_info;  // per cell (NCHILD, ICHILD, NBODY, 0): one load for the traversal
+  DevArr<int4> c_info;  // per cell (NCHILD, ICHILD, NBODY, IBODY): one load for the traversal
   DevArr<unsigned long long> c_icell;
   DevArr<int> order;
   // interaction lists
@@ -143,6 +143,13 @@ struct SolverBase {
   // (target root, source root) only (fmm_b200_solve_ij_*)
   bool ij = false;
   bool ij_common_box = true;  // else each tree on its own bodies' box (the petiga wrapper)
+  // target partition of one solve over nparts GPUs (fmm_b200_set_partition): the bodies of
+  // part `part` in tree order, [part_range[0], part_range[1]), set on the device after the
+  // tree build; the traversal keeps the pairs whose target cell holds some of them, and L2L
+  // and L2P run on the cells and bodies of the part only
+  int part = 0, nparts = 1;
+  DevArr<int> part_range;
+  const int* part_ptr() const { return nparts > 1 ? part_range.p : nullptr; }
   int nfront0 = 0;          // pairs of the first traversal step (roots x images)
   DevArr<unsigned long long> m2l, p2p, list_tmp;
   DevArr<int> m2l_off, p2p_off;
@@ -188,6 +195,7 @@ template <typename T> struct Solver : SolverBase {
 
 // ---- stage implementations (one translation unit each) ---------------------------------
 template <typename T> void build_tree(Solver<T>& s);          // fmm_tree.cu
+void partition_range(SolverBase& s);                         // fmm_tree.cu: part_range
 long long count_p2p_body_pairs(SolverBase& s);              // fmm_traverse.cu
 template <typename T> void upward_pass(Solver<T>& s);         // fmm_passes.cu
 template <typename T> void upward_expansions(Solver<T>& s);   // fmm_passes.cu: P2M, M2M

@@ -229,13 +229,15 @@ __device__ __forceinline__ void l2l_passes(const T* yr, const T* yi, const T* Lp
 template <typename T, int P>
 __global__ void __launch_bounds__(tr_threads<T>())
     k_l2l_reg(int lo, int hi, const int* __restrict__ npos, const int* __restrict__ iparent,
-              const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef) {
+              const vec4<T>* __restrict__ cX, T* __restrict__ L, int ncoef,
+              const int4* __restrict__ info, const int* __restrict__ range) {
   constexpr int NT = sph::NT(P), STR = (2 * NT) | 1;
   __shared__ T rows[tr_threads<T>() * STR];
   T* row = rows + threadIdx.x * STR;
   const int v = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= hi) return;
   const int c = npos[v];
+  if (range && !part_holds(info[c], range)) return;  // no body of this part below the cell
   const int p = iparent[c];
   const T* src = L + (size_t)p * ncoef;
 #pragma unroll
@@ -404,9 +406,11 @@ template <typename T, int P>
 __global__ void __launch_bounds__(128)
     k_l2p_bodies(int n, const int* __restrict__ body_leaf, const vec4<T>* __restrict__ cX,
                  const vec4<T>* __restrict__ bodies, const T* __restrict__ L, int ncoef,
-                 vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e) {
+                 vec4<T>* __restrict__ trg_s, vec4<T>* __restrict__ trg_e,
+                 const int* __restrict__ range) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (range && (i < range[0] || i >= range[1])) return;  // another part's body
   const int c = body_leaf[i];
   if (c < 0) return;  // a body outside the cells of a single-operator call
   const vec4<T> C = cX[c];
@@ -444,13 +448,15 @@ template <typename T, int P> static void m2l_(Solver<T>& s) { launch_m2l_passes<
 template <typename T, int P> static void l2l_(Solver<T>& s, int lo, int hi) {
   constexpr int NTH = tr_threads<T>();
   k_l2l_reg<T, P><<<ceil_div(hi - lo, NTH), NTH, 0, s.stream>>>(lo, hi, s.npos.p, s.c_iparent.p,
-                                                                s.cX.p, s.L.p, s.ncoef);
+                                                                s.cX.p, s.L.p, s.ncoef,
+                                                                s.c_info.p, s.part_ptr());
   FMM_LAUNCH_CHECK();
 }
 template <typename T, int P> static void l2p_(Solver<T>& s) {
   if (!s.nleaves) return;
   k_l2p_bodies<T, P><<<ceil_div(s.n, 128), 128, 0, s.stream>>>(
-      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p);
+      s.n, s.body_leaf.p, s.cX.p, s.bodies.p, s.L.p, s.ncoef, s.trg_s.p, s.trg_e.p,
+      s.part_ptr());
   FMM_LAUNCH_CHECK();
 }
 

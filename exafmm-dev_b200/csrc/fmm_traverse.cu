@@ -19,6 +19,7 @@
 namespace fmmb200 {
 
 enum {
+  PAIR_DROP = -1,  // a partitioned solve: the target cell holds none of the part's bodies
   PAIR_M2L = 0, PAIR_P2P = 1, PAIR_SPLIT_I = 2, PAIR_SPLIT_J = 3, PAIR_SPLIT_IJ = 4,
   PAIR_SPLIT_SELF = 5  // mutual: a cell against itself, its children pairs (a, b), a <= b
 };
@@ -30,17 +31,24 @@ enum {
 // a cell against itself always splits both sides (:200), and an M2L or a P2P between two
 // different cells is emitted in both directions (the mutual kernels update both cells);
 // *nout counts those outputs
-// The pair's cell data (centres with radii, and (NCHILD, ICHILD, NBODY)) are loaded
+// The pair's cell data (centres with radii, and (NCHILD, ICHILD, NBODY, IBODY)) are loaded
 // together, so that a pair costs one round trip to memory rather than one per decision.
+// A partitioned solve drops the pairs whose target cell holds none of the bodies [b0, b1):
+// every pair below them has a target inside that cell, so the pairs kept are exactly the
+// whole traversal's pairs of the part's targets (b0 = INT_MIN, b1 = INT_MAX keep all).
 template <typename T>
 __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
                                         const int4* __restrict__ info, int nspawn, T cycle,
-                                        int mutual, int* nout) {
+                                        int mutual, int b0, int b1, int* nout) {
   const int cj = pair_cell((unsigned)cjp);
   T px, py, pz;
   img_shift<T>(pair_img((unsigned)cjp), cycle, px, py, pz);
   const vec4<T> a = X[ci], b = X[cj];
   const int4 fi = info[ci], fj = info[cj];
+  if (!(fi.w < b1 && fi.w + fi.z > b0)) {
+    *nout = 0;
+    return PAIR_DROP;
+  }
   T R2 = norm_rn(sub_rn(sub_rn(a.x, b.x), px), sub_rn(sub_rn(a.y, b.y), py),
                  sub_rn(sub_rn(a.z, b.z), pz));
   T Rs = add_rn(a.w, b.w);
@@ -78,16 +86,28 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
 }
 
 // pass 1: per-block totals of (M2L, P2P, children) added to three device counters
+// the part's body range [range[0], range[1]) of a partitioned solve, else everything
+__device__ __forceinline__ void part_bounds(const int* __restrict__ range, int& b0, int& b1) {
+  b0 = INT_MIN;
+  b1 = INT_MAX;
+  if (range) {
+    b0 = range[0];
+    b1 = range[1];
+  }
+}
+
 template <typename T>
 __global__ void k_trav_count(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int4* __restrict__ info,
-                             int nspawn, T cycle, int mutual,
+                             int nspawn, T cycle, int mutual, const int* __restrict__ range,
                              unsigned long long* __restrict__ counters) {
+  int b0, b1;
+  part_bounds(range, b0, b1);
   unsigned long long c[3] = {0, 0, 0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
     int2 p = front[t];
     int k;
-    int ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, &k);
+    int ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, b0, b1, &k);
     c[ty == PAIR_M2L ? 0 : ty == PAIR_P2P ? 1 : 2] += k;
   }
   for (int i = 0; i < 3; i++) {
@@ -118,10 +138,12 @@ __device__ __forceinline__ unsigned long long warp_alloc(unsigned long long* cou
 template <typename T>
 __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
                              const vec4<T>* __restrict__ X, const int4* __restrict__ info,
-                             int nspawn, T cycle, int mutual,
+                             int nspawn, T cycle, int mutual, const int* __restrict__ range,
                              unsigned long long* __restrict__ counters,
                              unsigned long long* __restrict__ m2l,
                              unsigned long long* __restrict__ p2p, int2* __restrict__ next) {
+  int b0, b1;
+  part_bounds(range, b0, b1);
   const int stride = gridDim.x * blockDim.x;
   // every lane of a warp runs the same number of iterations (warp-uniform trip count)
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -132,7 +154,7 @@ __global__ void k_trav_write(const int2* __restrict__ front, int nfront,
     int2 p = make_int2(0, 0);
     if (t < nfront) {
       p = front[t];
-      ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, &k);
+      ty = classify<T>(p.x, p.y, X, info, nspawn, cycle, mutual, b0, b1, &k);
     }
     const unsigned long long packed = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
     // the reverse of a mutual pair (no periodic image with mutual)
@@ -180,12 +202,15 @@ __global__ void __launch_bounds__(256)
     k_trav_step(const int2* __restrict__ front, const unsigned long long* __restrict__ nfront_p,
                 unsigned long long front_cap, const vec4<T>* __restrict__ X,
                 const int4* __restrict__ info, int nspawn, T cycle, int mutual, int ncells,
+                const int* __restrict__ range,
                 unsigned long long* __restrict__ ctr,  // [0] M2L, [1] P2P, [2] bad index
                 unsigned long long* __restrict__ next_count, unsigned long long* __restrict__ m2l,
                 unsigned long long m2l_cap, unsigned long long* __restrict__ p2p,
                 unsigned long long p2p_cap, int2* __restrict__ next,
                 unsigned long long next_cap) {
   const long long nfront = (long long)min(*nfront_p, front_cap);
+  int b0, b1;
+  part_bounds(range, b0, b1);
   const int lane = lane_id();
   const long long stride = (long long)gridDim.x * blockDim.x * kTravItems;
   const long long wbase =
@@ -208,7 +233,7 @@ __global__ void __launch_bounds__(256)
         if ((unsigned)p[u].x < (unsigned)ncells &&
             (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
             pair_img((unsigned)p[u].y) < 27)
-          ty[u] = classify<T>(p[u].x, p[u].y, X, info, nspawn, cycle, mutual, &k[u]);
+          ty[u] = classify<T>(p[u].x, p[u].y, X, info, nspawn, cycle, mutual, b0, b1, &k[u]);
         else
           atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
       }
@@ -594,7 +619,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     int grid = std::min(ceil_div(nfront, TB), 148 * 16);
     k_trav_count<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_info.p,
                                                s.cfg.nspawn, (T)s.cfg.cycle,
-                                               mutual_of(s), cnt);
+                                               mutual_of(s), s.part_ptr(), cnt);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaMemcpyAsync(hc, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s.stream));
@@ -621,7 +646,7 @@ static long long counted_traversal(Solver<T>& s, long long& nm2l, long long& np2
     FMM_CUDA(cudaMemcpyAsync(cnt, base, sizeof(base), cudaMemcpyHostToDevice, s.stream));
     k_trav_write<T><<<grid, TB, 0, s.stream>>>(s.front.p, (int)nfront, s.cX.p, s.c_info.p,
                                                s.cfg.nspawn,
-                                               (T)s.cfg.cycle, mutual_of(s), cnt,
+                                               (T)s.cfg.cycle, mutual_of(s), s.part_ptr(), cnt,
                                                s.m2l.p, s.p2p.p, s.front2.p);
     FMM_LAUNCH_CHECK();
     FMM_CUDA(cudaStreamSynchronize(s.stream));  // base[] lives on the host stack
@@ -664,7 +689,8 @@ static bool fast_traversal(Solver<T>& s, long long& nm2l, long long& np2p) {
     DevArr<int2>& out = (l & 1) ? s.front : s.front2;
     k_trav_step<T><<<148 * 8, TB, 0, s.stream>>>(
         in.p, ctr + 3 + l, fcap, s.cX.p, s.c_info.p,
-        s.cfg.nspawn, (T)s.cfg.cycle, mutual_of(s), s.ncells, ctr, ctr + 4 + l, s.m2l.p,
+        s.cfg.nspawn, (T)s.cfg.cycle, mutual_of(s), s.ncells, s.part_ptr(), ctr, ctr + 4 + l,
+        s.m2l.p,
         s.m2l.cap, s.p2p.p,
         s.p2p.cap,
         out.p, fcap);

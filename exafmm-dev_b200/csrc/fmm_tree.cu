@@ -399,12 +399,12 @@ __global__ void k_pos(int lo, int hi, const int* __restrict__ nchildn,
   }
 }
 
-// (NCHILD, ICHILD, NBODY) of every cell in one 16-byte record, for the traversal
+// (NCHILD, ICHILD, NBODY, IBODY) of every cell in one 16-byte record, for the traversal
 __global__ void k_cell_info(int ncells, const int* __restrict__ nchild,
                             const int* __restrict__ ichild, const int* __restrict__ nbody,
-                            int4* __restrict__ info) {
+                            const int* __restrict__ ibody, int4* __restrict__ info) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < ncells) info[c] = make_int4(nchild[c], ichild[c], nbody[c], 0);
+  if (c < ncells) info[c] = make_int4(nchild[c], ichild[c], nbody[c], ibody[c]);
 }
 
 // Cell records (Nodes2cells::operator(), include/build_tree_tbb.h:250-262) with the
@@ -808,7 +808,7 @@ template <typename T> static void build_uniform(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
   s.c_info.ensure(nc);
   k_cell_info<<<ceil_div(nc, TB), TB, 0, s.stream>>>(nc, s.c_nchild.p, s.c_ichild.p,
-                                                     s.c_nbody.p, s.c_info.p);
+                                                     s.c_nbody.p, s.c_ibody.p, s.c_info.p);
   FMM_LAUNCH_CHECK();
   // the level passes walk cells level by level: node v is cell v (npos the identity), the
   // cells of level l at [nc - end[l], nc - begin[l]); every leaf is on the deepest level
@@ -999,7 +999,7 @@ template <typename T> void build_tree(Solver<T>& s) {
   FMM_LAUNCH_CHECK();
   s.c_info.ensure(nnodes);
   k_cell_info<<<ceil_div(nnodes, TB), TB, 0, s.stream>>>(nnodes, s.c_nchild.p, s.c_ichild.p,
-                                                         s.c_nbody.p, s.c_info.p);
+                                                         s.c_nbody.p, s.c_ibody.p, s.c_info.p);
   FMM_LAUNCH_CHECK();
   // bodies inside a leaf in input order (the stable partitions of the reference keep it)
   s.order.ensure(n);
@@ -1042,6 +1042,37 @@ template <typename T> void build_tree(Solver<T>& s) {
                            cudaMemcpyDeviceToHost, s.stream));
   FMM_CUDA(cudaStreamSynchronize(s.stream));
   s.nleaves = s.scal_host[0];
+}
+
+// The bodies of part `part` of nparts: [t0, t1) with t = floor(k n / nparts), each bound
+// moved down to the first body of the leaf that holds it, so that every leaf belongs to one
+// part.  One leaf holds each bound below n and writes it; the leaf that ends at n writes
+// the bound n.
+__global__ void k_part_range(int nleaves, const int* __restrict__ leaves,
+                             const int* __restrict__ ibody, const int* __restrict__ nbody, int n,
+                             int t0, int t1, int* __restrict__ range) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nleaves) return;
+  const int c = leaves[i];
+  const int b = ibody[c], e = b + nbody[c];
+  if (b <= t0 && t0 < e) range[0] = b;
+  if (b <= t1 && t1 < e) range[1] = b;
+  if (t1 >= n && e == n) range[1] = n;
+}
+
+void partition_range(SolverBase& s) {
+  if (s.nparts <= 1) return;
+  if (s.nroots > 1 || s.ij)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED, "a partitioned solve is one solve of one tree");
+  if (s.cfg.mutual && s.cfg.images == 0)
+    throw FmmError(FMM_ERR_NOT_SUPPORTED, "a partitioned solve with the mutual traversal");
+  s.part_range.ensure(2);
+  if (s.n == 0 || s.nleaves == 0) return;
+  const int t0 = (int)((long long)s.part * s.n / s.nparts);
+  const int t1 = (int)((long long)(s.part + 1) * s.n / s.nparts);
+  k_part_range<<<ceil_div(s.nleaves, 256), 256, 0, s.stream>>>(
+      s.nleaves, s.leaves.p, s.c_ibody.p, s.c_nbody.p, s.n, t0, t1, s.part_range.p);
+  FMM_LAUNCH_CHECK();
 }
 
 template void build_tree<float>(Solver<float>&);

@@ -111,6 +111,26 @@ int fmm_b200_trim(fmm_b200_solver* s);
 int fmm_b200_set_periodic(fmm_b200_solver* s, int images, double cycle);
 /* mutual flag of the next traversals (dualTreeTraversal's mutual argument) */
 int fmm_b200_set_mutual(fmm_b200_solver* s, int mutual);
+/* One solve over nparts GPUs, one handle per GPU, every handle given the same bodies: the
+ * handle computes the results of part `part` only.  After the tree build its bodies (tree
+ * order) are cut into nparts ranges of about n / nparts bodies, each cut moved down to the
+ * start of the leaf that holds it; the traversal keeps the pairs whose target cell holds
+ * bodies of this part (exactly the whole traversal's pairs for those targets), M2L and P2P
+ * run on them, L2L on the cells that hold bodies of this part, L2P on this part's bodies,
+ * and the other bodies' results are 0.  The tree and the upward pass are computed on every
+ * handle.  The sum of the nparts results (an all-reduce, or a reduce-scatter to the bodies'
+ * owners) is the one-GPU solve's result, bit for bit.  Whole single solves with an open or
+ * periodic boundary (FMM_ERR_NOT_SUPPORTED for batches, separate target/source sets and the
+ * mutual traversal).  nparts = 1 (the default) computes every body.  The reference spreads
+ * a solve over MPI ranks by an ORB partition of the bodies plus the exchange of a local
+ * essential tree (include/partition.h:69-195, include/tree_mpi.h:225-369); this replaces the
+ * exchange by replicated bodies and tree, for the GPUs of one node, each with room for all
+ * the bodies.  The single-operator calls (fmm_b200_kernel_*) ignore the partition. */
+int fmm_b200_set_partition(fmm_b200_solver* s, int part, int nparts);
+/* The handle's part and nparts, and after a solve this part's bodies [begin, end) in tree
+ * order (0, n when nparts = 1); any pointer may be NULL. */
+int fmm_b200_get_partition(fmm_b200_solver* s, int* part, int* nparts, int* body_begin,
+                           int* body_end);
 /* Message of the last failure on this handle (or of the last failed create if s is NULL). */
 const char* fmm_b200_last_error(const fmm_b200_solver* s);
 /* Which P values were compiled for a basis: writes up to cap values, returns the count. */
@@ -261,10 +281,12 @@ int fmm_b200_autotune_p2p(fmm_b200_solver* s, const int* lanes4_max, const int* 
 /* ---- serving: continuous batching of independent solves ------------------------------ *
  * A server owns nworkers worker threads (one CUDA stream and one solver handle per order
  * each) and a scheduler that batches pending requests of equal order P, in arrival order,
- * within hbm_budget_bytes of estimated device memory and max_batch solves per batch.
- * Batches on different workers overlap on the device; a request arriving while batches
- * run joins the next batch a worker takes.  cfg supplies basis, theta, ncrit, nspawn,
- * precision and device; P comes with each request.  submit copies the inputs; wait blocks
+ * within hbm_budget_bytes of estimated device memory, max_batch solves and 2^21 bodies
+ * per batch (a larger request rides alone).  Each worker holds pinned host staging for
+ * 2^21 bodies (128 MB) from the start.  Batches on different workers overlap on the device;
+ * a request arriving while batches run joins the next batch a worker takes.  cfg supplies
+ * basis, theta, ncrit, nspawn, precision and device (its P need not be compiled for the
+ * basis); P comes with each request.  submit copies the inputs; wait blocks
  * until the request is done, copies p (n) and f (3n), and reports its latency (submit to
  * done) and queueing time (submit to batch start) in seconds.  A request whose estimate
  * exceeds the whole budget is rejected with FMM_ERR_NO_MEMORY.  destroy drains the queue.

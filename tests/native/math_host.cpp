@@ -84,24 +84,31 @@ template <int P> void cart_m2l(const double* Xi, const double* Xj, const double*
   cart::derivs<double, P>(C, dx, dy, dz, invR2, std::sqrt(invR2));
   cart::m2l_pair<double, P>(C, Mj, Li);
 }
+// runtime-index terms and the unrolled per-child forms (the kernels) agree exactly
 template <int P> void cart_m2m(const double* Xp, const double* Xc, const double* Mc, double* Mp) {
-  double C[cart::NT(P)];
+  double C[cart::NT(P)], unr[cart::NT(P)] = {};
   C[0] = 1;
   cart::power<double, P>(C, Xp[0] - Xc[0], Xp[1] - Xc[1], Xp[2] - Xc[2]);
+  cart::m2m_child<double, P>(C, Mc, unr);
   for (int t = 0; t < cart::NT(P); t++) {
     int nx, ny, nz;
     cart::mi_of(t, nx, ny, nz);
-    Mp[t] += cart::m2m_term<double>(nx, ny, nz, C, Mc);
+    const double v = cart::m2m_term<double>(nx, ny, nz, C, Mc);
+    Mp[t] += v;
+    if (v != unr[t]) Mp[t] += 1e300;  // must agree exactly
   }
 }
 template <int P> void cart_l2l(const double* Xc, const double* Xp, const double* Lp, double* Lc) {
-  double C[cart::NT(P)];
+  double C[cart::NT(P)], unr[cart::NT(P)] = {};
   C[0] = 1;
   cart::power<double, P>(C, Xc[0] - Xp[0], Xc[1] - Xp[1], Xc[2] - Xp[2]);
+  cart::l2l_child<double, P>(C, Lp, unr);
   for (int t = 0; t < cart::NT(P); t++) {
     int nx, ny, nz;
     cart::mi_of(t, nx, ny, nz);
-    Lc[t] += cart::l2l_term<double>(P, nx, ny, nz, C, Lp);
+    const double v = cart::l2l_term<double>(P, nx, ny, nz, C, Lp);
+    Lc[t] += v;
+    if (v != unr[t]) Lc[t] += 1e300;  // must agree exactly
   }
 }
 template <int P> void cart_p2m(const double* Xc, int nb, const double* xq, double* M) {

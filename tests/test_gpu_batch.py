@@ -136,3 +136,30 @@ def test_server_rejects_requests_beyond_budget(datasets):
     with pytest.raises(fmm.FmmError):
         srv.submit(x[:10], q[:10], 3)  # order not compiled
     srv.close()
+
+
+@pytest.mark.parametrize("basis,prec,orders", [("cartesian", "f32", (4, 5)),
+                                                ("spherical", "f64", (6, 8))])
+def test_server_other_bases_and_precisions(basis, prec, orders, datasets):
+    """The serving loop on the Cartesian basis (whose compiled orders do not include the
+    configuration's default P = 10) and in FP64: every result bitwise the same request
+    solved alone."""
+    rng = np.random.default_rng(9)
+    reqs = []
+    for i in range(12):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(30000))))
+        P = int(orders[i % len(orders)])
+        x, q = datasets.make(("cube", "plummer")[i % 2], n, seed=700 + i, precision=prec)
+        reqs.append((x, q, P))
+    srv = fmm.Server(basis=basis, theta=0.45, ncrit=32, use_ropt=0, precision=prec,
+                     hbm_budget_gb=8.0, workers=2, max_batch=8)
+    ids = [(k, srv.submit(x, q, P)) for k, (x, q, P) in enumerate(reqs)]
+    results = {k: srv.wait(rid)[0] for k, rid in ids}
+    srv.close()
+    solvers = {}
+    for k, (x, q, P) in enumerate(reqs):
+        s = solvers.setdefault(P, fmm.Solver(basis=basis, P=P, theta=0.45, ncrit=32,
+                                             use_ropt=0, precision=prec))
+        ref = s.solve(x, q)
+        ok = ~np.isnan(ref)
+        assert np.array_equal(results[k][ok], ref[ok]), k

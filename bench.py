@@ -28,6 +28,10 @@ use_rmax = use_ropt = 1, FP32 expansions with compensated potential/gradient sum
   accuracy vs FP64 direct, and the reference CPU build on the same config.
 * multi-GPU (torchrun): replicas only; every rank solves its own instance, no collective
   on the data path (a barrier and a max-reduction of the timings only).
+* --strong (torchrun): one headline solve per step over all ranks through
+  exafmm-dev_b200.distributed (all_gather of the bodies, a partitioned solve per GPU,
+  reduce_scatter of the results), "scaling": "strong", value = N / step time (max over
+  ranks).  The default multi-rank run stays replicas.
 * partitioned (rank 0): the headline solve split by target parts for 2, 4 and 8 GPUs of a
   node (exafmm-dev_b200.distributed), the parts run in turn on this GPU: per-part device
   time, the slowest part plus the collectives' estimate, and the parts' sum checked bit for
@@ -607,6 +611,76 @@ def bench_cartesian(fmm, datasets, torch, dev, stream, flush, device, steps, clk
     return res
 
 
+def bench_strong(args, fmm, datasets, torch, pg, world, rank, local):
+    """--strong: one headline solve per step over all ranks (exafmm-dev_b200.distributed):
+    each rank owns a contiguous 1/world of the bodies; a step is the all_gather of the
+    bodies, the rank's partitioned solve and the reduce_scatter of the results, timed with
+    CUDA events on the rank's stream, max over ranks.  value = N / step time."""
+    dmod = importlib.import_module("exafmm-dev_b200.distributed")
+    dev = torch.device("cuda", local)
+    n = args.n
+    x, q = datasets.make(WORKLOAD["dist"], n, seed=43, precision="f32")
+    lo, hi = rank * n // world, (rank + 1) * n // world
+    mine = torch.tensor(np.concatenate([x[lo:hi], q[lo:hi, None]], axis=1),
+                        dtype=torch.float32, device=dev)
+    kw = {k: WORKLOAD[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax",
+                                   "use_ropt")}
+    if pg is None:  # one rank: a process group of one, so that the same collectives run
+        import torch.distributed as dist
+        if "RANK" in os.environ:  # under torchrun: its rendezvous
+            dist.init_process_group("nccl", device_id=dev)
+        else:
+            import socket
+            with socket.socket() as so:
+                so.bind(("127.0.0.1", 0))
+                port = so.getsockname()[1]
+            dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                                    world_size=1, device_id=dev)
+        pg = dist
+    ds = dmod.DistributedSolver(precision="f32", device=local, **kw)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    out = None
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            out = ds.solve(mine)
+    torch.cuda.synchronize()
+    pg.barrier()
+    torch.cuda.synchronize()
+    ms = []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = ds.solve(mine)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    pg.barrier()
+    t = torch.tensor([float(np.mean(ms))], device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    step_ms = float(t.item())
+    idx = datasets.sample_targets(hi - lo, min(1024, hi - lo))
+    trg = out.cpu().numpy().astype(np.float64)
+    dref = fmm.direct(x[lo:hi][idx], x, q, device=local)
+    err_pot = float(np.sqrt(((trg[idx, 0] - dref[:, 0]) ** 2).sum() / (dref[:, 0] ** 2).sum()))
+    err_acc = float(np.sqrt(((trg[idx, 1:] - dref[:, 1:]) ** 2).sum() / (dref[:, 1:] ** 2).sum()))
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": n / (step_ms * 1e-3), "unit": "particles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded Plummer sphere (a=1, r<10a, recentred), q = 1/N",
+            "config": {"workload": WORKLOAD_NAME, "n_bodies": n, "parallelism":
+                       "target parts of one tree over %d GPUs (all_gather, partitioned solve, "
+                       "reduce_scatter)" % world,
+                       "l2": "256 MB flush before each timed step"},
+            "accuracy": {"rel_l2_pot": err_pot, "rel_l2_acc": err_acc,
+                         "targets": len(idx), "reference": "FP64 direct sum on the GPU"}}))
+    pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -619,6 +693,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop line")
+    ap.add_argument("--strong", action="store_true",
+                    help="one headline solve over all ranks (target parts), not replicas")
     ap.add_argument("--no-partition", action="store_true",
                     help="skip the solve split by target parts (one node of GPUs, emulated)")
     ap.add_argument("--no-cart", action="store_true",
@@ -646,6 +722,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
         pg = dist
+    if args.strong:
+        return bench_strong(args, fmm, datasets, torch, pg, world, rank, local)
     dev = torch.device("cuda", local)
     n = args.n
     wl = CART if args.profile and args.profile_workload == "cartesian" else WORKLOAD

@@ -76,16 +76,23 @@ class DistributedSolver:
         if nmax == 0:
             return torch.zeros_like(bodies)
         # every rank's bodies in one block of nmax rows (all_gather takes equal sizes)
-        pad = torch.zeros((nmax, 4), dtype=bodies.dtype, device=dev)
-        pad[:n_local] = bodies
+        if n_local == nmax:
+            pad = bodies
+        else:
+            pad = torch.zeros((nmax, 4), dtype=bodies.dtype, device=dev)
+            pad[:n_local] = bodies
         gathered = torch.empty((self.world * nmax, 4), dtype=bodies.dtype, device=dev)
         dist.all_gather_into_tensor(gathered, pad, group=self.group)
+        mine = torch.empty_like(pad)
+        if all(c == nmax for c in counts):  # no padding: the gathered block is the bodies
+            trg = self.compute(gathered, self.rank, self.world)
+            dist.reduce_scatter_tensor(mine, trg, op=dist.ReduceOp.SUM, group=self.group)
+            return mine
         rows = torch.cat([torch.arange(r * nmax, r * nmax + counts[r], device=dev)
                           for r in range(self.world)])
         all_bodies = gathered[rows].contiguous()  # rank order, the padding left out
         trg = self.compute(all_bodies, self.rank, self.world)
         out = torch.zeros_like(gathered)
         out[rows] = trg
-        mine = torch.empty_like(pad)
         dist.reduce_scatter_tensor(mine, out, op=dist.ReduceOp.SUM, group=self.group)
         return mine[:n_local]

@@ -706,6 +706,9 @@ def main():
                     help="working precision of the --profile solve")
     ap.add_argument("--profile-workload", default="headline", choices=["headline", "cartesian"],
                     help="--profile solve: the headline workload, or the Cartesian P = 5 one")
+    ap.add_argument("--profile-parts", type=int, default=1,
+                    help="--profile solve: part 0 of this many target parts (one GPU's share "
+                         "of a solve split over a node)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     datasets = importlib.import_module("exafmm-dev_b200.datasets")
@@ -733,6 +736,8 @@ def main():
     kw = {k: wl[k] for k in ("basis", "P", "theta", "ncrit", "nspawn", "use_rmax", "use_ropt")}
     prec = args.profile_precision if args.profile else "f32"
     solver = fmm.Solver(precision=prec, device=local, **kw)
+    if args.profile and args.profile_parts > 1:
+        solver.set_partition(0, args.profile_parts)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
     bodies = torch.tensor(np.concatenate([x, q[:, None]], axis=1),
@@ -758,6 +763,7 @@ def main():
         if rank == 0:
             print(json.dumps({"profile": CART_NAME if wl is CART else WORKLOAD_NAME,
                               "n_bodies": n, "precision": prec,
+                              "parts": args.profile_parts,
                               "phases_ms": solver.timings(), "lists": solver.list_counts()}))
         return
     if pg:

@@ -24,7 +24,33 @@ template <> __device__ __forceinline__ double tmax<double>() { return DBL_MAX; }
 
 // ---------------------------------------------------------------- bounds
 // BoundBox::getBounds (include/bound_box.h:76-88): elementwise min / max of positions, per
-// chunk of one root's bodies (one block per chunk), then per root.
+// chunk of one root's bodies (one block per chunk), then per root (one block per root).
+// Min and max are exact whatever the order in which values meet.
+
+// the block's min / max of mn, mx (per thread) into thread 0's mn, mx
+template <typename T> __device__ __forceinline__ void block_minmax(T* mn, T* mx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T a = __shfl_xor_sync(0xffffffffu, mn[d], o);
+      T c = __shfl_xor_sync(0xffffffffu, mx[d], o);
+      mn[d] = a < mn[d] ? a : mn[d];
+      mx[d] = c > mx[d] ? c : mx[d];
+    }
+  __shared__ T sh[32][6];
+  int w = threadIdx.x >> 5;
+  if (lane_id() == 0)
+    for (int d = 0; d < 3; d++) sh[w][d] = mn[d], sh[w][3 + d] = mx[d];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+      for (int d = 0; d < 3; d++) {
+        mn[d] = sh[k][d] < mn[d] ? sh[k][d] : mn[d];
+        mx[d] = sh[k][3 + d] > mx[d] ? sh[k][3 + d] : mx[d];
+      }
+}
+
 template <typename T>
 __global__ void k_minmax_chunks(const vec4<T>* __restrict__ b, const int* __restrict__ cb,
                                 const int* __restrict__ ce, T* __restrict__ part) {
@@ -40,48 +66,31 @@ __global__ void k_minmax_chunks(const vec4<T>* __restrict__ b, const int* __rest
     mx[1] = p.y > mx[1] ? p.y : mx[1];
     mx[2] = p.z > mx[2] ? p.z : mx[2];
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      T a = __shfl_xor_sync(0xffffffffu, mn[d], o);
-      T c = __shfl_xor_sync(0xffffffffu, mx[d], o);
-      mn[d] = a < mn[d] ? a : mn[d];
-      mx[d] = c > mx[d] ? c : mx[d];
-    }
-  __shared__ T sh[32][6];
-  int w = threadIdx.x >> 5;
-  if (lane_id() == 0)
-    for (int d = 0; d < 3; d++) sh[w][d] = mn[d], sh[w][3 + d] = mx[d];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 1; k < (int)(blockDim.x >> 5); k++)
-      for (int d = 0; d < 3; d++) {
-        mn[d] = sh[k][d] < mn[d] ? sh[k][d] : mn[d];
-        mx[d] = sh[k][3 + d] > mx[d] ? sh[k][3 + d] : mx[d];
-      }
+  block_minmax(mn, mx);
+  if (threadIdx.x == 0)
     for (int d = 0; d < 3; d++) part[6 * blockIdx.x + d] = mn[d], part[6 * blockIdx.x + 3 + d] = mx[d];
-  }
 }
 
-// BuildTree::bounds2box (include/build_tree_tbb.h:298-310), one thread per root;
-// box[16 r ..] = X0[3], R0, Xmin[3], Xmax[3]
+// BuildTree::bounds2box (include/build_tree_tbb.h:298-310), one block per root over the
+// root's chunk bounds; box[16 r ..] = X0[3], R0, Xmin[3], Xmax[3]
 template <typename T>
 __global__ void k_box(int nroots, const int* __restrict__ chunk_lo, const T* __restrict__ part,
                       int shared, T* __restrict__ box) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.x;
   if (r >= nroots) return;
   // shared: every root takes the box of the bounds of all bodies (BoundBox::getBounds of
   // the targets, then of the sources with those bounds, include/bound_box.h:91-97)
   const int c0 = shared ? chunk_lo[0] : chunk_lo[r], c1 = shared ? chunk_lo[nroots] : chunk_lo[r + 1];
-  T mn[3], mx[3];
-  for (int d = 0; d < 3; d++) mn[d] = part[6 * c0 + d], mx[d] = part[6 * c0 + 3 + d];
-  for (int k = c0 + 1; k < c1; k++)
+  T mn[3] = {tmax<T>(), tmax<T>(), tmax<T>()};
+  T mx[3] = {-tmax<T>(), -tmax<T>(), -tmax<T>()};
+  for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x)
     for (int d = 0; d < 3; d++) {
       T a = part[6 * k + d], c = part[6 * k + 3 + d];
       mn[d] = a < mn[d] ? a : mn[d];
       mx[d] = c > mx[d] ? c : mx[d];
     }
+  block_minmax(mn, mx);
+  if (threadIdx.x != 0) return;
   T X[3], R = 0;
   for (int d = 0; d < 3; d++) X[d] = div_rn(add_rn(mx[d], mn[d]), (T)2);
   for (int d = 0; d < 3; d++) {
@@ -113,9 +122,12 @@ __global__ void k_keys(const vec4<T>* __restrict__ b, int n, const T* __restrict
   vec4<T> p = b[i];
   T c0 = bx[0], c1 = bx[1], c2 = bx[2], R0 = bx[3];
   unsigned long long key = 0;
-#pragma unroll 1
+  T sc = T(0.5);  // 2^-(l+1), exact
   for (int l = 0; l < kMaxLevel; l++) {
-    T r = div_rn(R0, (T)(1 << (l + 1)));
+    // R0 / 2^(l+1) as the product with 2^-(l+1): the same real number, so the same
+    // rounding as the reference's division
+    T r = mul_rn(R0, sc);
+    sc = mul_rn(sc, T(0.5));
     int o = (p.x > c0) | ((p.y > c1) << 1) | ((p.z > c2) << 2);
     key = (key << 3) | (unsigned)o;
     c0 = add_rn(c0, (o & 1) ? r : -r);
@@ -859,8 +871,8 @@ template <typename T> void build_tree(Solver<T>& s) {
     s.root_cell.clear();
     return;
   }
-  // bounds per root over chunks of at most 16384 bodies
-  const int CH = 16384;
+  // bounds per root over chunks of at most 4096 bodies (256 blocks at 2^20 bodies)
+  const int CH = 4096;
   std::vector<int> hb, he, hlo{0};
   for (int r = 0; r < nroots; r++) {
     for (int b0 = rfirst[r]; b0 < rfirst[r + 1]; b0 += CH) {
@@ -884,8 +896,8 @@ template <typename T> void build_tree(Solver<T>& s) {
   s.minmax_part.ensure(6 * (size_t)nch);
   k_minmax_chunks<T><<<nch, TB, 0, s.stream>>>(s.bodies_in.p, dcb, dce, s.minmax_part.p);
   FMM_LAUNCH_CHECK();
-  k_box<T><<<ceil_div(nroots, TB), TB, 0, s.stream>>>(
-      nroots, dlo, s.minmax_part.p, s.ij && s.ij_common_box ? 1 : 0, s.box.p);
+  k_box<T><<<nroots, TB, 0, s.stream>>>(nroots, dlo, s.minmax_part.p,
+                                        s.ij && s.ij_common_box ? 1 : 0, s.box.p);
   FMM_LAUNCH_CHECK();
   phase_end(s, FMM_PHASE_BOUNDS);
   phase_begin(s, FMM_PHASE_TREE);

@@ -104,6 +104,7 @@ SIGNATURES = {
     "fmm_b200_server_stats": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "fmm_b200_server_profile": (_i, [_vp, _vp, _vp, _vp]),
     "fmm_b200_server_destroy": (_i, [_vp]),
+    "fmm_b200_server_trim": (_i, [_vp]),
     "fmm_b200_direct": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_direct_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp, _d, _vp]),
     "fmm_b200_fp32_peak": (_i, [_i, _vp]),
@@ -549,6 +550,12 @@ class Server:
         if rc != FMM_OK:
             raise FmmError(rc, self.lib.fmm_b200_last_error(None).decode())
         self._n = {}
+
+    def trim(self):
+        """Free the buffers the workers' handles grew out of (fmm_b200_server_trim)."""
+        rc = self.lib.fmm_b200_server_trim(self.h)
+        if rc != FMM_OK:
+            raise FmmError(rc, "server trim failed")
 
     def set_theta(self, P, theta):
         """Opening angle of the requests of order P submitted from now on."""

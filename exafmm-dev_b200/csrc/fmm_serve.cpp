@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -78,6 +79,7 @@ struct fmm_b200_server {
   std::vector<std::unique_ptr<Worker>> workers;
   std::thread scheduler;
   bool stop = false;
+  bool paused = false;  // fmm_b200_server_trim holds new batches back while it frees
   long long next_id = 1;
   long long completed = 0, bodies_done = 0, batches = 0;
   // worker seconds spent staging inputs, in the batched solve, and copying results out
@@ -132,6 +134,42 @@ size_t estimate_bytes(const fmm_b200_config& c, int n, int P) {
   return (size_t)n * (8 * real + 48) + cells * (2 * ncoef * real + 160) + cells * 400 * 8;
 }
 
+// A new handle solves two synthetic batches of kBatchBodies bodies before its first
+// request: one Plummer sphere (a deep tree) and 256 cubes of equal size (many shallow trees,
+// the most cells and list entries per body), so that its device arrays reach the sizes of
+// a full batch now rather than one growth at a time during later passes.  Deterministic
+// (a 64-bit linear congruential generator); uses the worker's pinned staging.
+void presize(fmm_b200_solver* h, double* pin) {
+  const int n = (int)kBatchBodies;
+  double *x = pin, *q = x + 3 * (size_t)n, *p = q + n, *f = p + n;
+  unsigned long long st = 0x9e3779b97f4a7c15ULL;
+  auto uni = [&st]() {  // [0, 1)
+    st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+    return (double)(st >> 11) * (1.0 / 9007199254740992.0);
+  };
+  for (int i = 0; i < n; i++) {  // Plummer, a = 1, radii clipped at 10
+    double r;
+    do {
+      const double u = uni();
+      r = u > 0 ? 1.0 / std::sqrt(std::pow(u, -2.0 / 3.0) - 1.0) : 1e9;
+    } while (!(r < 10.0));
+    const double ct = 2 * uni() - 1, ph = 2 * 3.141592653589793 * uni();
+    const double st2 = std::sqrt(1 - ct * ct);
+    x[3 * i] = r * st2 * std::cos(ph);
+    x[3 * i + 1] = r * st2 * std::sin(ph);
+    x[3 * i + 2] = r * ct;
+    q[i] = 1.0 / n;
+  }
+  int one = n;
+  if (fmm_b200_solve_batch_host(h, 1, &one, x, q, p, f) != FMM_OK) return;
+  std::vector<int> counts(256, n / 256);
+  for (int i = 0; i < n; i++) {
+    for (int d = 0; d < 3; d++) x[3 * i + d] = 2 * uni() - 1;
+    q[i] = 2 * uni() - 1;
+  }
+  fmm_b200_solve_batch_host(h, 256, counts.data(), x, q, p, f);
+}
+
 void worker_loop(fmm_b200_server* S, Worker* W) {
   cudaSetDevice(S->cfg.device);
   cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking);
@@ -159,6 +197,7 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
       rc = fmm_b200_create(&c, &h);
       if (rc == FMM_OK) rc = fmm_b200_set_stream(h, W->stream);
       if (rc != FMM_OK) h = nullptr;
+      if (h && W->pin && W->pin_cap >= 8 * kBatchBodies) presize(h, W->pin);
     }
     std::vector<int> counts;
     size_t n = 0;
@@ -206,7 +245,6 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
       }
     }
     const auto t_done = Clock::now();
-    bool idle = false;
     {
       std::lock_guard<std::mutex> lk(S->mu);
       for (auto& r : batch) {
@@ -224,16 +262,9 @@ void worker_loop(fmm_b200_server* S, Worker* W) {
       S->t_unstage += std::chrono::duration<double>(t_done - t_b).count();
       W->busy = false;
       if (rc != FMM_OK && h) S->err = fmm_b200_last_error(h);
-      idle = S->pending.empty();
-      for (auto& w : S->workers) idle = idle && !w->busy;
     }
     S->cv.notify_all();
     S->done_cv.notify_all();
-    // the server has gone idle: give back the buffers this worker's handles grew out of (a
-    // device-wide synchronisation, which during a busy period would stall the other workers)
-    if (idle)
-      for (auto& kv : W->handles)
-        if (kv.second) fmm_b200_trim(kv.second);
   }
   for (auto& kv : W->handles)
     if (kv.second) fmm_b200_destroy(kv.second);
@@ -248,7 +279,7 @@ void scheduler_loop(fmm_b200_server* S) {
     Worker* free_w = nullptr;
     S->cv.wait(lk, [&] {
       if (S->stop) return true;
-      if (S->pending.empty()) return false;
+      if (S->pending.empty() || S->paused) return false;
       free_w = nullptr;
       for (auto& w : S->workers)
         if (!w->busy) {
@@ -405,6 +436,27 @@ int fmm_b200_server_profile(fmm_b200_server* S, double* stage_s, double* solve_s
   if (solve_s) *solve_s = S->t_solve;
   if (unstage_s) *unstage_s = S->t_unstage;
   return FMM_OK;
+}
+
+int fmm_b200_server_trim(fmm_b200_server* S) {
+  if (!S) return FMM_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(S->mu);
+  S->done_cv.wait(lk, [&] {  // no batch running; new ones wait until the trim is done
+    for (auto& w : S->workers)
+      if (w->busy) return false;
+    return true;
+  });
+  S->paused = true;
+  lk.unlock();
+  int rc = FMM_OK;
+  for (auto& w : S->workers)
+    for (auto& kv : w->handles)
+      if (kv.second && fmm_b200_trim(kv.second) != FMM_OK) rc = FMM_ERR_CUDA;
+  lk.lock();
+  S->paused = false;
+  lk.unlock();
+  S->cv.notify_all();
+  return rc;
 }
 
 int fmm_b200_server_destroy(fmm_b200_server* S) {

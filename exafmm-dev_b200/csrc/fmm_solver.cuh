@@ -25,8 +25,8 @@ namespace fmmb200 {
 // A grow-only device array owned by one solver: freed with it, moved (never copied).
 // Buffers it grows out of are retired, not freed, until the array is released: cudaFree
 // synchronises the whole device, which would stall every other stream at each growth (the
-// serving loop's other workers among them).  Growth is geometric (x1.5), so the retired
-// buffers add up to at most twice the final size.
+// serving loop's other workers among them).  Growth doubles, so the retired buffers add up
+// to at most the final size, and a handle that meets ever larger inputs grows a few times.
 template <typename U> struct DevArr {
   U* p = nullptr;
   size_t cap = 0;
@@ -57,7 +57,7 @@ template <typename U> struct DevArr {
     if (p) retired.push_back(p);
     p = nullptr;
     cap = 0;
-    size_t want = n + n / 2 + 256;
+    size_t want = 2 * n + 256;
     g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaMalloc((void**)&p, want * sizeof(U));
     if (e != cudaSuccess) {

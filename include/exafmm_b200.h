@@ -102,7 +102,7 @@ int fmm_b200_destroy(fmm_b200_solver* s);
 int fmm_b200_set_stream(fmm_b200_solver* s, void* stream);
 /* A handle grows its device arrays when a solve needs more, and keeps the buffers it grew
  * out of instead of freeing them during the solve (cudaFree synchronises the whole device,
- * which would stall the caller's other streams); they add up to at most twice the arrays'
+ * which would stall the caller's other streams); they add up to at most the arrays'
  * final size and are freed with the handle.  fmm_b200_trim frees them now: a device-wide
  * synchronisation, for a moment when the device is idle.  No reference counterpart. */
 int fmm_b200_trim(fmm_b200_solver* s);
@@ -283,7 +283,9 @@ int fmm_b200_autotune_p2p(fmm_b200_solver* s, const int* lanes4_max, const int* 
  * each) and a scheduler that batches pending requests of equal order P, in arrival order,
  * within hbm_budget_bytes of estimated device memory, max_batch solves and 2^21 bodies
  * per batch (a larger request rides alone).  Each worker holds pinned host staging for
- * 2^21 bodies (128 MB) from the start.  Batches on different workers overlap on the device;
+ * 2^21 bodies (128 MB) from the start, and sizes each new handle (the first request of an
+ * order on a worker) with two synthetic batches of 2^21 bodies before it takes requests, so
+ * that later passes rarely allocate.  Batches on different workers overlap on the device;
  * a request arriving while batches run joins the next batch a worker takes.  cfg supplies
  * basis, theta, ncrit, nspawn, precision and device (its P need not be compiled for the
  * basis); P comes with each request.  submit copies the inputs; wait blocks
@@ -311,6 +313,12 @@ int fmm_b200_server_stats(fmm_b200_server* srv, long long* completed, long long*
  * buffer, inside the batched solve (host<->device copies included), copying results out. */
 int fmm_b200_server_profile(fmm_b200_server* srv, double* stage_s, double* solve_s,
                             double* unstage_s);
+/* Free the device buffers the workers' handles have grown out of (fmm_b200_trim on each):
+ * waits until no batch runs and holds new batches back meanwhile (a device-wide
+ * synchronisation: for a quiet moment).  The server never does this by itself, so that a
+ * burst that arrives while it would run is not held up; the buffers kept add up to at most
+ * the handles' arrays, and destroy frees everything. */
+int fmm_b200_server_trim(fmm_b200_server* srv);
 int fmm_b200_server_destroy(fmm_b200_server* srv);
 
 /* ---- utilities ----------------------------------------------------------------------- */

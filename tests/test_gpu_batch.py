@@ -155,6 +155,11 @@ def test_server_other_bases_and_precisions(basis, prec, orders, datasets):
                      hbm_budget_gb=8.0, workers=2, max_batch=8)
     ids = [(k, srv.submit(x, q, P)) for k, (x, q, P) in enumerate(reqs)]
     results = {k: srv.wait(rid)[0] for k, rid in ids}
+    srv.trim()  # frees the grown-out buffers; the handles stay usable
+    x, q, P = reqs[-1]
+    again = srv.wait(srv.submit(x, q, P))[0]
+    ok = ~np.isnan(again)
+    assert np.array_equal(again[ok], results[len(reqs) - 1][ok])
     srv.close()
     solvers = {}
     for k, (x, q, P) in enumerate(reqs):

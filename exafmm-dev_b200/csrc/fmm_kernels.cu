@@ -410,6 +410,7 @@ void op_p2p(Solver<T>& s, int n, const int* ci, const int* cj, const int* image,
   check_disjoint_bodies(s, L.targets, "P2P");
   const int nt = (int)L.targets.size();
   upload_pairs(s, L, s.p2p, s.p2p_off);
+  s.p2p_ordered = false;  // the solver's P2P lists (and their target order) are replaced
   upload_list(s, nt, L.targets.data());
   // save the targets, let the P2P write its sums, add the saved values back
   s.k_trg.ensure(2 * (size_t)s.n);
@@ -507,6 +508,7 @@ int fmm_b200_kernel_set_cells(fmm_b200_solver* h, int nc, const double* X, const
     s.root_cell.clear();
     s.level_lo.assign({0, nc});
     s.nm2l = s.np2p = 0;
+    s.p2p_ordered = false;
     s.trav_sized = false;
     s.stage = ST_TREE;
     prepare(s);  // expansions and targets zero

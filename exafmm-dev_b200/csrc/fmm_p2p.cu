@@ -359,7 +359,7 @@ template <typename T> void run_p2p(Solver<T>& s) {
   if (s.nleaves == 0) return;
   constexpr bool comp = sizeof(T) == 4;
   k_p2p<T, comp><<<ceil_div(s.nleaves, kP2PWarps), 32 * kP2PWarps, 0, s.stream>>>(
-      s.leaves.p, s.nleaves, s.p2p_off.p, s.p2p.p, s.c_ibody.p, s.c_nbody.p, s.bodies.p,
+      s.p2p_ordered ? s.p2p_order.p : s.leaves.p, s.nleaves, s.p2p_off.p, s.p2p.p, s.c_ibody.p, s.c_nbody.p, s.bodies.p,
       (T)s.cfg.eps2, (T)s.cfg.cycle, s.trg_s.p, s.trg_e.p, std::min(s.p2p_g4, 8),
       std::min(s.p2p_g2, 16));
   FMM_LAUNCH_CHECK();

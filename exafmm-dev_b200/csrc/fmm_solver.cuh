@@ -162,6 +162,11 @@ struct SolverBase {
   bool p2p_pending = false;
   cudaEvent_t p2p_ready = nullptr;
   DevArr<int> m2l_tgt;  // M2L target cells, by descending number of 32-source batches
+  // P2P target leaves by descending body pairs (valid while p2p_ordered: the lists of the
+  // last traversal), so that the longest leaves start first and none is left alone at the end
+  DevArr<int> p2p_order, p2p_widx;
+  DevArr<unsigned> p2p_wkey, p2p_wkey2;
+  bool p2p_ordered = false;
   int m2l_ntgt = 0;
   DevArr<unsigned long long> p2p_pairs_count;
   DevArr<double> dtmp;  // host <-> device conversion scratch
@@ -236,7 +241,7 @@ void sort_pairs_u64(SolverBase& s, const unsigned long long* kin, unsigned long 
 void sort_keys_u64(SolverBase& s, const unsigned long long* kin, unsigned long long* kout,
                    int n, int end_bit);
 void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,
-                    int* vout, int n, int end_bit);
+                    int* vout, int n, int end_bit, DevArr<char>* tmp = nullptr);
 // scratch: s.cub_tmp, or tmp for a scan that may run beside other CUB calls of the solver
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n,
                        DevArr<char>* tmp = nullptr);

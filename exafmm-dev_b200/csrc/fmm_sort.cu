@@ -40,14 +40,15 @@ void segmented_sort_pairs_u64(SolverBase& s, const unsigned long long* kin,
 }
 
 void sort_pairs_u32(SolverBase& s, const unsigned* kin, unsigned* kout, const int* vin,
-                    int* vout, int n, int end_bit) {
+                    int* vout, int n, int end_bit, DevArr<char>* tmp) {
   if (n <= 0) return;
+  DevArr<char>& t = tmp ? *tmp : s.cub_tmp;
   size_t bytes = 0;
   FMM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit,
                                            s.stream));
-  s.cub_tmp.ensure(bytes);
-  FMM_CUDA(cub::DeviceRadixSort::SortPairs(s.cub_tmp.p, bytes, kin, kout, vin, vout, n, 0,
-                                           end_bit, s.stream));
+  t.ensure(bytes);
+  FMM_CUDA(cub::DeviceRadixSort::SortPairs(t.p, bytes, kin, kout, vin, vout, n, 0, end_bit,
+                                           s.stream));
 }
 
 void exclusive_sum_int(SolverBase& s, const int* in, int* out, int n, DevArr<char>* tmp) {

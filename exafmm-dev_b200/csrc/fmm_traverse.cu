@@ -729,9 +729,42 @@ void finish_p2p_list(SolverBase& s) {
   }
 }
 
+// P2P work of each leaf, as a descending sort key: its bodies times the bodies of its
+// source leaves (0 without pairs)
+__global__ void k_p2p_work(int nleaves, const int* __restrict__ leaves,
+                           const int* __restrict__ off,
+                           const unsigned long long* __restrict__ pairs,
+                           const int* __restrict__ nbody, unsigned* __restrict__ key,
+                           int* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nleaves) return;
+  const int c = leaves[i];
+  unsigned long long src = 0;
+  for (int k = off[c]; k < off[c + 1]; k++) src += nbody[pair_cell((unsigned)pairs[k])];
+  const unsigned long long w = src * (unsigned long long)nbody[c];
+  key[i] = ~(unsigned)(w < 0xffffffffULL ? w : 0xffffffffULL);
+  idx[i] = c;
+}
+
+// the leaves in the order of k_p2p_work's keys, on the solver's current stream
+static void order_p2p_targets(SolverBase& s, DevArr<char>* tmp) {
+  const int nl = s.nleaves;
+  if (nl <= 0) return;
+  s.p2p_wkey.ensure(nl);
+  s.p2p_wkey2.ensure(nl);
+  s.p2p_widx.ensure(nl);
+  s.p2p_order.ensure(nl);
+  k_p2p_work<<<ceil_div(nl, 256), 256, 0, s.stream>>>(nl, s.leaves.p, s.p2p_off.p, s.p2p.p,
+                                                      s.c_nbody.p, s.p2p_wkey.p, s.p2p_widx.p);
+  FMM_LAUNCH_CHECK();
+  sort_pairs_u32(s, s.p2p_wkey.p, s.p2p_wkey2.p, s.p2p_widx.p, s.p2p_order.p, nl, 32, tmp);
+  s.p2p_ordered = true;
+}
+
 template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
   const int TB = 256;
   s.nm2l = s.np2p = s.p2p_body_pairs = 0;
+  s.p2p_ordered = false;
   if (s.ncells == 0) return;
   if (s.ncells > (int)kCellMask)
     throw FmmError(FMM_ERR_NOT_SUPPORTED, "more than 2^27 - 1 cells (list pairs hold 27-bit cells)");
@@ -772,6 +805,7 @@ template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
     try {
       group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1, s.seg_cnt2.p,
                       s.seg_keys2.p, &s.cub_tmp2);
+      order_p2p_targets(s, &s.cub_tmp2);
       FMM_CUDA(cudaMemcpyAsync((int*)(hc + 5) + 1, overflow + 1, sizeof(int),
                                cudaMemcpyDeviceToHost, s.stream));
       FMM_CUDA(cudaEventRecord(s.p2p_ready, s.stream));
@@ -783,6 +817,7 @@ template <typename T> void build_lists(Solver<T>& s, bool defer_p2p) {
   } else {
     group_by_target(s, s.p2p.p, np2p, b, s.p2p_off.p, overflow + 1, s.seg_cnt.p,
                     (unsigned*)s.list_tmp.p, nullptr);
+    order_p2p_targets(s, nullptr);
   }
   // M2L target order: by descending pair count in buckets (stable in cell index)
   {

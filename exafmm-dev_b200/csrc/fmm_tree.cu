@@ -847,6 +847,7 @@ template <typename T> void build_tree(Solver<T>& s) {
   const int n = s.n;
   const int TB = 256;
   s.kc_valid = false;  // the host copies of the cells' index fields are stale
+  s.p2p_ordered = false;  // so is the P2P target order of the last traversal
   s.level_lo.clear();
   s.ncells = s.maxlevel = s.nleaves = 0;
   // roots: non-empty solves in order

@@ -520,6 +520,8 @@ int fmm_b200_destroy(fmm_b200_solver* h) {
     if (s.side_lo) cudaStreamDestroy(s.side_lo);
     if (s.p2p_ready) cudaEventDestroy(s.p2p_ready);
     if (s.scal_host) cudaFreeHost(s.scal_host);
+    if (s.roots_host) cudaFreeHost(s.roots_host);
+    for (int2* q : s.roots_retired) cudaFreeHost(q);
     delete h->base;
   }
   delete h;

@@ -120,6 +120,12 @@ struct SolverBase {
   DevArr<char> cub_tmp;
   DevArr<int> scal;          // small device scalars (counters, flags)
   int* scal_host = nullptr;  // pinned mirror of scal
+  // pinned staging of the traversal's first frontier (its copy needs no host wait: every
+  // solve reads the traversal's totals back before the next one writes here); buffers it
+  // grew out of are kept until the handle is destroyed (cudaFreeHost synchronises)
+  int2* roots_host = nullptr;
+  size_t roots_cap = 0;
+  std::vector<int2*> roots_retired;
   // cells
   DevArr<int> c_iparent, c_ichild, c_nchild, c_ibody, c_nbody, c_level;
   DevArr<int4> c_info;  // per cell (NCHILD, ICHILD, NBODY, IBODY): one load for the traversal

@@ -595,9 +595,18 @@ template <typename T> static void upload_roots(Solver<T>& s) {
   }
   s.nfront0 = (int)roots.size();
   s.front.ensure(std::max(s.nfront0, 1));
-  FMM_CUDA(cudaMemcpyAsync(s.front.p, roots.data(), sizeof(int2) * roots.size(),
+  if (roots.empty()) return;
+  if (roots.size() > s.roots_cap) {
+    if (s.roots_host) s.roots_retired.push_back(s.roots_host);
+    s.roots_host = nullptr;
+    s.roots_cap = 0;
+    const size_t cap = std::max<size_t>(2 * roots.size(), 64);
+    FMM_CUDA(cudaMallocHost((void**)&s.roots_host, sizeof(int2) * cap));
+    s.roots_cap = cap;
+  }
+  std::copy(roots.begin(), roots.end(), s.roots_host);
+  FMM_CUDA(cudaMemcpyAsync(s.front.p, s.roots_host, sizeof(int2) * roots.size(),
                            cudaMemcpyHostToDevice, s.stream));
-  FMM_CUDA(cudaStreamSynchronize(s.stream));  // roots[] lives on the host stack
 }
 
 // Traversal with the sizes known up front: per step a count pass, one host read of the

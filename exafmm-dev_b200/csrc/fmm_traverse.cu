@@ -37,14 +37,12 @@ enum {
 // every pair below them has a target inside that cell, so the pairs kept are exactly the
 // whole traversal's pairs of the part's targets (b0 = INT_MIN, b1 = INT_MAX keep all).
 template <typename T>
-__device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
-                                        const int4* __restrict__ info, int nspawn, T cycle,
-                                        int mutual, int b0, int b1, int* nout) {
+__device__ __forceinline__ int classify_data(int ci, int cjp, const vec4<T>& a, const vec4<T>& b,
+                                             const int4& fi, const int4& fj, int nspawn, T cycle,
+                                             int mutual, int b0, int b1, int* nout) {
   const int cj = pair_cell((unsigned)cjp);
   T px, py, pz;
   img_shift<T>(pair_img((unsigned)cjp), cycle, px, py, pz);
-  const vec4<T> a = X[ci], b = X[cj];
-  const int4 fi = info[ci], fj = info[cj];
   if (!(fi.w < b1 && fi.w + fi.z > b0)) {
     *nout = 0;
     return PAIR_DROP;
@@ -83,6 +81,14 @@ __device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restri
   }
   *nout = nj;
   return PAIR_SPLIT_J;
+}
+template <typename T>
+__device__ __forceinline__ int classify(int ci, int cjp, const vec4<T>* __restrict__ X,
+                                        const int4* __restrict__ info, int nspawn, T cycle,
+                                        int mutual, int b0, int b1, int* nout) {
+  const int cj = pair_cell((unsigned)cjp);
+  return classify_data<T>(ci, cjp, X[ci], X[cj], info[ci], info[cj], nspawn, cycle, mutual,
+                          b0, b1, nout);
 }
 
 // pass 1: per-block totals of (M2L, P2P, children) added to three device counters
@@ -227,16 +233,42 @@ __global__ void __launch_bounds__(256)
       k[u] = 0;
       p[u] = t0 + u < nfront ? front[t0 + u] : make_int2(0, 0);
     }
+    bool okp[kTravItems];
+#pragma unroll
+    for (int u = 0; u < kTravItems; u++)
+      okp[u] = t0 + u < nfront && (unsigned)p[u].x < (unsigned)ncells &&
+               (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
+               pair_img((unsigned)p[u].y) < 27;
+    if constexpr (sizeof(T) == 4) {
+      // FP32: all the items' cell data loaded before any is classified, so that the gathers
+      // of the four pairs are in flight together (FP64 cells take twice the registers: one
+      // pair at a time)
+      vec4<T> ca[kTravItems], cb[kTravItems];
+      int4 fa[kTravItems], fb[kTravItems];
+#pragma unroll
+      for (int u = 0; u < kTravItems; u++)
+        if (okp[u]) {
+          const int cj = pair_cell((unsigned)p[u].y);
+          ca[u] = X[p[u].x];
+          cb[u] = X[cj];
+          fa[u] = info[p[u].x];
+          fb[u] = info[cj];
+        }
+#pragma unroll
+      for (int u = 0; u < kTravItems; u++)
+        if (okp[u])
+          ty[u] = classify_data<T>(p[u].x, p[u].y, ca[u], cb[u], fa[u], fb[u], nspawn, cycle,
+                                   mutual, b0, b1, &k[u]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < kTravItems; u++)
+        if (okp[u])
+          ty[u] = classify<T>(p[u].x, p[u].y, X, info, nspawn, cycle, mutual, b0, b1, &k[u]);
+    }
 #pragma unroll
     for (int u = 0; u < kTravItems; u++) {
-      if (t0 + u < nfront) {
-        if ((unsigned)p[u].x < (unsigned)ncells &&
-            (unsigned)pair_cell((unsigned)p[u].y) < (unsigned)ncells &&
-            pair_img((unsigned)p[u].y) < 27)
-          ty[u] = classify<T>(p[u].x, p[u].y, X, info, nspawn, cycle, mutual, b0, b1, &k[u]);
-        else
-          atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
-      }
+      if (t0 + u < nfront && !okp[u])
+        atomicOr(&ctr[2], 1ULL);  // never expected: reported to the host, pair skipped
       v += (ty[u] == PAIR_M2L ? (unsigned)k[u] : 0u) |
            (ty[u] == PAIR_P2P ? (unsigned)k[u] << 9 : 0u) |
            (ty[u] >= PAIR_SPLIT_I ? (unsigned)k[u] << 18 : 0u);

@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(tr_threads<T>())
 //         of FP32's in registers; P = 10 takes four passes, none spilling.
 template <typename T> struct M2LBudget {
   static constexpr int W = sizeof(T) == 4 ? 12 : 8;
-  static constexpr int IN = sizeof(T) == 4 ? 115 : 100;
-  static constexpr int OUT = sizeof(T) == 4 ? 150 : 105;
+  static constexpr int IN = sizeof(T) == 4 ? 139 : 100;
+  static constexpr int OUT = sizeof(T) == 4 ? 149 : 105;
 };
 __host__ __device__ constexpr int m2l_regs_out(int P, int J0) {
   return sph::NT(P) - sph::sidx(J0, 0) + 2 * (sph::NT(P) - sph::sidx(J0, 0)) +

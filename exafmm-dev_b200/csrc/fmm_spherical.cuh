@@ -279,17 +279,15 @@ __host__ __device__ constexpr int m2l_regs_out(int P, int J0) {
 template <typename T> __host__ __device__ constexpr bool m2l_pass_out(int P, int J0) {
   return m2l_regs_out(P, J0) <= M2LBudget<T>::OUT;
 }
-// In FP32 a source-streaming pass takes every degree its registers hold (it runs faster
-// per term than the output-streaming one); FP64 also stops it where the rest fits one
-// output-streaming pass.
+// A source-streaming pass takes every degree its registers hold: it runs faster per term
+// than the output-streaming pass that finishes the remaining degrees.
 template <typename T> __host__ __device__ constexpr int m2l_pass_end(int P, int J0) {
   if (m2l_pass_out<T>(P, J0)) return P;
   const int rho = sph::NT(P) - sph::sidx(J0, 0);
   int j = J0, outs = 0;
   while (j < P) {
     const int o = outs + j + 1;
-    if (j > J0 && (rho + 4 * o > M2LBudget<T>::IN ||
-                   (sizeof(T) == 8 && m2l_pass_out<T>(P, j))))
+    if (j > J0 && rho + 4 * o > M2LBudget<T>::IN)
       break;
     outs = o;
     j++;
